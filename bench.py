@@ -1,0 +1,278 @@
+"""Benchmark of the fused VISCOPLASTIC-LBM time step on B200.
+
+Workload (one "step" = one fused time step over the whole lattice): the
+regularized Bingham plane channel, D3Q19, 256 x 128 x 64, plastic tau 0.8
+(eta_p = 0.1), yield stress 1e-5, body force gx = 5e-6, bounce-back walls at
+y = 0 and y = NY-1, periodic x and z, rho = 1 u = 0 initial state, FP32
+populations (the BASELINE second configuration).  Synthetic by construction:
+the lattice state evolves from the equilibrium initial condition.
+
+Metric: MLUPS (million lattice-node updates per second, all nodes counted as
+the reference does, src/CUDA/main.cu:411), plus the HBM-roofline fraction of
+the fused kernel.  Multi-GPU runs are independent replicas (the path is one
+lattice per GPU); value = all ranks' node updates / max-over-ranks time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "viscoplastic-lbm_b200"))
+
+NX, NY, NZ, Q = 256, 128, 64, 19
+WORKLOAD = "d3q19_regularized_bingham_channel_256x128x64"
+METRIC = "MLUPS"
+L2_BYTES = 126 * 2 ** 20
+
+
+def config_dict(storage="f32"):
+    return {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "velocity_set": "D3Q19",
+            "collision": "regularized", "rheology": "bingham", "tau_p": 0.8, "yield_stress": 1e-5,
+            "gx": 5e-6, "walls": "y (half-way bounce-back)", "periodic": "x,z", "storage": storage,
+            "streaming": "AA in-place", "l2_policy": "population array (159 MB) larger than the 126 MB L2",
+            "parallelism": "replicas"}
+
+
+def make_cfg(vlbm, storage=0):
+    return vlbm.Config.default(nx=NX, ny=NY, nz=NZ, vel_set=19, collision=vlbm.OP_REGULARIZED,
+                               rheology=vlbm.BINGHAM, eta_p=(0.8 - 0.5) / 3.0, yield_stress=1e-5,
+                               fx=5e-6, storage=storage)
+
+
+def measured_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """dram read+write bytes per launch of the fused kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "fused_step_d3q19_bingham_256x128x64.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        rows = []
+        for line in open(self.out.name):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.out.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_baseline(vlbm, seconds_budget=15.0):
+    """The FP64 OpenMP oracle (restated reference step) on the host cores."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    cfg = make_cfg(vlbm)
+    # bounded sample: same x-y cross-section, 8 z-planes (periodic in z)
+    nz = 8
+    cfg.nz = nz
+    node_map = vlbm.build_node_map(vlbm.BUILDER_PLATES_Y, NX, NY, nz)
+    o = oracle.Oracle(cfg, node_map)
+    o.step(2)
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds_budget:
+        o.step(5)
+        steps += 5
+    dt = time.perf_counter() - t0
+    mlups = steps * NX * NY * nz / dt / 1e6
+    return {"value": mlups, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{NX}x{NY}x{nz} slab of the workload, {steps} steps, FP64 oracle, {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    import vlbm
+    if rank != 0:
+        return 0
+    import oracle  # noqa: F401  (path added in cpu_baseline)
+    base = cpu_baseline(vlbm, seconds_budget=max(5.0, min(60.0, 2.0 * args.steps)))
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": METRIC,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict("f64"), "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="vlbm", choices=["vlbm", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import vlbm
+
+    storage = {"f32": vlbm.STORE_F32, "f16": vlbm.STORE_F16, "bf16": vlbm.STORE_BF16}[args.storage]
+    cfg = make_cfg(vlbm, storage)
+    cfg.device = local
+    sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sim.set_stream(stream.cuda_stream)
+    variant = sim.autotune()
+    sim.init_equilibrium(1.0, 0, 0, 0)
+
+    sim.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    sim.sync()
+    t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    N = NX * NY * NZ
+    value = world * N * args.steps / (ms_max / 1e3) / 1e6
+
+    info = sim.info()
+    bytes_per_node = info.bytes_per_node_step
+    achieved_gbs = bytes_per_node * N / (ms / 1e3 / args.steps) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = committed_traffic()
+
+    # end to end through the public API with host buffers: upload the state from
+    # pinned host memory, advance, read the macroscopics back
+    import numpy as np
+    pops_host = torch.empty(Q * N, dtype=torch.float32).pin_memory()
+    pops_host.copy_(torch.from_numpy(sim.populations().ravel()))
+    ux_host = torch.empty(4 * N, dtype=torch.float32).pin_memory()
+    import ctypes
+    lib = vlbm.lib()
+    F = ctypes.POINTER(ctypes.c_float)
+    pp = ctypes.cast(pops_host.data_ptr(), F)
+    outs = [ctypes.cast(ux_host.data_ptr() + k * N * 4, F) for k in range(4)]
+    e2e_steps = args.steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = lib.vlbm_set_populations(sim.handle, pp, Q * N)
+    st |= lib.vlbm_step(sim.handle, e2e_steps)
+    st |= lib.vlbm_get_macroscopics(sim.handle, outs[0], outs[1], outs[2], outs[3], None)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError("e2e leg failed: " + lib.vlbm_last_error().decode())
+    e2e_mlups = world * N * e2e_steps / e2e_s / 1e6
+    h2d = Q * N * 4 / e2e_steps
+    d2h = 4 * N * 4 / e2e_steps
+    sim.sync()
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(vlbm)
+
+    if rank == 0:
+        dtype = {"f32": "f32", "f16": "f32 arithmetic, f16 storage", "bf16": "f32 arithmetic, bf16 storage"}
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype[args.storage], "data": "synthetic",
+            "config": config_dict(args.storage),
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": achieved_gbs / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_node": bytes_per_node,
+                         "roofline_mlups": peak * 1e9 / bytes_per_node / 1e6},
+            "cpu_baseline": base,
+            "e2e": {"value": e2e_mlups, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "note": "vlbm_set_populations from pinned host + K steps + vlbm_get_macroscopics to host, "
+                            "wall clock, bytes amortised over K steps"},
+            "gpu_launches": args.steps,
+            "kernel_variant": variant,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,294 @@
+/*
+ * vlbm.h -- C ABI of the B200-native VISCOPLASTIC-LBM fluid time step.
+ *
+ * Plain C linkage, plain pointers and sizes, no CUDA or torch types in any
+ * signature.  Every call returns a vlbm_status (0 = ok); nothing calls exit().
+ * One simulation handle per host thread; the library holds no global state
+ * besides the per-device kernel caches.  Host buffers are owned by the
+ * caller, device buffers by the library.
+ *
+ * The reference has no library boundary: its hot path is entered through
+ * CUDA kernels and compile-time macros.  Each entry point below names the
+ * reference interface it replaces (paths inside CERNN/VISCOPLASTIC-LBM).
+ */
+#ifndef VLBM_H
+#define VLBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VLBM_ABI_VERSION 1
+
+typedef int vlbm_status;
+enum {
+    VLBM_OK = 0,
+    VLBM_ERR_INVALID = 1,      /* bad argument or configuration           */
+    VLBM_ERR_CUDA = 2,         /* CUDA runtime error (message: vlbm_last_error) */
+    VLBM_ERR_NOMEM = 3,        /* device or host allocation failed        */
+    VLBM_ERR_UNSUPPORTED = 4,  /* combination the reference does not define */
+    VLBM_ERR_DIVERGED = 5,     /* non-finite or non-positive density seen  */
+    VLBM_ERR_STATE = 6,        /* call out of order (e.g. no geometry yet) */
+    VLBM_ERR_TIMEOUT = 7,      /* a bounded device wait gave up            */
+    VLBM_ERR_NOT_FOUND = 8,    /* unknown name / missing file              */
+    VLBM_ERR_IO = 9            /* host file I/O failed                     */
+};
+
+/* Velocity sets: src/CUDA/velocitySets/D3Q19.h:31-46, D3Q27.h:39-56. */
+enum { VLBM_D3Q19 = 19, VLBM_D3Q27 = 27 };
+
+/* Collision operator.  REGULARIZED is the operator compiled by default in
+ * src/CUDA/lbm.cu:263-461; BGK is src/CUDA/collisionSchemes/collisionForceNoReg.txt. */
+enum { VLBM_OP_REGULARIZED = 0, VLBM_OP_BGK = 1 };
+
+/* Rheology: src/CUDA/NNF/nnf.h:10-24 (POWERLAW / BINGHAM), Newtonian otherwise. */
+enum { VLBM_NEWTONIAN = 0, VLBM_BINGHAM = 1, VLBM_POWERLAW = 2 };
+
+/* Population storage.  F32 is the reference's `dfloat=float` layout; F16/BF16
+ * store scaled deviations (f_i - w_i*rho0)*scale, arithmetic stays FP32. */
+enum { VLBM_STORE_F32 = 0, VLBM_STORE_F16 = 1, VLBM_STORE_BF16 = 2 };
+
+/* Node-map bit layout, identical to src/CUDA/structs/nodeTypeMap.h:15-133 so a
+ * map produced by a reference builder (gpuBuildBoundaryConditions) can be
+ * passed unchanged to vlbm_set_node_map. */
+#define VLBM_MAP_RHO_IDX_OFFSET 0
+#define VLBM_MAP_UZ_IDX_OFFSET 3
+#define VLBM_MAP_UY_IDX_OFFSET 6
+#define VLBM_MAP_UX_IDX_OFFSET 9
+#define VLBM_MAP_GEOMETRY_OFFSET 12
+#define VLBM_MAP_DIRECTION_OFFSET 13
+#define VLBM_MAP_SCHEME_OFFSET 18
+#define VLBM_MAP_IS_USED_OFFSET 21
+#define VLBM_MAP_SAVE_POST_COL_OFFSET 22
+
+/* BC schemes (nodeTypeMap.h:35-56) */
+enum {
+    VLBM_BC_NULL = 0, VLBM_BC_VEL_ZOUHE = 1, VLBM_BC_VEL_BOUNCE_BACK = 2,
+    VLBM_BC_PRES_ZOUHE = 3, VLBM_BC_FREE_SLIP = 4, VLBM_BC_BOUNCE_BACK = 5,
+    VLBM_BC_INTERP_BOUNCE_BACK = 6, VLBM_BC_SPECIAL = 7
+};
+/* Directions (nodeTypeMap.h:59-85) */
+enum {
+    VLBM_NORTH = 0, VLBM_SOUTH = 1, VLBM_WEST = 2, VLBM_EAST = 3, VLBM_FRONT = 4, VLBM_BACK = 5,
+    VLBM_NORTH_WEST = 6, VLBM_NORTH_EAST = 7, VLBM_NORTH_FRONT = 8, VLBM_NORTH_BACK = 9,
+    VLBM_SOUTH_WEST = 10, VLBM_SOUTH_EAST = 11, VLBM_SOUTH_FRONT = 12, VLBM_SOUTH_BACK = 13,
+    VLBM_WEST_FRONT = 14, VLBM_WEST_BACK = 15, VLBM_EAST_FRONT = 16, VLBM_EAST_BACK = 17,
+    VLBM_NORTH_WEST_FRONT = 18, VLBM_NORTH_WEST_BACK = 19, VLBM_NORTH_EAST_FRONT = 20,
+    VLBM_NORTH_EAST_BACK = 21, VLBM_SOUTH_WEST_FRONT = 22, VLBM_SOUTH_WEST_BACK = 23,
+    VLBM_SOUTH_EAST_FRONT = 24, VLBM_SOUTH_EAST_BACK = 25
+};
+enum { VLBM_CONCAVE = 0, VLBM_CONVEX = 1 };
+
+/* Named geometry builders (the builder .cu files of
+ * src/CUDA/boundaryConditionsBuilders/ that the reference copies into src/CUDA/). */
+enum {
+    VLBM_BUILDER_PERIODIC = 0,          /* no boundary nodes                           */
+    VLBM_BUILDER_PLATES_Y = 1,          /* parallelPlatesBounceBack_Y.cu: walls y=0, y=NY-1 */
+    VLBM_BUILDER_LID_DRIVEN = 2,        /* lidDrivenBounceBack.cu: walls x,y, lid y=NY-1, z periodic */
+    VLBM_BUILDER_CLOSED_BOX = 3,        /* closedBoxBounceBack.cu: all six faces       */
+    VLBM_BUILDER_SQUARE_DUCT = 4,       /* squareDuctBounceBack.cu: walls x,y, z periodic */
+    VLBM_BUILDER_DUCT_YZ = 5,           /* square duct walls y,z, periodic x (serving ducts) */
+    VLBM_BUILDER_LID_CAVITY_CLOSED = 6, /* all six faces, moving lid at y=NY-1          */
+    VLBM_BUILDER_PLATES_Y_FREE_SLIP = 7,/* bounce-back y=0, free-slip y=NY-1            */
+    VLBM_BUILDER_PLATES_Y_ZOUHE = 8     /* velocity Zou-He at y=0 and y=NY-1 (Couette)  */
+};
+
+typedef struct vlbm_config {
+    int32_t nx, ny, nz;          /* lattice size (var.h:95-100: NX, NY, NZ_TOTAL)  */
+    int32_t vel_set;             /* VLBM_D3Q19 / VLBM_D3Q27                         */
+    int32_t collision;           /* VLBM_OP_*                                       */
+    int32_t rheology;            /* VLBM_NEWTONIAN / BINGHAM / POWERLAW             */
+    int32_t storage;             /* VLBM_STORE_*                                    */
+    int32_t device;              /* CUDA device ordinal                             */
+    double tau;                  /* var.h:104 TAU (Newtonian relaxation time)       */
+    double rho0;                 /* var.h:107 RHO_0                                 */
+    double fx, fy, fz;           /* var.h:109-111 body force FX, FY, FZ             */
+    double eta_p;                /* nnf.h:125 ETA_P (Bingham plastic viscosity)     */
+    double yield_stress;         /* nnf.h:126 S_Y                                   */
+    double n_index;              /* nnf.h:116 N_INDEX (Power-Law)                   */
+    double k_consistency;        /* nnf.h:117 K_CONSISTENCY                         */
+    double gamma0;               /* nnf.h:118 GAMMA_0 (truncation)                  */
+    double ux_bc[8], uy_bc[8], uz_bc[8], rho_bc[8]; /* var.h:114-117 UX_BC..RHO_BC */
+    double storage_scale;        /* F16/BF16 deviation scale; 0 = library default   */
+    int32_t reserved[8];
+} vlbm_config;
+
+/* Fill `cfg` with the reference defaults (var.h / nnf.h values, D3Q19, FP32,
+ * regularized, Newtonian, tau=0.6, rho0=1, zero force, UX_BC etc. from var.h:114-117). */
+vlbm_status vlbm_config_default(vlbm_config* cfg);
+
+typedef struct vlbm_sim vlbm_sim;
+
+/* Replaces the allocation + gpuInitialization sequence of src/CUDA/main.cu:114-216
+ * (Populations::popAllocation populations.h:46-52, Macroscopics::macrAllocation
+ * macroscopics.h:83-124, gpuInitialization lbmInitialization.cu:48-90).
+ * Populations start at f_eq(rho0, u=0) (lbmInitialization.cu:93-111). */
+vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out);
+vlbm_status vlbm_destroy(vlbm_sim* sim);
+
+/* Replaces gpuBuildBoundaryConditions + setupBoundaryConditionsInfo
+ * (main.cu:174-194, boundaryConditionsInfo.h:76-116): takes the per-node 32-bit
+ * map in the reference's bit layout, [nz][ny][nx] order (idxScalar,
+ * globalFunctions.h:111-115).  n must equal nx*ny*nz. */
+vlbm_status vlbm_set_node_map(vlbm_sim* sim, const uint32_t* map, size_t n);
+
+/* Host-side restatement of the named builders; writes nx*ny*nz words. */
+vlbm_status vlbm_build_node_map(int builder, int nx, int ny, int nz, uint32_t* map_out, size_t n);
+
+/* Re-initialise populations to equilibrium at (rho, ux, uy, uz) everywhere and
+ * reset step counter, omega state and IBM forces (lbmInitialization.cu:48-150). */
+vlbm_status vlbm_init_equilibrium(vlbm_sim* sim, double rho, double ux, double uy, double uz);
+
+/* Advance nsteps fluid time steps (one iteration of the loop at main.cu:270-394
+ * each: gpuMacrCollisionStream lbm.cu:4-504, gpuPopulationsTransfer lbm.cu:601-657,
+ * gpuApplyBC lbm.cu:580-598, and the IBM step ibm.cu:6-192 when spheres exist).
+ * Asynchronous on the simulation's stream. */
+vlbm_status vlbm_step(vlbm_sim* sim, uint32_t nsteps);
+
+/* Block until the simulation's stream is idle; returns VLBM_ERR_DIVERGED when the
+ * device-side guard saw a non-finite or non-positive density since the last check. */
+vlbm_status vlbm_sync(vlbm_sim* sim);
+
+/* Use an external CUDA stream (cudaStream_t passed as void*; NULL = library stream). */
+vlbm_status vlbm_set_stream(vlbm_sim* sim, void* cuda_stream);
+
+/* Macroscopics of the current state, the values gpuMacrCollisionStream would save
+ * (lbm.cu:79-111, 247-261) and copyMacr would bring to the host
+ * (macroscopics.h:173-283): rho, u = (sum f c + F/2)/rho, omega.  Host arrays of
+ * nx*ny*nz floats in [nz][ny][nx] order; any pointer may be NULL.  With spheres
+ * present the values are those after the IBM step (ibm.cu:544-648 plus the
+ * multi-direct-forcing velocity corrections). */
+vlbm_status vlbm_get_macroscopics(vlbm_sim* sim, float* rho, float* ux, float* uy,
+                                  float* uz, float* omega);
+/* Same into device pointers (each nx*ny*nz floats), asynchronous. */
+vlbm_status vlbm_get_macroscopics_device(vlbm_sim* sim, float* rho, float* ux, float* uy,
+                                         float* uz, float* omega);
+
+/* Populations f_i(x) of the current state after boundary conditions, [Q][nz][ny][nx]
+ * floats (idxPop order without the ghost plane, globalFunctions.h:143-147). */
+vlbm_status vlbm_get_populations(vlbm_sim* sim, float* pops, size_t n);
+
+/* Set the full population state (same layout); resets boundary side-state. */
+vlbm_status vlbm_set_populations(vlbm_sim* sim, const float* pops, size_t n);
+
+/* Per-node IBM force (macr.f, macroscopics.h) of the current state, [3][nz][ny][nx]. */
+vlbm_status vlbm_get_forces(vlbm_sim* sim, float* fxyz, size_t n);
+
+typedef struct vlbm_info {
+    int32_t nx, ny, nz, q;
+    int32_t storage_bytes;       /* bytes per stored population value            */
+    int64_t step;                /* current step counter                          */
+    int64_t n_bc_nodes;          /* boundary nodes with side-state                */
+    int64_t device_bytes;        /* device memory held by the simulation          */
+    double bytes_per_node_step;  /* algorithmic bytes: 2*Q*storage_bytes          */
+    int32_t n_particles, n_lagrangian_nodes;
+    int32_t last_kernel_variant; /* autotuned launch variant of the fused kernel  */
+    int32_t reserved[7];
+} vlbm_info;
+vlbm_status vlbm_get_info(vlbm_sim* sim, vlbm_info* info);
+
+/* ---------------------------------------------------------------- IBM --- */
+/* IBM parameters (src/CUDA/IBM/ibmVar.h:21-126, ibmBoundaryCondition.h:19-107). */
+typedef struct vlbm_ibm_config {
+    int32_t max_iterations;      /* IBM_MAX_ITERATION                             */
+    int32_t stencil;             /* 4 = Peskin 4-point (STENCIL_4), 2 = STENCIL_2  */
+    double thickness;            /* IBM_THICKNESS                                  */
+    double movement_alpha;       /* IBM_MOVEMENT_DISCRETIZATION                    */
+    double fluid_density;        /* FLUID_DENSITY                                  */
+    double gx, gy, gz;           /* GX, GY, GZ                                     */
+    int32_t wall_x, wall_y, wall_z; /* 1 = IBM_BC_?_WALL, 0 = IBM_BC_?_PERIODIC    */
+    double pp_friction, pw_friction, pp_restitution, pw_restitution;
+    double particle_young, particle_poisson, wall_young, wall_poisson;
+    double mesh_scale;           /* MESH_SCALE                                     */
+    double breugem;              /* BREUGEM_PARAMETER                              */
+    int32_t reserved[8];
+} vlbm_ibm_config;
+
+typedef struct vlbm_sphere {
+    double diameter;
+    double cx, cy, cz;
+    double vx, vy, vz;
+    double wx, wy, wz;
+    double density;
+    int32_t movable;
+    int32_t reserved;
+} vlbm_sphere;
+
+/* Particle state, the ParticleCenter fields (IBM/structs/particleCenter.h:65-118)
+ * that saveParticlesInfo writes (IBM/ibmReport.cpp:26-102). */
+typedef struct vlbm_particle_state {
+    double pos[3], vel[3], w[3], f[3], M[3];
+    double pos_old[3], vel_old[3], w_old[3], f_old[3], M_old[3];
+    double w_avg[3], w_pos[3];
+    double I[6];                 /* xx, yy, zz, xy, xz, yz                        */
+    double radius, volume, density, S;
+    int32_t movable, n_nodes;
+} vlbm_particle_state;
+
+vlbm_status vlbm_ibm_config_default(vlbm_ibm_config* cfg);
+/* Replaces createParticles (IBM/ibmParticlesCreation.cpp:5-43) with
+ * Particle::makeSpherePolar (IBM/structs/particle.cpp:698-995) per sphere, and
+ * ParticlesSoA::updateParticlesAsSoA (particle.cpp:5-62).  Call before vlbm_step. */
+vlbm_status vlbm_add_spheres(vlbm_sim* sim, const vlbm_ibm_config* ibm,
+                             const vlbm_sphere* spheres, int32_t n);
+vlbm_status vlbm_get_particles(vlbm_sim* sim, vlbm_particle_state* out, int32_t n);
+/* Lagrangian node positions [3][n_nodes] doubles and forces [3][n_nodes]. */
+vlbm_status vlbm_get_lagrangian_nodes(vlbm_sim* sim, double* pos, double* force, size_t n_nodes);
+
+/* ------------------------------------------------------------ outputs --- */
+/* Write PATH/ID/ID_<var><step>.bin files (lbmReport.cpp:55-172) for rho, ux, uy,
+ * uz [, fx, fy, fz when export_forces and spheres exist] [, omega when non-Newtonian]. */
+vlbm_status vlbm_write_macr_bin(vlbm_sim* sim, const char* path_files, const char* id_sim,
+                                uint32_t step_label, int32_t export_forces);
+
+/* ------------------------------------------------------------ serving --- */
+typedef struct vlbm_server vlbm_server;
+typedef struct vlbm_request {
+    vlbm_config cfg;
+    int32_t builder;             /* VLBM_BUILDER_*                                */
+    uint32_t steps;              /* steps to run before completion                */
+    uint64_t tag;                /* caller's id, returned in the completion      */
+    int32_t n_spheres;
+    const vlbm_sphere* spheres;  /* copied at submit                              */
+    vlbm_ibm_config ibm;
+} vlbm_request;
+typedef struct vlbm_completion {
+    uint64_t tag;
+    vlbm_status status;
+    double submit_time_s, start_time_s, finish_time_s; /* server clock, seconds   */
+    double mean_ux;              /* volume-averaged ux of the final state         */
+    uint64_t steps;
+} vlbm_completion;
+
+/* A continuous-batching server on one GPU: requests are admitted by HBM budget,
+ * stay resident, advance together in one batched launch per step, and retire at
+ * their step count.  The reference has no counterpart (one compile-time
+ * simulation per process). */
+vlbm_status vlbm_server_create(int device, size_t hbm_budget_bytes, int32_t max_resident,
+                               vlbm_server** out);
+vlbm_status vlbm_server_submit(vlbm_server* srv, const vlbm_request* req);
+/* Advance every resident simulation by up to `steps` steps, admitting queued work
+ * as memory frees up; returns the number of completions copied to `out`. */
+vlbm_status vlbm_server_pump(vlbm_server* srv, uint32_t steps, vlbm_completion* out,
+                             int32_t max_out, int32_t* n_out);
+vlbm_status vlbm_server_stats(vlbm_server* srv, int32_t* resident, int32_t* queued,
+                              int64_t* bytes_in_use, double* lattice_updates);
+/* Copy the macroscopics of the finished request `tag` (kept until fetched). */
+vlbm_status vlbm_server_fetch(vlbm_server* srv, uint64_t tag, float* ux, size_t n);
+vlbm_status vlbm_server_destroy(vlbm_server* srv);
+
+/* --------------------------------------------------------------- misc --- */
+const char* vlbm_last_error(void);     /* thread-local message of the last failure */
+int vlbm_abi_version(void);
+/* Autotuner: time the fused kernel variants for this simulation and keep the best. */
+vlbm_status vlbm_autotune(vlbm_sim* sim, int32_t* chosen_variant);
+/* Force a kernel launch variant (0 = autotuned default). */
+vlbm_status vlbm_set_variant(vlbm_sim* sim, int32_t variant);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VLBM_H */

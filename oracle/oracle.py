@@ -1,0 +1,245 @@
+"""ctypes binding of the FP64 oracle (oracle/oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py, always as the checker, never as the product.
+
+Also holds a literal restatement of the reference builders' if-chains
+(src/CUDA/boundaryConditionsBuilders/*.cu) used to check libvlbm's builders.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile (g++, OpenMP)."""
+    r = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB_PATH
+
+
+def _load():
+    srcs = [os.path.join(HERE, f) for f in os.listdir(HERE) if f.endswith(".cpp")]
+    if not os.path.exists(LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in srcs):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.oracle_create.restype = P
+    lib.oracle_create.argtypes = [P, C.POINTER(C.c_uint32)]
+    lib.oracle_destroy.argtypes = [P]
+    lib.oracle_set_threads.argtypes = [C.c_int]
+    lib.oracle_step.argtypes = [P, C.c_int]
+    lib.oracle_macro.argtypes = [P, D, D, D, D, D]
+    lib.oracle_get_pops.argtypes = [P, D]
+    lib.oracle_set_pops.argtypes = [P, D]
+    lib.oracle_set_omega.argtypes = [P, D]
+    lib.oracle_step_count.restype = C.c_longlong
+    lib.oracle_step_count.argtypes = [P]
+    lib.oracle_bb_role.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.oracle_bb_role.restype = C.c_int
+    lib.oracle_free_slip_source.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]
+    lib.oracle_free_slip_source.restype = C.c_int
+    lib.oracle_lattice.argtypes = [C.c_int, C.POINTER(C.c_int)]
+    lib.oracle_weight.argtypes = [C.c_int, C.c_int]
+    lib.oracle_weight.restype = C.c_double
+    if hasattr(lib, "oracle_ibm_create"):
+        _bind_ibm(lib)
+    return lib
+
+
+def _bind_ibm(lib):
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.oracle_ibm_create.restype = P
+    lib.oracle_ibm_create.argtypes = [P, C.POINTER(C.c_uint32), P, P, C.c_int]
+    lib.oracle_ibm_step.argtypes = [P, C.c_int]
+    lib.oracle_ibm_macro.argtypes = [P, D, D, D, D]
+    lib.oracle_ibm_particles.argtypes = [P, D, C.c_int]
+    lib.oracle_ibm_particles.restype = C.c_int
+    lib.oracle_ibm_nodes.argtypes = [P, D, C.c_int]
+    lib.oracle_ibm_nodes.restype = C.c_int
+    lib.oracle_ibm_destroy.argtypes = [P]
+    lib.oracle_sphere_mesh.argtypes = [C.c_double, C.c_double, D, D, C.c_int]
+    lib.oracle_sphere_mesh.restype = C.c_int
+
+
+_lib = _load()
+
+
+def lib():
+    return _lib
+
+
+def set_threads(n):
+    _lib.oracle_set_threads(int(n))
+
+
+def bb_role(q, direction, i):
+    return _lib.oracle_bb_role(q, direction, i)
+
+
+def velocities(q):
+    """The oracle's population ordering, [(cx, cy, cz)] for i < q."""
+    out = []
+    for i in range(q):
+        c = (C.c_int * 3)()
+        _lib.oracle_lattice(i, c)
+        out.append((c[0], c[1], c[2]))
+    return out
+
+
+def weight(q, i):
+    return _lib.oracle_weight(q, i)
+
+
+def free_slip_source(q, direction, i):
+    off = (C.c_int * 3)()
+    j = _lib.oracle_free_slip_source(q, direction, i, off)
+    return j, [off[0], off[1], off[2]]
+
+
+class Oracle:
+    """One lattice advanced by the FP64 restatement (reference push/AB scheme)."""
+
+    def __init__(self, cfg, node_map):
+        self.cfg = cfg
+        self.q = cfg.vel_set
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        self.n = cfg.nx * cfg.ny * cfg.nz
+        m = np.ascontiguousarray(node_map, dtype=np.uint32).ravel()
+        assert m.size == self.n
+        self._h = _lib.oracle_create(C.byref(cfg), m.ctypes.data_as(C.POINTER(C.c_uint32)))
+
+    def close(self):
+        if self._h:
+            _lib.oracle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        _lib.oracle_step(self._h, int(n))
+
+    def macroscopics(self):
+        out = [np.empty(self.n) for _ in range(5)]
+        ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in out]
+        _lib.oracle_macro(self._h, *ptr)
+        return {k: v.reshape(self.shape) for k, v in zip(("rho", "ux", "uy", "uz", "omega"), out)}
+
+    def populations(self):
+        out = np.empty(self.q * self.n)
+        _lib.oracle_get_pops(self._h, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out.reshape((self.q,) + self.shape)
+
+    def set_populations(self, pops):
+        a = np.ascontiguousarray(pops, dtype=np.float64).ravel()
+        _lib.oracle_set_pops(self._h, a.ctypes.data_as(C.POINTER(C.c_double)))
+
+
+# --------------------------------------------------------------------------
+# Literal restatement of the reference builders (node-map words).
+# Bit layout src/CUDA/structs/nodeTypeMap.h:15-133.
+USED = 1 << 21
+SCHEME_OFF, DIR_OFF, UX_OFF, UY_OFF, UZ_OFF = 18, 13, 9, 6, 3
+BB, VELBB, VELZH, FREESLIP = 5, 2, 1, 4
+(N_, S_, W_, E_, F_, B_, NW, NE, NF, NB, SW, SE, SF, SB, WF, WB, EF, EB,
+ NWF, NWB, NEF, NEB, SWF, SWB, SEF, SEB) = range(26)
+
+
+def _w(scheme, d, ux=0, uz=0):
+    return USED | (scheme << SCHEME_OFF) | (d << DIR_OFF) | (ux << UX_OFF) | (uz << UZ_OFF)
+
+
+def reference_builder_map(name, nx, ny, nz):
+    """Node map as the named reference builder writes it ([nz][ny][nx] uint32)."""
+    out = np.full((nz, ny, nx), USED, dtype=np.uint32)
+    for z in range(nz):
+        for y in range(ny):
+            for x in range(nx):
+                out[z, y, x] = _builder_word(name, x, y, z, nx, ny, nz)
+    return out.ravel()
+
+
+def _builder_word(name, x, y, z, NX, NY, NZ):
+    w = USED
+    if name == "periodic":
+        return w
+    if name == "plates_y":  # parallelPlatesBounceBack_Y.cu
+        if y == 0:
+            return _w(BB, S_)
+        if y == NY - 1:
+            return _w(BB, N_)
+        return w
+    if name == "plates_y_free_slip":  # parallelPlatesBounceBackFreeSlip.cu
+        if y == 0:
+            return _w(BB, S_)
+        if y == NY - 1:
+            return _w(FREESLIP, N_)
+        return w
+    if name == "plates_y_zouhe":  # couetteZouHe.cu
+        if y == 0:
+            return _w(VELZH, S_, uz=2)
+        if y == NY - 1:
+            return _w(VELZH, N_, uz=1)
+        return w
+    if name in ("lid_driven", "square_duct"):  # lidDrivenBounceBack.cu / squareDuctBounceBack.cu
+        lid = name == "lid_driven"
+        top = (lambda: _w(VELBB, N_, ux=1)) if lid else (lambda: _w(BB, N_))
+        if y == 0 and x == 0:
+            return _w(BB, SW)
+        if y == 0 and x == NX - 1:
+            return _w(BB, SE)
+        if y == NY - 1 and x == 0:
+            return _w(BB, NW)
+        if y == NY - 1 and x == NX - 1:
+            return _w(BB, NE)
+        if y == 0:
+            return _w(BB, S_)
+        if y == NY - 1:
+            return top()
+        if x == 0:
+            return _w(BB, W_)
+        if x == NX - 1:
+            return _w(BB, E_)
+        return w
+    if name in ("closed_box", "lid_cavity_closed"):  # closedBoxBounceBack.cu:56-208
+        chain = [
+            (y == 0 and x == 0 and z == 0, SWB), (y == 0 and x == 0 and z == NZ - 1, SWF),
+            (y == 0 and x == NX - 1 and z == 0, SEB), (y == 0 and x == NX - 1 and z == NZ - 1, SEF),
+            (y == NY - 1 and x == 0 and z == 0, NWB), (y == NY - 1 and x == 0 and z == NZ - 1, NWF),
+            (y == NY - 1 and x == NX - 1 and z == 0, NEB), (y == NY - 1 and x == NX - 1 and z == NZ - 1, NEF),
+            (y == 0 and x == 0, SW), (y == 0 and x == NX - 1, SE), (y == NY - 1 and x == 0, NW),
+            (y == NY - 1 and x == NX - 1, NE), (y == 0 and z == 0, SB), (y == 0 and z == NZ - 1, SF),
+            (y == NY - 1 and z == 0, NB), (y == NY - 1 and z == NZ - 1, NF), (x == 0 and z == 0, WB),
+            (x == 0 and z == NZ - 1, WF), (x == NX - 1 and z == 0, EB), (x == NX - 1 and z == NZ - 1, EF),
+            (y == 0, S_), (y == NY - 1, N_), (x == 0, W_), (x == NX - 1, E_), (z == 0, B_), (z == NZ - 1, F_)]
+        for cond, d in chain:
+            if cond:
+                if name == "lid_cavity_closed" and d == N_:
+                    return _w(VELBB, N_, ux=1)
+                return _w(BB, d)
+        return w
+    if name == "duct_yz":  # walls on y and z faces, periodic x
+        chain = [(y == 0 and z == 0, SB), (y == 0 and z == NZ - 1, SF), (y == NY - 1 and z == 0, NB),
+                 (y == NY - 1 and z == NZ - 1, NF), (y == 0, S_), (y == NY - 1, N_), (z == 0, B_),
+                 (z == NZ - 1, F_)]
+        for cond, d in chain:
+            if cond:
+                return _w(BB, d)
+        return w
+    raise KeyError(name)
+
+
+BUILDER_NAMES = {0: "periodic", 1: "plates_y", 2: "lid_driven", 3: "closed_box", 4: "square_duct",
+                 5: "duct_yz", 6: "lid_cavity_closed", 7: "plates_y_free_slip", 8: "plates_y_zouhe"}

@@ -1,0 +1,174 @@
+"""CUDA fused step (through the C ABI) against the FP64 oracle, same seeded inputs.
+
+Tolerances (FP32 arithmetic and storage vs FP64, after <= 100 steps):
+  populations  max |f_gpu - f_oracle|            <= 2e-6
+  density      max |rho_gpu - rho_oracle|         <= 2e-6
+  velocity     relative L2 ||u_gpu - u_or||/||u_or|| <= 1e-3  (flows with |u| >~ 1e-3)
+               and max abs error                  <= 2e-6
+  omega        max abs (non-Newtonian)            <= 1e-4 * omega_p
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+POP_TOL = 2e-6
+U_ABS_TOL = 2e-6
+U_REL_TOL = 1e-3
+
+# (name, Q, op, rheology, builder, (nx, ny, nz), steps, extra config)
+CASES = [
+    ("poiseuille_bgk_q19", 19, 1, 0, 1, (16, 12, 6), 100, dict(tau=0.9, fx=1e-4)),
+    ("plates_reg_q19_odd", 19, 0, 0, 1, (12, 10, 4), 37, dict(tau=0.7, fx=2e-4, fz=-5e-5)),
+    ("bingham_reg_q19", 19, 0, 1, 1, (16, 16, 4), 80, dict(fx=5e-4, eta_p=0.1, yield_stress=2e-6)),
+    ("bingham_bgk_q27", 27, 1, 1, 5, (10, 12, 12), 60, dict(fx=5e-4, eta_p=0.1, yield_stress=1e-6)),
+    ("powerlaw_reg_q27_cavity", 27, 0, 2, 6, (12, 12, 12), 70,
+     dict(n_index=0.5, k_consistency=0.02, ux_bc=[0, 0.05])),
+    ("powerlaw_reg_q19_shear_thick", 19, 0, 2, 2, (12, 12, 6), 50,
+     dict(n_index=1.5, k_consistency=0.05, ux_bc=[0, 0.05])),
+    ("closed_box_bgk_q27", 27, 1, 0, 3, (9, 8, 7), 61, dict(tau=0.8, fx=1e-4, fy=-2e-4, fz=3e-4)),
+    ("closed_box_reg_q19", 19, 0, 0, 3, (9, 8, 7), 60, dict(tau=0.65, fx=1e-4, fy=-2e-4, fz=3e-4)),
+    ("lid_driven_q19", 19, 0, 0, 2, (12, 12, 4), 80, dict(tau=0.6, ux_bc=[0, 0.1])),
+    ("lid_cavity_q27", 27, 0, 0, 6, (10, 10, 10), 50, dict(tau=0.6, ux_bc=[0, 0.1])),
+    ("square_duct_q27", 27, 0, 0, 4, (8, 8, 10), 60, dict(tau=0.9, fz=2e-4)),
+    ("duct_yz_q19_bingham", 19, 0, 1, 5, (12, 9, 9), 60, dict(fx=3e-4, eta_p=0.2, yield_stress=1e-6)),
+    ("free_slip_q19", 19, 0, 0, 7, (10, 12, 6), 70, dict(tau=0.8, fx=2e-4)),
+    ("free_slip_q27", 27, 1, 0, 7, (10, 12, 6), 51, dict(tau=0.8, fx=2e-4)),
+    ("zouhe_couette_q19", 19, 0, 0, 8, (8, 12, 8), 60, dict(tau=0.8, uz_bc=[0, 0.02, -0.02])),
+]
+
+
+def run_pair(vlbm, oracle, Q, op, rheo, builder, size, steps, extra, storage=0):
+    nx, ny, nz = size
+    cfg = vlbm.Config.default(nx=nx, ny=ny, nz=nz, vel_set=Q, collision=op, rheology=rheo,
+                              storage=storage, **extra)
+    node_map = vlbm.build_node_map(builder, nx, ny, nz)
+    sim = vlbm.Simulation(cfg, node_map=node_map)
+    sim.step(steps)
+    sim.sync()
+    o = oracle.Oracle(cfg, node_map)
+    o.step(steps)
+    return cfg, sim, o
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_fused_step_matches_oracle(vlbm, oracle, case):
+    name, Q, op, rheo, builder, size, steps, extra = case
+    cfg, sim, o = run_pair(vlbm, oracle, Q, op, rheo, builder, size, steps, extra)
+    fg = sim.populations().astype(np.float64)
+    fo = o.populations()
+    assert np.max(np.abs(fg - fo)) <= POP_TOL, (name, np.max(np.abs(fg - fo)))
+    mg, mo = sim.macroscopics(), o.macroscopics()
+    assert np.max(np.abs(mg["rho"] - mo["rho"])) <= POP_TOL
+    ug = np.stack([mg["ux"], mg["uy"], mg["uz"]]).astype(np.float64)
+    uo = np.stack([mo["ux"], mo["uy"], mo["uz"]])
+    assert np.max(np.abs(ug - uo)) <= U_ABS_TOL, (name, np.max(np.abs(ug - uo)))
+    if np.abs(uo).max() > 1e-3:
+        assert rel_l2(ug, uo) <= U_REL_TOL, (name, rel_l2(ug, uo))
+    if rheo != 0:
+        om_p = 1.0 / (3 * cfg.eta_p + 0.5) if rheo == 1 else 2.0
+        assert np.max(np.abs(mg["omega"] - mo["omega"])) <= 1e-4 * om_p
+    assert sim.info().step == steps
+
+
+def test_even_and_odd_parity_agree_with_oracle_every_step(vlbm, oracle):
+    cfg = vlbm.Config.default(nx=8, ny=10, nz=5, vel_set=19, collision=0, rheology=1, fx=5e-4,
+                              eta_p=0.1, yield_stress=1e-6)
+    m = vlbm.build_node_map(vlbm.BUILDER_CLOSED_BOX, 8, 10, 5)
+    sim = vlbm.Simulation(cfg, node_map=m)
+    o = oracle.Oracle(cfg, m)
+    for k in range(1, 7):
+        sim.step(1)
+        o.step(1)
+        assert np.max(np.abs(sim.populations() - o.populations())) <= POP_TOL, k
+
+
+def test_set_populations_roundtrip_and_continue(vlbm, oracle):
+    cfg = vlbm.Config.default(nx=8, ny=8, nz=8, vel_set=27, tau=0.7, fx=1e-4)
+    m = vlbm.build_node_map(vlbm.BUILDER_LID_CAVITY_CLOSED, 8, 8, 8)
+    sim = vlbm.Simulation(cfg, node_map=m)
+    sim.step(11)
+    f = sim.populations()
+    sim2 = vlbm.Simulation(cfg, node_map=m)
+    sim2.set_populations(f)
+    np.testing.assert_array_equal(sim2.populations(), f)
+    o = oracle.Oracle(cfg, m)
+    o.set_populations(f.astype(np.float64))
+    sim2.step(9)
+    o.step(9)
+    assert np.max(np.abs(sim2.populations() - o.populations())) <= POP_TOL
+
+
+def test_reinit_equilibrium_resets_state(vlbm):
+    cfg = vlbm.Config.default(nx=6, ny=6, nz=6, fx=1e-3, rheology=2, n_index=0.7, k_consistency=0.03)
+    sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_CLOSED_BOX)
+    first = None
+    for _ in range(2):
+        sim.init_equilibrium(1.0, 0, 0, 0)
+        sim.step(5)
+        u = sim.macroscopics()["ux"].copy()
+        if first is None:
+            first = u
+    np.testing.assert_array_equal(first, u)
+
+
+def test_divergence_is_reported_not_hidden(vlbm):
+    cfg = vlbm.Config.default(nx=4, ny=4, nz=4)
+    sim = vlbm.Simulation(cfg)
+    f = sim.populations()
+    f[:, 1, 1, 1] = np.nan
+    sim.set_populations(f)
+    sim.step(1)
+    with pytest.raises(vlbm.VlbmError) as e:
+        sim.sync()
+    assert e.value.status == vlbm.ERR_DIVERGED
+    sim.sync()  # flag cleared after being reported
+
+
+def test_autotune_preserves_state(vlbm):
+    cfg = vlbm.Config.default(nx=32, ny=16, nz=8, fx=1e-4, tau=0.8)
+    a = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+    b = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+    a.step(3)
+    b.step(3)
+    v = b.autotune()
+    assert v in (1, 2, 3)
+    a.step(10)
+    b.step(10)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3])
+def test_launch_variants_bit_identical(vlbm, variant):
+    cfg = vlbm.Config.default(nx=20, ny=12, nz=6, vel_set=27, fx=1e-4, tau=0.8)
+    ref = vlbm.Simulation(cfg, builder=vlbm.BUILDER_DUCT_YZ)
+    ref.step(7)
+    s = vlbm.Simulation(cfg, builder=vlbm.BUILDER_DUCT_YZ)
+    s.set_variant(variant)
+    s.step(7)
+    np.testing.assert_array_equal(ref.populations(), s.populations())
+
+
+def test_poiseuille_gpu_against_analytic(vlbm):
+    ny, tau, g = 32, 0.9, 1e-6
+    cfg = vlbm.Config.default(nx=64, ny=ny, nz=32, tau=tau, fx=g, collision=vlbm.OP_BGK)
+    sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+    sim.step(10000)  # the BGK Poiseuille channel, 64x32x32, 10k steps
+    ux = sim.macroscopics()["ux"].mean(axis=(0, 2))
+    nu = (tau - 0.5) / 3
+    y = np.arange(ny)
+    ana = g / (2 * nu) * (y + 0.5) * (ny - 0.5 - y)
+    assert np.linalg.norm(ux - ana) / np.linalg.norm(ana) < 2e-2  # 10k steps: not fully developed
+
+
+@pytest.mark.parametrize("storage,tol", [(1, 2e-3), (2, 2e-2)])
+def test_half_precision_storage_close_to_fp64(vlbm, oracle, storage, tol):
+    cfg, sim, o = run_pair(vlbm, oracle, 19, 0, 1, 1, (16, 24, 4), 400,
+                           dict(fx=5e-5, eta_p=0.1, yield_stress=1e-6), storage=storage)
+    ug = sim.macroscopics()["ux"].astype(np.float64)
+    uo = o.macroscopics()["ux"]
+    assert rel_l2(ug, uo) < tol, rel_l2(ug, uo)

@@ -1,0 +1,497 @@
+// capi.cu -- C ABI of the fluid time step (include/vlbm.h).
+#include <cuda_runtime.h>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+#include "sim.h"
+#include "lattice.cuh"
+
+namespace vlbm {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+vlbm_status cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return VLBM_OK;
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? VLBM_ERR_NOMEM : VLBM_ERR_CUDA;
+}
+
+#define VLBM_CUDA(call)                                              \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return cuda_status(e_, #call);        \
+    } while (0)
+
+static float default_scale(int storage) { return storage == VLBM_STORE_F16 ? 4096.0f : 1.0f; }
+
+vlbm_status sim_validate_config(const vlbm_config& c, std::string& why) {
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1) { why = "lattice sizes must be >= 1"; return VLBM_ERR_INVALID; }
+    const long long N = (long long)c.nx * c.ny * c.nz;
+    if (N >= (1LL << 31)) { why = "lattice has 2^31 nodes or more"; return VLBM_ERR_INVALID; }
+    if (c.vel_set != 19 && c.vel_set != 27) { why = "vel_set must be 19 or 27"; return VLBM_ERR_INVALID; }
+    if (c.collision != VLBM_OP_REGULARIZED && c.collision != VLBM_OP_BGK) { why = "unknown collision operator"; return VLBM_ERR_INVALID; }
+    if (c.rheology < VLBM_NEWTONIAN || c.rheology > VLBM_POWERLAW) { why = "unknown rheology"; return VLBM_ERR_INVALID; }
+    if (c.storage < VLBM_STORE_F32 || c.storage > VLBM_STORE_BF16) { why = "unknown storage"; return VLBM_ERR_INVALID; }
+    if (c.rheology == VLBM_NEWTONIAN && !(c.tau > 0.5)) { why = "tau must be > 0.5"; return VLBM_ERR_INVALID; }
+    if (c.rheology == VLBM_BINGHAM && !(c.eta_p > 0.0 && c.yield_stress >= 0.0)) { why = "Bingham needs eta_p > 0, yield_stress >= 0"; return VLBM_ERR_INVALID; }
+    if (c.rheology == VLBM_POWERLAW && !(c.n_index > 0.0 && c.k_consistency > 0.0)) { why = "Power-Law needs n_index > 0, k_consistency > 0"; return VLBM_ERR_INVALID; }
+    if (!(c.rho0 > 0.0)) { why = "rho0 must be > 0"; return VLBM_ERR_INVALID; }
+    return VLBM_OK;
+}
+
+StepParams make_params(vlbm_sim* s) {
+    StepParams p;
+    std::memset(&p, 0, sizeof(p));
+    const vlbm_config& c = s->cfg;
+    p.pop = s->pop;
+    p.cls = s->cls;
+    p.bc_slot = s->bc_slot;
+    p.bc = s->bc;
+    p.side_prev = s->side[s->side_cur];
+    p.side_next = s->side[s->side_cur ^ 1];
+    p.omega = s->omega;
+    p.fibm = s->fibm;
+    p.err = s->err;
+    p.nx = c.nx; p.ny = c.ny; p.nz = c.nz;
+    p.N = s->N;
+    p.nbc = s->nbc;
+    p.apply_bc = s->apply_bc;
+    p.omega_newt = (float)(1.0 / c.tau);                 // var.h:105 OMEGA
+    p.fx = (float)c.fx; p.fy = (float)c.fy; p.fz = (float)c.fz;
+    p.omega_p = (float)(1.0 / (3.0 * c.eta_p + 0.5));    // nnf.h:128 OMEGA_P
+    p.yield = (float)c.yield_stress;
+    p.n_index = (float)c.n_index;
+    p.k_cons = (float)c.k_consistency;
+    p.gamma0 = (float)c.gamma0;
+    const float sc = c.storage_scale > 0 ? (float)c.storage_scale : default_scale(c.storage);
+    p.scale = sc;
+    p.inv_scale = 1.0f / sc;
+    p.rho0 = (float)c.rho0;
+    return p;
+}
+
+vlbm_status fluid_step(vlbm_sim* s) {
+    StepParams p = make_params(s);
+    LaunchShape ls{s->block};
+    cudaError_t e = launch_step(s->Q, s->cfg.storage, p, s->cfg.collision, s->cfg.rheology, s->parity == 1, ls,
+                                s->stream);
+    if (e != cudaSuccess) return cuda_status(e, "fused step launch");
+    s->parity ^= 1;
+    s->side_cur ^= 1;
+    s->apply_bc = 1;
+    s->step += 1;
+    return VLBM_OK;
+}
+
+static vlbm_status alloc_dev(vlbm_sim* s, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc");
+    s->device_bytes += bytes;
+    return VLBM_OK;
+}
+
+static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
+    if (s->nbc == 0) return VLBM_OK;
+    std::vector<float> h((size_t)s->Q * s->nbc);
+    for (int i = 0; i < s->Q; ++i) {
+        float v = (float)(lattice_weight(s->Q, i) * s->cfg.rho0);
+        for (int k = 0; k < s->nbc; ++k) h[(size_t)i * s->nbc + k] = v;
+    }
+    for (int b = 0; b < 2; ++b)
+        VLBM_CUDA(cudaMemcpyAsync(s->side[b], h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    return VLBM_OK;
+}
+
+vlbm_status sim_macroscopics_device(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz, float* omega) {
+    MacroParams mp;
+    std::memset(&mp, 0, sizeof(mp));
+    mp.s = make_params(s);
+    mp.rho = rho; mp.ux = ux; mp.uy = uy; mp.uz = uz; mp.omega_out = omega;
+    mp.fibm_const = nullptr;
+    cudaError_t e = launch_macro(s->Q, s->cfg.storage, mp, s->cfg.rheology, s->parity == 1, s->stream);
+    if (e != cudaSuccess) return cuda_status(e, "macroscopics launch");
+    if (s->ibm) return ibm_macroscopics_fixup(s, rho, ux, uy, uz);
+    return VLBM_OK;
+}
+
+static vlbm_status ensure_scratch(vlbm_sim* s) {
+    if (s->scratch) return VLBM_OK;
+    void* p = nullptr;
+    vlbm_status st = alloc_dev(s, &p, (size_t)5 * s->N * sizeof(float));
+    if (st != VLBM_OK) return st;
+    s->scratch = static_cast<float*>(p);
+    return VLBM_OK;
+}
+
+}  // namespace vlbm
+
+using namespace vlbm;
+
+vlbm_sim::~vlbm_sim() {
+    if (ibm) { ibm_destroy(ibm); ibm = nullptr; }
+    cudaFree(pop); cudaFree(cls); cudaFree(bc_slot); cudaFree(bc);
+    cudaFree(side[0]); cudaFree(side[1]); cudaFree(omega); cudaFree(fibm); cudaFree(err); cudaFree(scratch);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+#define CHECK_SIM(s)                                                        \
+    do {                                                                    \
+        if (!(s)) { set_last_error("null simulation handle"); return VLBM_ERR_INVALID; } \
+        cudaError_t e_ = cudaSetDevice((s)->device);                        \
+        if (e_ != cudaSuccess) return cuda_status(e_, "cudaSetDevice");     \
+    } while (0)
+
+extern "C" {
+
+int vlbm_abi_version(void) { return VLBM_ABI_VERSION; }
+const char* vlbm_last_error(void) { return g_last_error.c_str(); }
+
+vlbm_status vlbm_config_default(vlbm_config* c) {
+    if (!c) return VLBM_ERR_INVALID;
+    std::memset(c, 0, sizeof(*c));
+    c->nx = c->ny = 128; c->nz = 384;      // var.h:95-100 (N=128, NZ=3N)
+    c->vel_set = VLBM_D3Q19;               // var.h:19
+    c->collision = VLBM_OP_REGULARIZED;    // lbm.cu:263-461
+    c->rheology = VLBM_NEWTONIAN;
+    c->storage = VLBM_STORE_F32;           // var.h:18 SINGLE_PRECISION
+    c->device = 0;
+    c->tau = 0.6;                          // var.h:104
+    c->rho0 = 1.0;                         // var.h:107
+    c->eta_p = 0.3;                        // nnf.h:125
+    c->yield_stress = 1e-4;                // nnf.h:126
+    c->n_index = 0.5;                      // nnf.h:116
+    c->k_consistency = c->rho0 * (c->tau - 0.5) / 3.0;  // nnf.h:117
+    c->gamma0 = 0.0;                       // nnf.h:118
+    const double umax = 0.1;               // var.h:102 U_MAX
+    const double ux[8] = {0, umax, 0, 0, 0, 0, 0, 0};            // var.h:114
+    const double uy[8] = {0, umax / 2, -umax / 2, 0, 0, 0, 0, 0}; // var.h:115
+    const double uz[8] = {0, umax, -umax, 0, 0, 0, 0, 0};        // var.h:116
+    const double rb[8] = {1, 1, 1, 1, 1, 1, 1, 1};               // var.h:117 (RHO_0 first)
+    for (int i = 0; i < 8; ++i) { c->ux_bc[i] = ux[i]; c->uy_bc[i] = uy[i]; c->uz_bc[i] = uz[i]; c->rho_bc[i] = rb[i]; }
+    c->storage_scale = 0.0;
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) {
+    if (!cfg || !out) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    *out = nullptr;
+    std::string why;
+    vlbm_status st = sim_validate_config(*cfg, why);
+    if (st != VLBM_OK) { set_last_error(why); return st; }
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
+    vlbm_sim* s = new vlbm_sim();
+    s->cfg = *cfg;
+    s->Q = cfg->vel_set;
+    s->N = (long long)cfg->nx * cfg->ny * cfg->nz;
+    s->store_bytes = cfg->storage == VLBM_STORE_F32 ? 4 : 2;
+    s->device = cfg->device;
+    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete s; return cuda_status(e, "cudaStreamCreate"); }
+    s->own_stream = true;
+    const size_t N = (size_t)s->N;
+    void* p;
+    if ((st = alloc_dev(s, &p, (size_t)s->Q * N * s->store_bytes)) != VLBM_OK) { delete s; return st; }
+    s->pop = p;
+    if ((st = alloc_dev(s, &p, N)) != VLBM_OK) { delete s; return st; }
+    s->cls = static_cast<uint8_t*>(p);
+    if ((st = alloc_dev(s, &p, N * sizeof(int32_t))) != VLBM_OK) { delete s; return st; }
+    s->bc_slot = static_cast<int32_t*>(p);
+    if ((st = alloc_dev(s, &p, sizeof(unsigned int))) != VLBM_OK) { delete s; return st; }
+    s->err = static_cast<unsigned int*>(p);
+    if (cfg->rheology == VLBM_POWERLAW) {
+        if ((st = alloc_dev(s, &p, N * sizeof(float))) != VLBM_OK) { delete s; return st; }
+        s->omega = static_cast<float*>(p);
+    }
+    cudaMemsetAsync(s->cls, 0, N, s->stream);
+    cudaMemsetAsync(s->bc_slot, 0xff, N * sizeof(int32_t), s->stream);
+    cudaMemsetAsync(s->err, 0, sizeof(unsigned int), s->stream);
+    st = vlbm_init_equilibrium(s, cfg->rho0, 0.0, 0.0, 0.0);
+    if (st != VLBM_OK) { delete s; return st; }
+    *out = s;
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_destroy(vlbm_sim* s) {
+    if (!s) return VLBM_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_set_node_map(vlbm_sim* s, const uint32_t* map, size_t n) {
+    CHECK_SIM(s);
+    if (!map) { set_last_error("null node map"); return VLBM_ERR_INVALID; }
+    std::string why;
+    BcTables t;
+    vlbm_status st = build_bc_tables(s->cfg, map, n, t, why);
+    if (st != VLBM_OK) { set_last_error(why); return st; }
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    cudaFree(s->bc); cudaFree(s->side[0]); cudaFree(s->side[1]);
+    s->bc = nullptr; s->side[0] = s->side[1] = nullptr;
+    s->nbc = (int)t.recs.size();
+    VLBM_CUDA(cudaMemcpy(s->cls, t.cls.data(), t.cls.size(), cudaMemcpyHostToDevice));
+    VLBM_CUDA(cudaMemcpy(s->bc_slot, t.slot.data(), t.slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    if (s->nbc > 0) {
+        void* p;
+        if ((st = alloc_dev(s, &p, t.recs.size() * sizeof(BcRec))) != VLBM_OK) return st;
+        s->bc = static_cast<BcRec*>(p);
+        VLBM_CUDA(cudaMemcpy(s->bc, t.recs.data(), t.recs.size() * sizeof(BcRec), cudaMemcpyHostToDevice));
+        for (int b = 0; b < 2; ++b) {
+            if ((st = alloc_dev(s, &p, (size_t)s->Q * s->nbc * sizeof(float))) != VLBM_OK) return st;
+            s->side[b] = static_cast<float*>(p);
+        }
+        if ((st = fill_side_equilibrium(s)) != VLBM_OK) return st;
+    }
+    s->host_map.assign(map, map + n);
+    s->tables = std::move(t);
+    s->geometry = true;
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_init_equilibrium(vlbm_sim* s, double rho, double ux, double uy, double uz) {
+    CHECK_SIM(s);
+    StepParams p = make_params(s);
+    VLBM_CUDA(launch_set_pops(s->Q, s->cfg.storage, p, nullptr, (float)rho, (float)ux, (float)uy, (float)uz,
+                              s->stream));
+    s->parity = 0;
+    s->apply_bc = 0;     // the initial state carries no boundary rule (main.cu:204-213)
+    s->step = 0;
+    if (s->fibm) VLBM_CUDA(cudaMemsetAsync(s->fibm, 0, (size_t)3 * s->N * sizeof(float), s->stream));
+    if (s->nbc > 0) { vlbm_status st = fill_side_equilibrium(s); if (st != VLBM_OK) return st; }
+    if (s->ibm) ibm_reset(s);
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_step(vlbm_sim* s, uint32_t nsteps) {
+    CHECK_SIM(s);
+    if (!s->geometry) { set_last_error("vlbm_set_node_map must be called before vlbm_step"); return VLBM_ERR_STATE; }
+    for (uint32_t k = 0; k < nsteps; ++k) {
+        vlbm_status st = fluid_step(s);
+        if (st != VLBM_OK) return st;
+        if (s->ibm) {
+            st = ibm_step(s);
+            if (st != VLBM_OK) return st;
+        }
+    }
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_sync(vlbm_sim* s) {
+    CHECK_SIM(s);
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    unsigned int h = 0;
+    VLBM_CUDA(cudaMemcpy(&h, s->err, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h) {
+        VLBM_CUDA(cudaMemset(s->err, 0, sizeof(unsigned int)));
+        set_last_error("non-finite or non-positive density detected on the device");
+        return VLBM_ERR_DIVERGED;
+    }
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_set_stream(vlbm_sim* s, void* stream) {
+    CHECK_SIM(s);
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    if (stream) {
+        s->stream = static_cast<cudaStream_t>(stream);
+        s->own_stream = false;
+    } else {
+        VLBM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        s->own_stream = true;
+    }
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_get_macroscopics_device(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz, float* omega) {
+    CHECK_SIM(s);
+    return sim_macroscopics_device(s, rho, ux, uy, uz, omega);
+}
+
+vlbm_status vlbm_get_macroscopics(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz, float* omega) {
+    CHECK_SIM(s);
+    vlbm_status st = ensure_scratch(s);
+    if (st != VLBM_OK) return st;
+    const size_t N = (size_t)s->N;
+    float* d[5] = {s->scratch, s->scratch + N, s->scratch + 2 * N, s->scratch + 3 * N, s->scratch + 4 * N};
+    st = sim_macroscopics_device(s, d[0], d[1], d[2], d[3], d[4]);
+    if (st != VLBM_OK) return st;
+    float* h[5] = {rho, ux, uy, uz, omega};
+    for (int k = 0; k < 5; ++k)
+        if (h[k]) VLBM_CUDA(cudaMemcpyAsync(h[k], d[k], N * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_get_populations(vlbm_sim* s, float* pops, size_t n) {
+    CHECK_SIM(s);
+    if (!pops || n != (size_t)s->Q * s->N) { set_last_error("population buffer size must be Q*N"); return VLBM_ERR_INVALID; }
+    void* d = nullptr;
+    VLBM_CUDA(cudaMallocAsync(&d, n * sizeof(float), s->stream));
+    StepParams p = make_params(s);
+    cudaError_t e = launch_get_pops(s->Q, s->cfg.storage, p, s->parity == 1, static_cast<float*>(d), s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pops, d, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(d, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return cuda_status(e, "vlbm_get_populations");
+}
+
+vlbm_status vlbm_set_populations(vlbm_sim* s, const float* pops, size_t n) {
+    CHECK_SIM(s);
+    if (!pops || n != (size_t)s->Q * s->N) { set_last_error("population buffer size must be Q*N"); return VLBM_ERR_INVALID; }
+    void* d = nullptr;
+    VLBM_CUDA(cudaMallocAsync(&d, n * sizeof(float), s->stream));
+    cudaError_t e = cudaMemcpyAsync(d, pops, n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+    StepParams p = make_params(s);
+    p.omega = nullptr;  // keep the omega state
+    if (e == cudaSuccess) e = launch_set_pops(s->Q, s->cfg.storage, p, static_cast<const float*>(d), 0.f, 0.f, 0.f, 0.f, s->stream);
+    cudaFreeAsync(d, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    s->parity = 0;
+    s->apply_bc = 0;   // given populations already carry their boundary values
+    return cuda_status(e, "vlbm_set_populations");
+}
+
+vlbm_status vlbm_get_forces(vlbm_sim* s, float* fxyz, size_t n) {
+    CHECK_SIM(s);
+    if (!fxyz || n != (size_t)3 * s->N) { set_last_error("force buffer size must be 3*N"); return VLBM_ERR_INVALID; }
+    const size_t N = (size_t)s->N;
+    if (!s->fibm) {
+        for (size_t k = 0; k < N; ++k) { fxyz[k] = (float)s->cfg.fx; fxyz[N + k] = (float)s->cfg.fy; fxyz[2 * N + k] = (float)s->cfg.fz; }
+        return VLBM_OK;
+    }
+    VLBM_CUDA(cudaMemcpyAsync(fxyz, s->fibm, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    const float b[3] = {(float)s->cfg.fx, (float)s->cfg.fy, (float)s->cfg.fz};
+    for (int a = 0; a < 3; ++a)
+        for (size_t k = 0; k < N; ++k) fxyz[a * N + k] += b[a];
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_get_info(vlbm_sim* s, vlbm_info* info) {
+    if (!s || !info) return VLBM_ERR_INVALID;
+    std::memset(info, 0, sizeof(*info));
+    info->nx = s->cfg.nx; info->ny = s->cfg.ny; info->nz = s->cfg.nz; info->q = s->Q;
+    info->storage_bytes = s->store_bytes;
+    info->step = s->step;
+    info->n_bc_nodes = s->nbc;
+    info->device_bytes = (int64_t)s->device_bytes;
+    info->bytes_per_node_step = 2.0 * s->Q * s->store_bytes;
+    info->last_kernel_variant = s->variant;
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_set_variant(vlbm_sim* s, int32_t variant) {
+    if (!s) return VLBM_ERR_INVALID;
+    static const int blocks[] = {256, 64, 128, 256};
+    if (variant < 0 || variant > 3) { set_last_error("unknown launch variant"); return VLBM_ERR_INVALID; }
+    s->variant = variant;
+    s->block = blocks[variant];
+    return VLBM_OK;
+}
+
+// Project-written autotuner: times each launch variant over whole even/odd step
+// pairs on a copy of the state, then restores the state and keeps the fastest.
+vlbm_status vlbm_autotune(vlbm_sim* s, int32_t* chosen) {
+    CHECK_SIM(s);
+    if (!s->geometry) { set_last_error("set the node map before autotuning"); return VLBM_ERR_STATE; }
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    const size_t popb = (size_t)s->Q * s->N * s->store_bytes;
+    const size_t sideb = (size_t)s->Q * s->nbc * sizeof(float);
+    void *bp = nullptr, *bs0 = nullptr, *bs1 = nullptr, *bo = nullptr;
+    VLBM_CUDA(cudaMalloc(&bp, popb));
+    if (sideb) { VLBM_CUDA(cudaMalloc(&bs0, sideb)); VLBM_CUDA(cudaMalloc(&bs1, sideb)); }
+    if (s->omega) VLBM_CUDA(cudaMalloc(&bo, (size_t)s->N * sizeof(float)));
+    VLBM_CUDA(cudaMemcpy(bp, s->pop, popb, cudaMemcpyDeviceToDevice));
+    if (sideb) { VLBM_CUDA(cudaMemcpy(bs0, s->side[0], sideb, cudaMemcpyDeviceToDevice));
+                 VLBM_CUDA(cudaMemcpy(bs1, s->side[1], sideb, cudaMemcpyDeviceToDevice)); }
+    if (bo) VLBM_CUDA(cudaMemcpy(bo, s->omega, (size_t)s->N * sizeof(float), cudaMemcpyDeviceToDevice));
+    const int parity = s->parity, side_cur = s->side_cur, apply = s->apply_bc;
+    const long long step = s->step;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    float best = 1e30f;
+    int bestv = 3;
+    const int reps = s->N > (1 << 22) ? 4 : 20;
+    for (int v = 1; v <= 3; ++v) {
+        vlbm_set_variant(s, v);
+        for (int w = 0; w < 2; ++w) fluid_step(s);
+        cudaEventRecord(e0, s->stream);
+        for (int r = 0; r < reps; ++r) fluid_step(s);
+        cudaEventRecord(e1, s->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; bestv = v; }
+    }
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    VLBM_CUDA(cudaMemcpy(s->pop, bp, popb, cudaMemcpyDeviceToDevice));
+    if (sideb) { VLBM_CUDA(cudaMemcpy(s->side[0], bs0, sideb, cudaMemcpyDeviceToDevice));
+                 VLBM_CUDA(cudaMemcpy(s->side[1], bs1, sideb, cudaMemcpyDeviceToDevice)); }
+    if (bo) VLBM_CUDA(cudaMemcpy(s->omega, bo, (size_t)s->N * sizeof(float), cudaMemcpyDeviceToDevice));
+    cudaFree(bp); cudaFree(bs0); cudaFree(bs1); cudaFree(bo);
+    s->parity = parity; s->side_cur = side_cur; s->apply_bc = apply; s->step = step;
+    vlbm_set_variant(s, bestv);
+    if (chosen) *chosen = bestv;
+    VLBM_CUDA(cudaGetLastError());
+    return VLBM_OK;
+}
+
+// lbmReport.cpp:55-83 file names: PATH/ID/ID_<var><step, 6 digits>.bin;
+// saveAllMacrBin lbmReport.cpp:133-172: raw little-endian floats [NZ][NY][NX].
+vlbm_status vlbm_write_macr_bin(vlbm_sim* s, const char* path_files, const char* id_sim, uint32_t step_label,
+                                int32_t export_forces) {
+    CHECK_SIM(s);
+    if (!path_files || !id_sim) { set_last_error("null path"); return VLBM_ERR_INVALID; }
+    const size_t N = (size_t)s->N;
+    std::vector<float> rho(N), ux(N), uy(N), uz(N), om(N);
+    bool nnf = s->cfg.rheology != VLBM_NEWTONIAN;
+    vlbm_status st = vlbm_get_macroscopics(s, rho.data(), ux.data(), uy.data(), uz.data(), nnf ? om.data() : nullptr);
+    if (st != VLBM_OK) return st;
+    std::string dir = std::string(path_files) + "/" + id_sim;
+    {   // mkdir -p (folderSetup, lbmReport.cpp:25-52)
+        std::string acc;
+        for (size_t k = 0; k <= dir.size(); ++k) {
+            if (k == dir.size() || dir[k] == '/') {
+                if (!acc.empty()) mkdir(acc.c_str(), 0777);
+            }
+            if (k < dir.size()) acc.push_back(dir[k]);
+        }
+    }
+    char num[32];
+    std::snprintf(num, sizeof(num), "%06u", step_label);
+    auto write = [&](const char* var, const float* data) -> vlbm_status {
+        std::string fn = dir + "/" + id_sim + "_" + var + num + ".bin";
+        FILE* f = std::fopen(fn.c_str(), "wb");
+        if (!f) { set_last_error("cannot open " + fn); return VLBM_ERR_IO; }
+        size_t w = std::fwrite(data, sizeof(float), N, f);
+        std::fclose(f);
+        if (w != N) { set_last_error("short write " + fn); return VLBM_ERR_IO; }
+        return VLBM_OK;
+    };
+    if ((st = write("rho", rho.data())) != VLBM_OK) return st;
+    if ((st = write("ux", ux.data())) != VLBM_OK) return st;
+    if ((st = write("uy", uy.data())) != VLBM_OK) return st;
+    if ((st = write("uz", uz.data())) != VLBM_OK) return st;
+    if (export_forces && s->ibm) {
+        std::vector<float> fr(3 * N);
+        if ((st = vlbm_get_forces(s, fr.data(), fr.size())) != VLBM_OK) return st;
+        if ((st = write("fx", fr.data())) != VLBM_OK) return st;
+        if ((st = write("fy", fr.data() + N)) != VLBM_OK) return st;
+        if ((st = write("fz", fr.data() + 2 * N)) != VLBM_OK) return st;
+    }
+    if (nnf && (st = write("omega", om.data())) != VLBM_OK) return st;
+    return VLBM_OK;
+}
+
+}  // extern "C"

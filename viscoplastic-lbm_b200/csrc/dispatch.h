@@ -1,0 +1,32 @@
+// dispatch.h -- host entry points into the templated kernels of step_impl.cuh.
+// Each (velocity set, storage) pair is instantiated in its own translation
+// unit (step_q<Q>_<storage>.cu); dispatch.cpp selects one at run time.
+#pragma once
+#include <cuda_runtime.h>
+#include "internal.h"
+
+namespace vlbm {
+
+struct LaunchShape {
+    int block;      // threads per block
+};
+
+template <int Q, int ST>
+cudaError_t launch_step_st(const StepParams& p, int op, int rheo, bool odd, LaunchShape ls, cudaStream_t s);
+template <int Q, int ST>
+cudaError_t launch_macro_st(const MacroParams& mp, int rheo, bool odd, cudaStream_t s);
+template <int Q, int ST>
+cudaError_t launch_get_pops_st(const StepParams& p, bool odd, float* out, cudaStream_t s);
+template <int Q, int ST>
+cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, float ux, float uy, float uz,
+                               cudaStream_t s);
+
+// Run-time selection over (Q, storage).
+cudaError_t launch_step(int Q, int st, const StepParams& p, int op, int rheo, bool odd, LaunchShape ls,
+                        cudaStream_t s);
+cudaError_t launch_macro(int Q, int st, const MacroParams& mp, int rheo, bool odd, cudaStream_t s);
+cudaError_t launch_get_pops(int Q, int st, const StepParams& p, bool odd, float* out, cudaStream_t s);
+cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in, float rho, float ux, float uy,
+                            float uz, cudaStream_t s);
+
+}  // namespace vlbm

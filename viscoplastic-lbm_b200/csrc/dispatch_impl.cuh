@@ -1,0 +1,80 @@
+// dispatch_impl.cuh -- template bodies of dispatch.h (included by step_q19.cu / step_q27.cu).
+#pragma once
+#include "dispatch.h"
+#include "step_impl.cuh"
+
+namespace vlbm {
+
+inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+template <int Q, int OP, int RHEO, int ST>
+cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s) {
+    const unsigned g = grid_for(p.N, ls.block);
+    if (odd) k_step<Q, OP, RHEO, ST, true><<<g, ls.block, 0, s>>>(p);
+    else k_step<Q, OP, RHEO, ST, false><<<g, ls.block, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+template <int Q, int OP, int ST>
+cudaError_t step_rh(const StepParams& p, int rheo, bool odd, LaunchShape ls, cudaStream_t s) {
+    switch (rheo) {
+    case VLBM_NEWTONIAN: return step_t<Q, OP, VLBM_NEWTONIAN, ST>(p, odd, ls, s);
+    case VLBM_BINGHAM: return step_t<Q, OP, VLBM_BINGHAM, ST>(p, odd, ls, s);
+    case VLBM_POWERLAW: return step_t<Q, OP, VLBM_POWERLAW, ST>(p, odd, ls, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int Q, int ST>
+cudaError_t launch_step_st(const StepParams& p, int op, int rheo, bool odd, LaunchShape ls, cudaStream_t s) {
+    if (op == VLBM_OP_BGK) return step_rh<Q, VLBM_OP_BGK, ST>(p, rheo, odd, ls, s);
+    return step_rh<Q, VLBM_OP_REGULARIZED, ST>(p, rheo, odd, ls, s);
+}
+
+template <int Q, int RHEO, int ST>
+cudaError_t macro_t(const MacroParams& mp, bool odd, cudaStream_t s) {
+    const unsigned g = grid_for(mp.s.N, 256);
+    if (odd) k_macro<Q, RHEO, ST, true><<<g, 256, 0, s>>>(mp);
+    else k_macro<Q, RHEO, ST, false><<<g, 256, 0, s>>>(mp);
+    return cudaGetLastError();
+}
+
+template <int Q, int ST>
+cudaError_t launch_macro_st(const MacroParams& mp, int rheo, bool odd, cudaStream_t s) {
+    switch (rheo) {
+    case VLBM_NEWTONIAN: return macro_t<Q, VLBM_NEWTONIAN, ST>(mp, odd, s);
+    case VLBM_BINGHAM: return macro_t<Q, VLBM_BINGHAM, ST>(mp, odd, s);
+    case VLBM_POWERLAW: return macro_t<Q, VLBM_POWERLAW, ST>(mp, odd, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int Q, int ST>
+cudaError_t get_pops_t(const StepParams& p, bool odd, float* out, cudaStream_t s) {
+    const unsigned g = grid_for(p.N, 256);
+    if (odd) k_get_pops<Q, ST, true><<<g, 256, 0, s>>>(p, out);
+    else k_get_pops<Q, ST, false><<<g, 256, 0, s>>>(p, out);
+    return cudaGetLastError();
+}
+
+template <int Q, int ST>
+cudaError_t launch_get_pops_st(const StepParams& p, bool odd, float* out, cudaStream_t s) {
+    return get_pops_t<Q, ST>(p, odd, out, s);
+}
+
+template <int Q, int ST>
+cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, float ux, float uy, float uz,
+                               cudaStream_t s) {
+    const unsigned g = grid_for(p.N, 256);
+    k_set_pops<Q, ST><<<g, 256, 0, s>>>(p, in, rho, ux, uy, uz);
+    return cudaGetLastError();
+}
+
+#define VLBM_INSTANTIATE(QQ, SS)                                                                              \
+    template cudaError_t launch_step_st<QQ, SS>(const StepParams&, int, int, bool, LaunchShape, cudaStream_t); \
+    template cudaError_t launch_macro_st<QQ, SS>(const MacroParams&, int, bool, cudaStream_t);                 \
+    template cudaError_t launch_get_pops_st<QQ, SS>(const StepParams&, bool, float*, cudaStream_t);            \
+    template cudaError_t launch_set_pops_st<QQ, SS>(const StepParams&, const float*, float, float, float, float, \
+                                                    cudaStream_t);
+
+}  // namespace vlbm

@@ -1,0 +1,84 @@
+// internal.h -- structures shared by the host side and the kernels of libvlbm.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+#include "../../include/vlbm.h"
+
+namespace vlbm {
+
+// Node class byte (one per lattice node, read by every fused step).
+enum : uint8_t {
+    NODE_BULK = 0,       // plain periodic streaming, no boundary rule
+    NODE_BC = 1,         // boundary node: look up bc_slot / BcRec
+    NODE_IBM_FORCE = 0x40 // IBM force present in the dense force field
+};
+
+// Boundary schemes as evaluated by the fused kernel.
+enum : uint8_t {
+    K_BC_NONE = 0,        // boundary node whose rule changes nothing (convex edge, ...)
+    K_BC_BOUNCE = 1,      // half-way bounce-back from own post-collision opposite
+    K_BC_VEL_BOUNCE = 2,  // moving-wall bounce-back from post-streaming opposite
+    K_BC_FREE_SLIP = 3,   // specular reflection from tangential neighbours
+    K_BC_VEL_ZOUHE = 4,   // D3Q19 velocity Zou-He (reference formulas)
+    K_BC_PRES_ZOUHE = 5   // D3Q19 pressure Zou-He (reference formulas)
+};
+
+// One record per boundary node, built on the host from the reference map.
+struct BcRec {
+    uint8_t scheme;      // K_BC_*
+    uint8_t dir;         // VLBM_NORTH ... (direction of the reference map)
+    uint8_t axis;        // wall-normal axis for faces (0 x, 1 y, 2 z)
+    uint8_t pad;
+    uint32_t mask;       // bit i set: population i is an unknown replaced by the rule
+    float uw[3];         // wall velocity (moving wall, velocity Zou-He)
+    float rhow;          // wall density (pressure Zou-He)
+};
+static_assert(sizeof(BcRec) == 24, "BcRec layout");
+
+struct StepParams {
+    void* pop;                  // populations [Q][N] (storage type per template)
+    uint8_t* cls;               // node class bytes [N]
+    const int32_t* bc_slot;     // [N], valid where cls & NODE_BC
+    const BcRec* bc;            // [nbc]
+    const float* side_prev;     // post-collision of boundary nodes, previous step [Q][nbc]
+    float* side_next;           // same, this step
+    float* omega;               // Power-Law omega state [N] (nullptr otherwise)
+    float* fibm;                // IBM force [3][N] (nullptr without spheres)
+    unsigned int* err;          // device error word (bit 0: bad density)
+    int nx, ny, nz;
+    long long N;
+    int nbc;
+    int apply_bc;               // 0 on the first step after (re)initialisation
+    float omega_newt;           // 1/tau
+    float fx, fy, fz;           // body force
+    float omega_p, yield;       // Bingham
+    float n_index, k_cons, gamma0;  // Power-Law
+    float scale, inv_scale, rho0;   // deviation storage
+};
+
+struct MacroParams {
+    StepParams s;
+    float *rho, *ux, *uy, *uz, *omega_out;
+    const float* fibm_const;    // IBM force to use in the half-force correction (may be null)
+};
+
+// Host-side analysis of a reference node map.
+struct BcTables {
+    std::vector<uint8_t> cls;        // [N]
+    std::vector<int32_t> slot;       // [N] (-1 for bulk)
+    std::vector<BcRec> recs;         // [nbc]
+    std::vector<int32_t> bc_nodes;   // [nbc] node index of each slot
+};
+
+vlbm_status build_bc_tables(const vlbm_config& cfg, const uint32_t* map, size_t n, BcTables& out,
+                            std::string& err);
+
+// Role of population i at a bounce-back node with direction dir:
+// 0 known, 1 replaced, 2 kept with its streamed value ("dead" population).
+int bb_role(int dir, int i);
+
+void set_last_error(const std::string& msg);
+
+}  // namespace vlbm

@@ -1,0 +1,72 @@
+// sim.h -- the simulation object behind the opaque vlbm_sim handle.
+#pragma once
+#include <cuda_runtime.h>
+#include <memory>
+#include <string>
+#include <vector>
+#include "internal.h"
+#include "dispatch.h"
+
+namespace vlbm {
+
+struct IbmState;   // ibm.cu
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace vlbm
+
+struct vlbm_sim {
+    vlbm_config cfg{};
+    int Q = 19;
+    long long N = 0;
+    int store_bytes = 4;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // device state
+    void* pop = nullptr;             // [Q][N] populations (AA in place)
+    uint8_t* cls = nullptr;          // [N] node class
+    int32_t* bc_slot = nullptr;      // [N]
+    vlbm::BcRec* bc = nullptr;       // [nbc]
+    float* side[2] = {nullptr, nullptr};  // [Q][nbc] post-collision at boundary nodes
+    int nbc = 0;
+    float* omega = nullptr;          // [N] Power-Law state
+    float* fibm = nullptr;           // [3][N] IBM force (allocated with spheres)
+    unsigned int* err = nullptr;     // device error word
+    float* scratch = nullptr;        // [5][N] macroscopic output scratch (lazy)
+    size_t device_bytes = 0;
+
+    // host state
+    int parity = 0;                  // 0: natural layout, 1: swapped layout
+    int side_cur = 0;                // side[side_cur] holds the last step's values
+    int apply_bc = 0;                // boundary rules active for the next gather
+    long long step = 0;
+    bool geometry = false;
+    int block = 256;                 // launch variant (threads per block)
+    int variant = 0;
+    std::vector<uint32_t> host_map;  // last node map (for outputs / servers)
+    vlbm::BcTables tables;
+
+    vlbm::IbmState* ibm = nullptr;   // owned; released by ibm_destroy
+    ~vlbm_sim();
+};
+
+namespace vlbm {
+
+StepParams make_params(vlbm_sim* s);
+vlbm_status cuda_status(cudaError_t e, const char* what);
+vlbm_status fluid_step(vlbm_sim* s);   // one fused step (no IBM)
+vlbm_status sim_macroscopics_device(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz, float* omega);
+vlbm_status sim_validate_config(const vlbm_config& c, std::string& why);
+
+// IBM hooks (ibm.cu)
+vlbm_status ibm_step(vlbm_sim* s);
+vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz);
+void ibm_destroy(IbmState* st);
+void ibm_reset(vlbm_sim* s);
+
+}  // namespace vlbm

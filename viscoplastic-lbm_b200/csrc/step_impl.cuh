@@ -1,0 +1,559 @@
+// step_impl.cuh -- the fused lattice-Boltzmann time step for sm_100a.
+//
+// One kernel per step does what the reference splits into four launches
+// (gpuMacrCollisionStream lbm.cu:4-504, gpuPopulationsTransfer lbm.cu:601-657,
+// gpuApplyBC lbm.cu:580-598 and the AB pointer swap populations.h:63-70):
+//
+//  * populations live in ONE array [Q][N] (SoA planes, x fastest) updated in
+//    place with the AA access pattern: even steps read slot i of the node and
+//    write the post-collision value of i into slot opp(i) of the same node;
+//    odd steps read the value streamed towards the node from slot opp(i) of the
+//    upstream neighbour and write into slot i of the downstream neighbour.
+//    Every slot is read and written by exactly one thread, so no barrier is
+//    needed and half the reference's population memory is used.
+//  * streaming is fully periodic (index wrap, which is what the reference's
+//    ghost-plane transfer amounts to on one GPU); boundary rules are applied
+//    when a boundary node READS its populations, from the streamed values and
+//    from a small double-buffered side store holding the post-collision
+//    populations of boundary nodes from the previous step (the reference keeps
+//    those in `pop` at nodes with SAVE_POST_COL, lbm.cu:463-470).  This
+//    reproduces the reference's semantics exactly, including the populations it
+//    leaves with their wrapped values at concave edges ("dead pops") and the
+//    moving-wall rule that sums the wrapped unknowns into rho_w.
+//  * collision (BGK or regularized), Guo forcing and the Bingham / Power-Law
+//    relaxation are computed in FP32 registers; storage is FP32 or FP16/BF16
+//    deviations (f_i - w_i*rho0)*scale.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include "internal.h"
+#include "lattice.cuh"
+
+namespace vlbm {
+
+// ------------------------------------------------------------- storage --
+template <int ST> struct Store;
+template <> struct Store<VLBM_STORE_F32> {
+    using T = float;
+    static __device__ __forceinline__ float ld(const T* p, float, const StepParams&) { return *p; }
+    static __device__ __forceinline__ void st(T* p, float v, float, const StepParams&) { *p = v; }
+};
+template <> struct Store<VLBM_STORE_F16> {
+    using T = __half;
+    static __device__ __forceinline__ float ld(const T* p, float w, const StepParams& s) {
+        return fmaf(__half2float(*p), s.inv_scale, w * s.rho0);
+    }
+    static __device__ __forceinline__ void st(T* p, float v, float w, const StepParams& s) {
+        *p = __float2half_rn((v - w * s.rho0) * s.scale);
+    }
+};
+template <> struct Store<VLBM_STORE_BF16> {
+    using T = __nv_bfloat16;
+    static __device__ __forceinline__ float ld(const T* p, float w, const StepParams& s) {
+        return fmaf(__bfloat162float(*p), s.inv_scale, w * s.rho0);
+    }
+    static __device__ __forceinline__ void st(T* p, float v, float w, const StepParams& s) {
+        *p = __float2bfloat16_rn((v - w * s.rho0) * s.scale);
+    }
+};
+
+// Reflection of population i across the plane normal to `axis`.
+VLBM_HD constexpr int lat_refl(int i, int axis) {
+    int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
+    if (axis == 0) cx = -cx;
+    else if (axis == 1) cy = -cy;
+    else cz = -cz;
+    for (int j = 0; j < 27; ++j)
+        if (lat_cx(j) == cx && lat_cy(j) == cy && lat_cz(j) == cz) return j;
+    return i;
+}
+
+// Periodic neighbour offsets of one node (in nodes).
+struct Nbr {
+    int xm, xp, ym, yp, zm, zp;
+    __device__ __forceinline__ void init(int x, int y, int z, int nx, int ny, int nz) {
+        const int nxy = nx * ny;
+        xm = (x == 0) ? nx - 1 : -1;
+        xp = (x == nx - 1) ? -(nx - 1) : 1;
+        ym = (y == 0) ? (ny - 1) * nx : -nx;
+        yp = (y == ny - 1) ? -(ny - 1) * nx : nx;
+        zm = (z == 0) ? (nz - 1) * nxy : -nxy;
+        zp = (z == nz - 1) ? -(nz - 1) * nxy : nxy;
+    }
+    // offset of the node at (x+dx, y+dy, z+dz), dx,dy,dz in {-1,0,1}
+    __device__ __forceinline__ int off(int dx, int dy, int dz) const {
+        return (dx > 0 ? xp : (dx < 0 ? xm : 0)) + (dy > 0 ? yp : (dy < 0 ? ym : 0)) +
+               (dz > 0 ? zp : (dz < 0 ? zm : 0));
+    }
+};
+
+// ------------------------------------------------- D3Q19 Zou-He (reference) --
+// Velocity Zou-He, D3Q19_VelZouHe.cu:27-172, per face as the reference writes it.
+__device__ __forceinline__ void zouhe_vel19(float (&f)[19], int dir, float ux, float uy, float uz) {
+    float g4 = f[4], g8 = f[8], g13 = f[13], g12 = f[12], g18 = f[18];
+    switch (dir) {
+    case VLBM_NORTH: {
+        float rw = (1.f / (1.f + uy)) * (f[1] + f[2] + f[5] + f[6] + f[9] + f[15] + f[16] + f[10] + f[0] +
+                                         2.f * (f[3] + f[7] + f[14] + f[11] + f[17]));
+        float nyx = 0.5f * (f[1] + f[9] + f[15] - (f[2] + f[16] + f[10])) - ux * rw / 3.f;
+        float nyz = 0.5f * (f[5] + f[9] + f[16] - (f[6] + f[15] + f[10])) - uz * rw / 3.f;
+        g4 = f[3] + rw * (-uy) / 3.f;
+        g8 = f[7] + rw * (-uy - ux) / 6.f + nyx;
+        g13 = f[14] + rw * (-uy + ux) / 6.f - nyx;
+        g12 = f[11] + rw * (-uy - uz) / 6.f + nyz;
+        g18 = f[17] + rw * (-uy + uz) / 6.f - nyz;
+        f[4] = g4; f[8] = g8; f[13] = g13; f[12] = g12; f[18] = g18;
+        break; }
+    case VLBM_SOUTH: {
+        float rw = (1.f / (1.f - uy)) * (f[1] + f[2] + f[5] + f[6] + f[9] + f[15] + f[16] + f[10] + f[0] +
+                                         2.f * (f[4] + f[13] + f[8] + f[18] + f[12]));
+        float nyx = 0.5f * (f[1] + f[9] + f[15] - (f[2] + f[16] + f[10])) - ux * rw / 3.f;
+        float nyz = 0.5f * (f[5] + f[9] + f[16] - (f[6] + f[15] + f[10])) - uz * rw / 3.f;
+        float a3 = f[4] + rw * uy / 3.f, a7 = f[8] + rw * (uy + ux) / 6.f - nyx,
+              a14 = f[13] + rw * (uy - ux) / 6.f + nyx, a11 = f[12] + rw * (uy + uz) / 6.f - nyz,
+              a17 = f[18] + rw * (uy - uz) / 6.f + nyz;
+        f[3] = a3; f[7] = a7; f[14] = a14; f[11] = a11; f[17] = a17;
+        break; }
+    case VLBM_WEST: {
+        float rw = (1.f / (1.f - ux)) * (f[3] + f[4] + f[5] + f[6] + f[11] + f[17] + f[18] + f[12] + f[0] +
+                                         2.f * (f[2] + f[14] + f[8] + f[16] + f[10]));
+        float nxy = 0.5f * (f[3] + f[11] + f[17] - (f[4] + f[18] + f[12])) - uy * rw / 3.f;
+        float nxz = 0.5f * (f[5] + f[18] + f[11] - (f[6] + f[17] + f[12])) - uz * rw / 3.f;
+        float a1 = f[2] + rw * ux / 3.f, a13 = f[14] + rw * (ux - uy) / 6.f + nxy,
+              a7 = f[8] + rw * (ux + uy) / 6.f - nxy, a9 = f[10] + rw * (ux + uz) / 6.f - nxz,
+              a15 = f[16] + rw * (ux - uy) / 6.f + nxz;
+        f[1] = a1; f[13] = a13; f[7] = a7; f[9] = a9; f[15] = a15;
+        break; }
+    case VLBM_EAST: {
+        float rw = (1.f / (1.f + ux)) * (f[3] + f[4] + f[5] + f[6] + f[11] + f[17] + f[18] + f[12] + f[0] +
+                                         2.f * (f[2] + f[14] + f[8] + f[16] + f[10]));
+        float nxy = 0.5f * (f[3] + f[11] + f[17] - (f[4] + f[18] + f[12])) - uy * rw / 3.f;
+        float nxz = 0.5f * (f[5] + f[18] + f[11] - (f[6] + f[17] + f[12])) - uz * rw / 3.f;
+        float a2 = f[2] + rw * ux / 3.f, a14 = f[14] + rw * (ux - uy) / 6.f + nxy,
+              a8 = f[8] + rw * (ux + uy) / 6.f - nxy, a10 = f[10] + rw * (ux + uz) / 6.f - nxz,
+              a16 = f[16] + rw * (ux - uy) / 6.f + nxz;
+        f[2] = a2; f[14] = a14; f[8] = a8; f[10] = a10; f[16] = a16;
+        break; }
+    case VLBM_FRONT: {
+        float rw = (1.f / (1.f + uz)) * (f[1] + f[2] + f[3] + f[4] + f[7] + f[14] + f[8] + f[13] + f[0] +
+                                         2.f * (f[5] + f[9] + f[16] + f[11] + f[18]));
+        float nzx = 0.5f * (f[1] + f[7] + f[13] - (f[2] + f[14] + f[8])) - rw * ux / 3.f;
+        float nzy = 0.5f * (f[3] + f[7] + f[14] - (f[4] + f[13] + f[8])) - rw * uy / 3.f;
+        float a6 = f[5] + rw * (-uz) / 3.f, a15 = f[16] + rw * (-uz + ux) / 6.f - nzx,
+              a10 = f[9] + rw * (-uz - ux) / 6.f + nzx, a17 = f[18] + rw * (-uz + uy) / 6.f - nzy,
+              a12 = f[11] + rw * (-uz - uy) / 6.f + nzy;
+        f[6] = a6; f[15] = a15; f[10] = a10; f[17] = a17; f[12] = a12;
+        break; }
+    case VLBM_BACK: {
+        float rw = (1.f / (1.f + uz)) * (f[1] + f[2] + f[3] + f[4] + f[7] + f[14] + f[8] + f[13] + f[0] +
+                                         2.f * (f[6] + f[15] + f[10] + f[17] + f[12]));
+        float nzx = 0.5f * (f[1] + f[7] + f[13] - (f[2] + f[14] + f[8])) - rw * ux / 3.f;
+        float nzy = 0.5f * (f[3] + f[7] + f[14] - (f[4] + f[13] + f[8])) - rw * uy / 3.f;
+        float a5 = f[6] + rw * uz / 3.f, a9 = f[10] + rw * (uz + ux) / 6.f - nzx,
+              a16 = f[15] + rw * (uz - ux) / 6.f + nzx, a11 = f[12] + rw * (uz + ux) / 6.f - nzy,
+              a18 = f[17] + rw * (uz - ux) / 6.f + nzy;
+        f[5] = a5; f[9] = a9; f[16] = a16; f[11] = a11; f[18] = a18;
+        break; }
+    default: break;
+    }
+}
+
+// Pressure Zou-He, D3Q19_PresZouHe.cu:27-176, per face as the reference writes it.
+__device__ __forceinline__ void zouhe_pres19(float (&f)[19], int dir, float rw) {
+    switch (dir) {
+    case VLBM_NORTH: {
+        float uy = -1.f + (1.f / rw) * (f[1] + f[2] + f[5] + f[6] + f[9] + f[15] + f[16] + f[10] + f[0] +
+                                        2.f * (f[3] + f[7] + f[14] + f[11] + f[17]));
+        float nyx = 0.5f * (f[1] + f[9] + f[15] - (f[2] + f[16] + f[10]));
+        float nyz = 0.5f * (f[5] + f[9] + f[16] - (f[6] + f[15] + f[10]));
+        float a4 = f[3] + rw * (-uy) / 3.f, a8 = f[7] + rw * (-uy) / 6.f + nyx,
+              a13 = f[14] + rw * (-uy) / 6.f - nyx, a12 = f[11] + rw * (-uy) / 6.f + nyz,
+              a18 = f[17] + rw * (-uy) / 6.f - nyz;
+        f[4] = a4; f[8] = a8; f[13] = a13; f[12] = a12; f[18] = a18;
+        break; }
+    case VLBM_SOUTH: {
+        float uy = 1.f - (1.f / rw) * (f[1] + f[2] + f[5] + f[6] + f[9] + f[15] + f[16] + f[10] + f[0] +
+                                       2.f * (f[4] + f[13] + f[8] + f[18] + f[12]));
+        float nyx = 0.5f * (f[1] + f[9] + f[15] - (f[2] + f[16] + f[10]));
+        float nyz = 0.5f * (f[5] + f[9] + f[16] - (f[6] + f[15] + f[10]));
+        float a3 = f[4] + rw * uy / 3.f, a7 = f[8] + rw * uy / 6.f - nyx, a14 = f[13] + rw * uy / 6.f + nyx,
+              a11 = f[12] + rw * uy / 6.f - nyz, a17 = f[18] + rw * uy / 6.f + nyz;
+        f[3] = a3; f[7] = a7; f[14] = a14; f[11] = a11; f[17] = a17;
+        break; }
+    case VLBM_WEST: {
+        float ux = 1.f - (1.f / rw) * (f[3] + f[4] + f[5] + f[6] + f[11] + f[17] + f[18] + f[12] + f[0] +
+                                       2.f * (f[2] + f[14] + f[8] + f[16] + f[10]));
+        float nxy = 0.5f * (f[3] + f[11] + f[17] - (f[4] + f[18] + f[12]));
+        float nxz = 0.5f * (f[5] + f[18] + f[11] - (f[6] + f[17] + f[12]));
+        float a1 = f[2] + rw * ux / 3.f, a13 = f[14] + rw * ux / 6.f + nxy, a7 = f[8] + rw * ux / 6.f - nxy,
+              a9 = f[10] + rw * ux / 6.f - nxz, a15 = f[16] + rw * ux / 6.f + nxz;
+        f[1] = a1; f[13] = a13; f[7] = a7; f[9] = a9; f[15] = a15;
+        break; }
+    case VLBM_EAST: {
+        float ux = -1.f + (1.f / rw) * (f[3] + f[4] + f[5] + f[6] + f[11] + f[17] + f[18] + f[12] + f[0] +
+                                        2.f * (f[2] + f[14] + f[8] + f[16] + f[10]));
+        float nxy = 0.5f * (f[3] + f[11] + f[17] - (f[4] + f[18] + f[12]));
+        float nxz = 0.5f * (f[5] + f[18] + f[11] - (f[6] + f[17] + f[12]));
+        float a2 = f[2] + rw * ux / 3.f, a14 = f[14] + rw * ux / 6.f + nxy, a8 = f[8] + rw * ux / 6.f - nxy,
+              a10 = f[10] + rw * ux / 6.f - nxz, a16 = f[16] + rw * ux / 6.f + nxz;
+        f[2] = a2; f[14] = a14; f[8] = a8; f[10] = a10; f[16] = a16;
+        break; }
+    case VLBM_FRONT: {
+        float uz = -1.f + (1.f / rw) * (f[1] + f[2] + f[3] + f[4] + f[7] + f[14] + f[8] + f[13] + f[0] +
+                                        2.f * (f[5] + f[9] + f[16] + f[11] + f[18]));
+        float nzx = 0.5f * (f[1] + f[7] + f[13] - (f[2] + f[14] + f[8]));
+        float nzy = 0.5f * (f[3] + f[7] + f[14] - (f[4] + f[13] + f[8]));
+        float a6 = f[5] + rw * (-uz) / 3.f, a15 = f[16] + rw * (-uz) / 6.f - nzx,
+              a10 = f[9] + rw * (-uz) / 6.f + nzx, a17 = f[18] + rw * (-uz) / 6.f - nzy,
+              a12 = f[11] + rw * (-uz) / 6.f + nzy;
+        f[6] = a6; f[15] = a15; f[10] = a10; f[17] = a17; f[12] = a12;
+        break; }
+    case VLBM_BACK: {
+        float uz = 1.f - (1.f / rw) * (f[1] + f[2] + f[3] + f[4] + f[7] + f[14] + f[8] + f[13] + f[0] +
+                                       2.f * (f[6] + f[10] + f[12] + f[15] + f[17]));
+        float nzx = 0.5f * (f[1] + f[7] + f[13] - (f[2] + f[14] + f[8]));
+        float nzy = 0.5f * (f[3] + f[7] + f[14] - (f[4] + f[13] + f[8]));
+        float a5 = f[6] + rw * uz / 3.f, a9 = f[10] + rw * uz / 6.f - nzx, a16 = f[15] + rw * uz / 6.f + nzx,
+              a11 = f[12] + rw * uz / 6.f - nzy, a18 = f[17] + rw * uz / 6.f + nzy;
+        f[5] = a5; f[9] = a9; f[16] = a16; f[11] = a11; f[18] = a18;
+        break; }
+    default: break;
+    }
+}
+
+// ----------------------------------------------------- boundary at gather --
+template <int Q>
+__device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int slot, int x, int y, int z,
+                                      const Nbr& nb, unsigned n) {
+    const BcRec r = p.bc[slot];
+    const size_t nbc = (size_t)p.nbc;
+    switch (r.scheme) {
+    case K_BC_BOUNCE:
+        // bounceBack.cu:26-498: unknown <- own post-collision opposite
+#pragma unroll
+        for (int i = 1; i < Q; ++i)
+            if ((r.mask >> i) & 1u) f[i] = p.side_prev[(size_t)lat_opp(i) * nbc + slot];
+        break;
+    case K_BC_VEL_BOUNCE: {
+        // D3Q19_VelBounceBack.cu:31-43: rho_w over all streamed populations
+        // (including the wrapped unknowns), unknown <- streamed opposite
+        // - 6 rho_w w_i (c_opp . u_w).  The opposite of an unknown at a face is
+        // always a known population, so the update can run in place.
+        float rw = 0.f;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) rw += f[i];
+#pragma unroll
+        for (int i = 1; i < Q; ++i)
+            if ((r.mask >> i) & 1u) {
+                const int o = lat_opp(i);
+                const float cu = lat_cx(o) * r.uw[0] + lat_cy(o) * r.uw[1] + lat_cz(o) * r.uw[2];
+                f[i] = f[o] - 6.f * rw * Lattice<Q>::w(i) * cu;
+            }
+        break;
+    }
+    case K_BC_FREE_SLIP:
+        // freeSlip.cu:26-167: reflected post-collision population of the node one
+        // tangential step upstream
+#pragma unroll
+        for (int i = 1; i < Q; ++i)
+            if ((r.mask >> i) & 1u) {
+                const int a = r.axis;
+                const int j = a == 0 ? lat_refl(i, 0) : (a == 1 ? lat_refl(i, 1) : lat_refl(i, 2));
+                const int tx = a == 0 ? 0 : lat_cx(i), ty = a == 1 ? 0 : lat_cy(i), tz = a == 2 ? 0 : lat_cz(i);
+                const unsigned src = n + nb.off(-tx, -ty, -tz);
+                const int sslot = p.bc_slot[src];
+                f[i] = p.side_prev[(size_t)j * nbc + sslot];
+            }
+        break;
+    case K_BC_VEL_ZOUHE:
+        if constexpr (Q == 19) zouhe_vel19(f, r.dir, r.uw[0], r.uw[1], r.uw[2]);
+        break;
+    case K_BC_PRES_ZOUHE:
+        if constexpr (Q == 19) zouhe_pres19(f, r.dir, r.rhow);
+        break;
+    default: break;
+    }
+    (void)x; (void)y; (void)z;
+}
+
+// Gather f_i(x, t) of node n (after boundary rules).  Returns the side-store
+// slot of a boundary node, -1 for bulk nodes.
+template <int Q, int ST, bool ODD>
+__device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr& nb, int x, int y, int z,
+                                      float (&f)[Q], uint8_t& cls) {
+    using S = Store<ST>;
+    using T = typename S::T;
+    const T* A = static_cast<const T*>(p.pop);
+    const size_t N = (size_t)p.N;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        if (!ODD) {
+            f[i] = S::ld(A + (size_t)i * N + n, Lattice<Q>::w(i), p);
+        } else {
+            const unsigned src = n + nb.off(-lat_cx(i), -lat_cy(i), -lat_cz(i));
+            f[i] = S::ld(A + (size_t)lat_opp(i) * N + src, Lattice<Q>::w(i), p);
+        }
+    }
+    cls = p.cls[n];
+    int slot = -1;
+    if (cls & NODE_BC) {
+        slot = p.bc_slot[n];
+        if (p.apply_bc) apply_bc<Q>(f, p, slot, x, y, z, nb, n);
+    }
+    return slot;
+}
+
+// Moments of a node: rho, u (with half force, lbm.cu:79-111), non-equilibrium
+// second moments (lbm.cu:149-190) and the stress magnitude used by the
+// rheology models (lbm.cu:192-208).
+struct Mom {
+    float rho, ux, uy, uz;
+    float pxx, pyy, pzz, pxy, pxz, pyz;
+};
+
+template <int Q, bool NEED_PI>
+__device__ __forceinline__ Mom moments(const float (&f)[Q], float fx, float fy, float fz) {
+    Mom m;
+    float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
+        rho += f[i];
+        if (cx) jx += cx * f[i];
+        if (cy) jy += cy * f[i];
+        if (cz) jz += cz * f[i];
+        if (NEED_PI) {
+            if (cx) sxx += f[i];
+            if (cy) syy += f[i];
+            if (cz) szz += f[i];
+            if (cx && cy) sxy += cx * cy * f[i];
+            if (cx && cz) sxz += cx * cz * f[i];
+            if (cy && cz) syz += cy * cz * f[i];
+        }
+    }
+    const float inv = 1.f / rho;
+    m.rho = rho;
+    m.ux = (jx + 0.5f * fx) * inv;
+    m.uy = (jy + 0.5f * fy) * inv;
+    m.uz = (jz + 0.5f * fz) * inv;
+    if (NEED_PI) {
+        const float cs2 = 1.f / 3.f;
+        m.pxx = sxx - rho * (m.ux * m.ux + cs2);
+        m.pyy = syy - rho * (m.uy * m.uy + cs2);
+        m.pzz = szz - rho * (m.uz * m.uz + cs2);
+        m.pxy = sxy - rho * m.ux * m.uy;
+        m.pxz = sxz - rho * m.ux * m.uz;
+        m.pyz = syz - rho * m.uy * m.uz;
+    } else {
+        m.pxx = m.pyy = m.pzz = m.pxy = m.pxz = m.pyz = 0.f;
+    }
+    return m;
+}
+
+__device__ __forceinline__ float stress_aux(const Mom& m, float fx, float fy, float fz) {
+    const float a = m.pxx + m.ux * fx, b = m.pyy + m.uy * fy, c = m.pzz + m.uz * fz;
+    const float d = m.pxy + 0.5f * (m.ux * fy + m.uy * fx);
+    const float e = m.pxz + 0.5f * (m.ux * fz + m.uz * fx);
+    const float g = m.pyz + 0.5f * (m.uy * fz + m.uz * fy);
+    return sqrtf(0.5f * (a * a + b * b + c * c + 2.f * (d * d + e * e + g * g)));
+}
+
+// nnf.h:32-87 calcOmega.
+template <int RHEO>
+__device__ __forceinline__ float relax(const StepParams& p, float omega_old, float aux) {
+    if (RHEO == VLBM_BINGHAM) {
+        return p.omega_p * fmaxf(0.f, 1.f - p.yield / aux);
+    } else if (RHEO == VLBM_POWERLAW) {
+        float eta = ((1.f / omega_old) - 0.5f) / 3.f;
+        const float gd = (1.f - 0.5f * omega_old) * aux / eta;
+        eta = (gd <= p.gamma0) ? p.k_cons : p.k_cons * powf(gd, p.n_index - 1.f);
+        return 1.f / (0.5f + 3.f * eta);
+    }
+    return p.omega_newt;
+}
+
+// Collision in place: f <- f*.
+//  regularized (lbm.cu:263-461):
+//    f*_i = w_i [ A (Q_i:Pi - c_i.F/3) + rho(1 - 1.5u^2 + 3cu + 4.5cu^2) + B(3(c_i-u).F + 9 cu cF) ]
+//    A = 4.5(1-omega), B = 1-omega/2
+//  BGK (collisionForceNoReg.txt): f*_i = (1-omega) f_i + omega f_eq_i + B F_i
+template <int Q, int OP>
+__device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega, float fx, float fy, float fz) {
+    const float B = 1.f - 0.5f * omega;
+    const float uu = m.ux * m.ux + m.uy * m.uy + m.uz * m.uz;
+    const float uF = m.ux * fx + m.uy * fy + m.uz * fz;
+    if (OP == VLBM_OP_REGULARIZED) {
+        const float A = 4.5f * (1.f - omega);
+        const float tr = (m.pxx + m.pyy + m.pzz) * (1.f / 3.f);
+        const float K0 = m.rho * (1.f - 1.5f * uu) - 3.f * B * uF - A * tr;
+        const float alpha = 3.f * B - A * (1.f / 3.f);
+        const float r3 = 3.f * m.rho, r45 = 4.5f * m.rho, b9 = 9.f * B;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
+            float S = 0.f, cu = 0.f, cF = 0.f;
+            if (cx) { S += m.pxx; cu += cx * m.ux; cF += cx * fx; }
+            if (cy) { S += m.pyy; cu += cy * m.uy; cF += cy * fy; }
+            if (cz) { S += m.pzz; cu += cz * m.uz; cF += cz * fz; }
+            if (cx && cy) S += 2.f * cx * cy * m.pxy;
+            if (cx && cz) S += 2.f * cx * cz * m.pxz;
+            if (cy && cz) S += 2.f * cy * cz * m.pyz;
+            const float v = K0 + A * S + alpha * cF + cu * (r3 + r45 * cu + b9 * cF);
+            f[i] = Lattice<Q>::w(i) * v;
+        }
+    } else {
+        const float om1 = 1.f - omega;
+        const float base = 1.f - 1.5f * uu;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
+            float cu = 0.f, cF = 0.f;
+            if (cx) { cu += cx * m.ux; cF += cx * fx; }
+            if (cy) { cu += cy * m.uy; cF += cy * fy; }
+            if (cz) { cu += cz * m.uz; cF += cz * fz; }
+            const float w = Lattice<Q>::w(i);
+            const float feq = w * m.rho * (base + 3.f * cu + 4.5f * cu * cu);
+            const float frc = w * (3.f * cF - 3.f * uF + 9.f * cu * cF);
+            f[i] = om1 * f[i] + omega * feq + B * frc;
+        }
+    }
+}
+
+// ------------------------------------------------------------ kernels --
+template <int Q, int OP, int RHEO, int ST, bool ODD>
+__global__ void __launch_bounds__(256) k_step(const StepParams p) {
+    using S = Store<ST>;
+    using T = typename S::T;
+    const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= (unsigned)p.N) return;
+    const int x = (int)(n % (unsigned)p.nx);
+    const unsigned t = n / (unsigned)p.nx;
+    const int y = (int)(t % (unsigned)p.ny);
+    const int z = (int)(t / (unsigned)p.ny);
+    Nbr nb;
+    nb.init(x, y, z, p.nx, p.ny, p.nz);
+
+    float f[Q];
+    uint8_t cls;
+    const int slot = gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
+
+    float fx = p.fx, fy = p.fy, fz = p.fz;
+    if (cls & NODE_IBM_FORCE) {  // IBM force read and reset (lbm.cu:45-58)
+        const size_t N = (size_t)p.N;
+        fx += p.fibm[n]; fy += p.fibm[N + n]; fz += p.fibm[2 * N + n];
+        p.fibm[n] = 0.f; p.fibm[N + n] = 0.f; p.fibm[2 * N + n] = 0.f;
+        p.cls[n] = cls & (uint8_t)~NODE_IBM_FORCE;
+    }
+    constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
+    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz);
+    if (!(m.rho > 0.f && m.rho < 1e30f)) atomicOr(p.err, 1u);
+    float omega = p.omega_newt;
+    if (RHEO != VLBM_NEWTONIAN) {
+        const float aux = stress_aux(m, fx, fy, fz);
+        const float old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;
+        omega = relax<RHEO>(p, old, aux);
+        if (RHEO == VLBM_POWERLAW) p.omega[n] = omega;  // lbm.cu:215-219
+    }
+    collide<Q, OP>(f, m, omega, fx, fy, fz);
+
+    if (slot >= 0) {
+        const size_t nbc = (size_t)p.nbc;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) p.side_next[(size_t)i * nbc + slot] = f[i];
+    }
+    T* A = static_cast<T*>(p.pop);
+    const size_t N = (size_t)p.N;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        if (!ODD) {
+            S::st(A + (size_t)lat_opp(i) * N + n, f[i], Lattice<Q>::w(i), p);
+        } else {
+            const unsigned dst = n + nb.off(lat_cx(i), lat_cy(i), lat_cz(i));
+            S::st(A + (size_t)i * N + dst, f[i], Lattice<Q>::w(i), p);
+        }
+    }
+}
+
+// Macroscopics of the current state (what gpuMacrCollisionStream saves).
+template <int Q, int RHEO, int ST, bool ODD>
+__global__ void __launch_bounds__(256) k_macro(const MacroParams mp) {
+    const StepParams& p = mp.s;
+    const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= (unsigned)p.N) return;
+    const int x = (int)(n % (unsigned)p.nx);
+    const unsigned t = n / (unsigned)p.nx;
+    const int y = (int)(t % (unsigned)p.ny);
+    const int z = (int)(t / (unsigned)p.ny);
+    Nbr nb;
+    nb.init(x, y, z, p.nx, p.ny, p.nz);
+    float f[Q];
+    uint8_t cls;
+    gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
+    float fx = p.fx, fy = p.fy, fz = p.fz;
+    if (mp.fibm_const) {
+        const size_t N = (size_t)p.N;
+        fx += mp.fibm_const[n]; fy += mp.fibm_const[N + n]; fz += mp.fibm_const[2 * N + n];
+    }
+    constexpr bool NEED_PI = RHEO != VLBM_NEWTONIAN;
+    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz);
+    if (mp.rho) mp.rho[n] = m.rho;
+    if (mp.ux) mp.ux[n] = m.ux;
+    if (mp.uy) mp.uy[n] = m.uy;
+    if (mp.uz) mp.uz[n] = m.uz;
+    if (mp.omega_out) {
+        float omega = p.omega_newt;
+        if (RHEO != VLBM_NEWTONIAN) {
+            const float aux = stress_aux(m, fx, fy, fz);
+            const float old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;
+            omega = relax<RHEO>(p, old, aux);
+        }
+        mp.omega_out[n] = omega;
+    }
+}
+
+// Populations f_i(x,t) after boundary rules, natural [Q][N] float layout.
+template <int Q, int ST, bool ODD>
+__global__ void __launch_bounds__(256) k_get_pops(const StepParams p, float* out) {
+    const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= (unsigned)p.N) return;
+    const int x = (int)(n % (unsigned)p.nx);
+    const unsigned t = n / (unsigned)p.nx;
+    const int y = (int)(t % (unsigned)p.ny);
+    const int z = (int)(t / (unsigned)p.ny);
+    Nbr nb;
+    nb.init(x, y, z, p.nx, p.ny, p.nz);
+    float f[Q];
+    uint8_t cls;
+    gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) out[(size_t)i * (size_t)p.N + n] = f[i];
+}
+
+// Natural-layout store of given populations (equilibrium init or user state).
+template <int Q, int ST>
+__global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const float* in, float rho, float ux,
+                                                  float uy, float uz) {
+    using S = Store<ST>;
+    using T = typename S::T;
+    const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= (unsigned)p.N) return;
+    T* A = static_cast<T*>(p.pop);
+    const size_t N = (size_t)p.N;
+    const float uu = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        float v;
+        if (in) {
+            v = in[(size_t)i * N + n];
+        } else {  // gpu_f_eq, globalFunctions.h:50-56 / lbmInitialization.cu:78-89
+            const float cu = lat_cx(i) * ux + lat_cy(i) * uy + lat_cz(i) * uz;
+            v = Lattice<Q>::w(i) * rho * (1.f - 1.5f * uu + 3.f * cu * (1.f + 1.5f * cu));
+        }
+        S::st(A + (size_t)i * N + n, v, Lattice<Q>::w(i), p);
+    }
+    if (p.omega) p.omega[n] = 0.f;  // lbmInitialization.cu:111
+}
+
+}  // namespace vlbm
