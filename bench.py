@@ -152,8 +152,8 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="vlbm", choices=["vlbm", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

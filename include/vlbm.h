@@ -174,6 +174,13 @@ vlbm_status vlbm_get_populations(vlbm_sim* sim, float* pops, size_t n);
 /* Set the full population state (same layout); resets boundary side-state. */
 vlbm_status vlbm_set_populations(vlbm_sim* sim, const float* pops, size_t n);
 
+/* Global mass and momentum of the current state in FP64: out4 = {sum rho,
+ * sum rho*ux, sum rho*uy, sum rho*uz} with rho*u = sum_i f_i c_i + F/2 per node
+ * (host array of 4 doubles).  Replaces the FP32 density reduction of
+ * AuxFunctions/reduction.cu:36-98 / auxFunction.cu:3-62 and the host sums of
+ * treatData.cpp:25-449.  Allocates its partial-sum buffer on first use. */
+vlbm_status vlbm_moments_sum(vlbm_sim* sim, double* out4);
+
 /* Per-node IBM force (macr.f, macroscopics.h) of the current state, [3][nz][ny][nx]. */
 vlbm_status vlbm_get_forces(vlbm_sim* sim, float* fxyz, size_t n);
 

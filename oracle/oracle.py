@@ -59,6 +59,8 @@ def _bind_ibm(lib):
     D = C.POINTER(C.c_double)
     lib.oracle_ibm_create.restype = P
     lib.oracle_ibm_create.argtypes = [P, C.POINTER(C.c_uint32), P, P, C.c_int]
+    lib.oracle_ibm_fluid.restype = P
+    lib.oracle_ibm_fluid.argtypes = [P]
     lib.oracle_ibm_step.argtypes = [P, C.c_int]
     lib.oracle_ibm_macro.argtypes = [P, D, D, D, D]
     lib.oracle_ibm_particles.argtypes = [P, D, C.c_int]
@@ -145,6 +147,70 @@ class Oracle:
     def set_populations(self, pops):
         a = np.ascontiguousarray(pops, dtype=np.float64).ravel()
         _lib.oracle_set_pops(self._h, a.ctypes.data_as(C.POINTER(C.c_double)))
+
+
+class OracleIbm:
+    """Fluid step + immersed-boundary step for spheres, FP64 (reference loop order)."""
+
+    def __init__(self, cfg, node_map, ibm_cfg, spheres):
+        self.cfg = cfg
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        self.n = cfg.nx * cfg.ny * cfg.nz
+        m = np.ascontiguousarray(node_map, dtype=np.uint32).ravel()
+        arr = (type(spheres[0]) * len(spheres))(*spheres)
+        self._keep = arr
+        self.np = len(spheres)
+        self._h = _lib.oracle_ibm_create(C.byref(cfg), m.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                         C.byref(ibm_cfg), C.cast(arr, C.c_void_p), len(spheres))
+
+    def close(self):
+        if self._h:
+            _lib.oracle_ibm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        _lib.oracle_ibm_step(self._h, int(n))
+
+    def macroscopics(self):
+        out = [np.empty(self.n) for _ in range(4)]
+        _lib.oracle_ibm_macro(self._h, *[a.ctypes.data_as(C.POINTER(C.c_double)) for a in out])
+        return {k: v.reshape(self.shape) for k, v in zip(("rho", "ux", "uy", "uz"), out)}
+
+    def particles(self):
+        out = np.empty(24 * self.np)
+        _lib.oracle_ibm_particles(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), self.np)
+        out = out.reshape(self.np, 24)
+        return {"pos": out[:, 0:3], "vel": out[:, 3:6], "w": out[:, 6:9], "f": out[:, 9:12],
+                "M": out[:, 12:15], "w_avg": out[:, 15:18], "I": out[:, 18:24]}
+
+    def nodes(self):
+        n = _lib.oracle_ibm_nodes(self._h, None, 0)
+        out = np.empty(3 * n)
+        _lib.oracle_ibm_nodes(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        return out.reshape(3, n)
+
+    def populations(self):
+        fl = _lib.oracle_ibm_fluid(self._h)
+        q = self.cfg.vel_set
+        out = np.empty(q * self.n)
+        _lib.oracle_get_pops(fl, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out.reshape((q,) + self.shape)
+
+
+def sphere_mesh(diameter, mesh_scale=1.0):
+    """makeSpherePolar node positions relative to the centre [3][n] and areas [n]."""
+    n = _lib.oracle_sphere_mesh(diameter, mesh_scale, None, None, 0)
+    xyz = np.empty(3 * n)
+    S = np.empty(n)
+    _lib.oracle_sphere_mesh(diameter, mesh_scale, xyz.ctypes.data_as(C.POINTER(C.c_double)),
+                            S.ctypes.data_as(C.POINTER(C.c_double)), n)
+    return xyz.reshape(3, n), S
 
 
 # --------------------------------------------------------------------------

@@ -137,7 +137,7 @@ using namespace vlbm;
 vlbm_sim::~vlbm_sim() {
     if (ibm) { ibm_destroy(ibm); ibm = nullptr; }
     cudaFree(pop); cudaFree(cls); cudaFree(bc_slot); cudaFree(bc);
-    cudaFree(side[0]); cudaFree(side[1]); cudaFree(omega); cudaFree(fibm); cudaFree(err); cudaFree(scratch);
+    cudaFree(side[0]); cudaFree(side[1]); cudaFree(omega); cudaFree(fibm); cudaFree(err); cudaFree(scratch); cudaFree(red_scratch);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -200,7 +200,9 @@ vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) {
     void* p;
     if ((st = alloc_dev(s, &p, (size_t)s->Q * N * s->store_bytes)) != VLBM_OK) { delete s; return st; }
     s->pop = p;
-    if ((st = alloc_dev(s, &p, N)) != VLBM_OK) { delete s; return st; }
+    // class bytes padded to whole 32-bit words (the IBM marks nodes with atomicOr on words)
+    const size_t cls_bytes = (N + 3) & ~(size_t)3;
+    if ((st = alloc_dev(s, &p, cls_bytes)) != VLBM_OK) { delete s; return st; }
     s->cls = static_cast<uint8_t*>(p);
     if ((st = alloc_dev(s, &p, N * sizeof(int32_t))) != VLBM_OK) { delete s; return st; }
     s->bc_slot = static_cast<int32_t*>(p);
@@ -210,7 +212,7 @@ vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) {
         if ((st = alloc_dev(s, &p, N * sizeof(float))) != VLBM_OK) { delete s; return st; }
         s->omega = static_cast<float*>(p);
     }
-    cudaMemsetAsync(s->cls, 0, N, s->stream);
+    cudaMemsetAsync(s->cls, 0, cls_bytes, s->stream);
     cudaMemsetAsync(s->bc_slot, 0xff, N * sizeof(int32_t), s->stream);
     cudaMemsetAsync(s->err, 0, sizeof(unsigned int), s->stream);
     st = vlbm_init_equilibrium(s, cfg->rho0, 0.0, 0.0, 0.0);
@@ -388,6 +390,7 @@ vlbm_status vlbm_get_info(vlbm_sim* s, vlbm_info* info) {
     info->device_bytes = (int64_t)s->device_bytes;
     info->bytes_per_node_step = 2.0 * s->Q * s->store_bytes;
     info->last_kernel_variant = s->variant;
+    ibm_counts(s, &info->n_particles, &info->n_lagrangian_nodes);
     return VLBM_OK;
 }
 

@@ -1,17 +1,830 @@
-// ibm.cu -- immersed-boundary step for movable spheres.
+// ibm.cu -- immersed-boundary step for movable spheres on the GPU.
+//
+// The reference (src/CUDA/IBM/ibm.cu:6-192) runs, after every fluid step, ~9 +
+// 4*IBM_MAX_ITERATION host-synchronised launches, two of which sweep the whole
+// lattice (gpuUpdateMacrIBM recomputes rho,u everywhere; gpuEulerSumIBMAuxsReset
+// adds the auxiliary fields everywhere, once per iteration).  Here only the
+// Eulerian nodes inside each sphere's stencil support are touched:
+//
+//   k_ibm_box        one CTA per sphere: unwrapped node extent -> Eulerian box,
+//                    node forces reset (gpuResetNodesForces ibm.cu:651-668)
+//   k_ibm_gather     one CTA per sphere: rho,u of the post-boundary populations
+//                    with the constant body force (gpuUpdateMacrIBM ibm.cu:544-648)
+//                    for the box nodes, written to dense fields; each node is
+//                    appended once to a compact list (atomicOr on its class bit)
+//   k_ibm_contacts   one CTA: old values, Hertz-Mindlin contacts with
+//                    deterministic slot updates and sums, predictor
+//   per multi-direct-forcing iteration:
+//     k_ibm_interp_spread  one CTA per sphere: the box's rho,u staged in shared
+//                    memory, Peskin 4-point interpolation, direct forcing, the
+//                    spread accumulated in shared memory and flushed once with
+//                    global atomics; sphere force/torque by block reduction
+//     k_ibm_update   particle velocity/rotation update
+//     k_ibm_euler    over the node list: u += fAux/(2 rho), F += fAux, fAux = 0
+//   k_ibm_move / k_ibm_move_nodes   particle and Lagrangian node movement
+//
+// Particle state, contacts and integration are FP64; the Eulerian fields FP32.
 #include <cuda_runtime.h>
+#include <cmath>
+#include <cstring>
+#include <vector>
 #include "sim.h"
+#include "step_impl.cuh"
 
 namespace vlbm {
 
-struct IbmState {
-    int dummy_unused = 0;
+constexpr int IBM_MAX_SLOTS = 13;           // MAX_ACTIVE_COLLISIONS, ibmBoundaryCondition.h:78
+constexpr int IBM_THREADS = 256;
+constexpr int IBM_SMEM_MAX_NODES = 13312;   // 13312 * 16 B = 208 KB of staged rho,u
+constexpr int IBM_MAX_PARTICLES = 1024;   // pair buffer np*np*6 doubles <= 50 MB
+
+struct DPart {
+    double pos[3], pos_old[3], vel[3], vel_old[3], w[3], w_avg[3], w_old[3], w_pos[3];
+    double f[3], f_old[3], M[3], M_old[3], I[6], dP[3], dL[3];
+    double S, radius, volume, density;
+    int movable, node_begin, node_count, pad;
+    int partner[IBM_MAX_SLOTS], last[IBM_MAX_SLOTS];
+    double tdisp[IBM_MAX_SLOTS][3];
+    int box_lo[3], box_n[3];
 };
 
-vlbm_status ibm_step(vlbm_sim*) { return VLBM_OK; }
-vlbm_status ibm_macroscopics_fixup(vlbm_sim*, float*, float*, float*, float*) { return VLBM_OK; }
-void ibm_destroy(IbmState* st) { delete st; }
-void ibm_reset(vlbm_sim*) {}
+struct IbmParams {
+    int np, nnodes;
+    int nx, ny, nz;
+    int wall[3];
+    double alpha, rho_f, g[3], thickness;
+    double ss_n, sw_n, ss_t, sw_t, dpp, dpw, mu_pp, mu_pw;
+    float fx, fy, fz;
+    int step;
+};
+
+struct IbmState {
+    vlbm_ibm_config cfg{};
+    IbmParams prm{};
+    int np = 0, nnodes = 0;
+    DPart* parts = nullptr;
+    double *nx = nullptr, *ny = nullptr, *nz = nullptr, *nS = nullptr;
+    double *nfx = nullptr, *nfy = nullptr, *nfz = nullptr, *ndx = nullptr, *ndy = nullptr, *ndz = nullptr;
+    int* npid = nullptr;
+    float* fields = nullptr;      // [4][N] rho,ux,uy,uz (IBM macroscopics) + [3][N] fAux
+    int* list = nullptr;          // [N] touched Eulerian nodes
+    int* count = nullptr;
+    double* contrib = nullptr;    // [np][np][6] pair force/torque on the row particle
+    int smem_nodes = 0;           // staged box capacity of k_ibm_interp_spread
+    std::vector<DPart> initial;   // for vlbm_init_equilibrium
+    std::vector<double> init_nodes;
+    size_t bytes = 0;
+};
+
+__device__ __forceinline__ double pdelta(double d, double L) {
+    if (fabs(d) > L / 2.0) d = d < 0 ? d + L : d - L;
+    return d;
+}
+__device__ __forceinline__ void dcross(const double a[3], const double b[3], double o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ int wrapi(int v, int n) { v %= n; return v < 0 ? v + n : v; }
+
+// Peskin 4-point kernel (ibmGlobalFunctions.h:28-48, STENCIL_4)
+__device__ __forceinline__ float stencil4(float x) {
+    const float a = fabsf(x);
+    if (a <= 1.f) return 0.125f * (3.f - 2.f * a + sqrtf(1.f + 4.f * a - 4.f * a * a));
+    if (a <= 2.f) return 0.125f * (5.f - 2.f * a - sqrtf(-7.f + 12.f * a - 4.f * a * a));
+    return 0.f;
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w];
+    return s;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------- box --
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_box(IbmParams P, DPart* parts, const double* X, const double* Y,
+                                                          const double* Z, double* fx, double* fy, double* fz,
+                                                          double* dx, double* dy, double* dz) {
+    __shared__ double sh[32];
+    DPart& p = parts[blockIdx.x];
+    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
+    const int Li[3] = {P.nx, P.ny, P.nz};
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int k = threadIdx.x; k < p.node_count; k += blockDim.x) {
+        const int j = p.node_begin + k;
+        const double q[3] = {X[j], Y[j], Z[j]};
+        for (int a = 0; a < 3; ++a) {
+            const double u = P.wall[a] ? q[a] : p.pos[a] + pdelta(q[a] - p.pos[a], L[a]);
+            mn[a] = fmin(mn[a], u);
+            mx[a] = fmax(mx[a], u);
+        }
+        fx[j] = fy[j] = fz[j] = 0.0;
+        dx[j] = dy[j] = dz[j] = 0.0;
+    }
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    // min/max block reductions
+    for (int a = 0; a < 3; ++a) {
+        double v = mn[a];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+        double w = mx[a];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_down_sync(0xffffffffu, w, o));
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) { sh[threadIdx.x >> 5] = v; sh[16 + (threadIdx.x >> 5)] = w; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a1 = 1e300, a2 = -1e300;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a1 = fmin(a1, sh[k]); a2 = fmax(a2, sh[16 + k]); }
+            lo[a] = a1;
+            hi[a] = a2;
+        }
+    }
+    if (threadIdx.x == 0) {
+        for (int a = 0; a < 3; ++a) {
+            // stencil of a node at x covers int(x)-1 .. int(x)+2 (ibm.cu:236-240).
+            // Extents are clamped in double before any integer conversion so a
+            // diverged (non-finite or far-away) sphere yields an empty or
+            // axis-sized box, never an out-of-range one.
+            int l, h;
+            const double La = (double)Li[a];
+            if (!isfinite(lo[a]) || !isfinite(hi[a])) {
+                l = 0; h = -1;
+            } else if (P.wall[a]) {
+                const double cl = fmin(fmax(lo[a], -4.0), La + 4.0), ch = fmin(fmax(hi[a], -4.0), La + 4.0);
+                l = (int)floor(cl) - 1;
+                h = (int)ch + 2;
+                if (l < 0) l = 0;
+                if (h > Li[a] - 1) h = Li[a] - 1;
+            } else if (hi[a] - lo[a] + 5.0 >= La) {
+                l = 0; h = Li[a] - 1;
+            } else {
+                l = (int)floor(lo[a]) - 1;
+                h = (int)floor(hi[a]) + 3;   // +1: truncated bases of negative coordinates
+            }
+            p.box_lo[a] = l;
+            p.box_n[a] = h >= l ? h - l + 1 : 0;
+        }
+    }
+}
+
+// -------------------------------------------------------------- gather --
+template <int Q, int ST, bool ODD>
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmParams P, const DPart* parts,
+                                                             float* fields, int* list, int* count) {
+    const DPart& p = parts[blockIdx.x];
+    const int bx = p.box_n[0], by = p.box_n[1], bz = p.box_n[2];
+    const long long tot = (long long)bx * by * bz;
+    const size_t N = (size_t)sp.N;
+    for (long long k = threadIdx.x; k < tot; k += blockDim.x) {
+        const int ix = (int)(k % bx), iy = (int)((k / bx) % by), iz = (int)(k / ((long long)bx * by));
+        const int x = wrapi(p.box_lo[0] + ix, P.nx), y = wrapi(p.box_lo[1] + iy, P.ny), z = wrapi(p.box_lo[2] + iz, P.nz);
+        const unsigned n = (unsigned)(((size_t)z * P.ny + y) * P.nx + x);
+        Nbr nb;
+        nb.init(x, y, z, sp.nx, sp.ny, sp.nz);
+        float f[Q];
+        uint8_t cls;
+        gather<Q, ST, ODD>(sp, n, nb, x, y, z, f, cls);
+        const Mom m = moments<Q, false>(f, P.fx, P.fy, P.fz);
+        fields[n] = m.rho;
+        fields[N + n] = m.ux;
+        fields[2 * N + n] = m.uy;
+        fields[3 * N + n] = m.uz;
+        unsigned* word = reinterpret_cast<unsigned*>(sp.cls + (n & ~3u));
+        const unsigned bit = (unsigned)NODE_IBM_SET << (8u * (n & 3u));
+        if (!(atomicOr(word, bit) & bit)) list[atomicAdd(count, 1)] = (int)n;
+    }
+}
+
+// ------------------------------------------------------------- contacts --
+__device__ int wall_index(const double n[3]) {  // calculateWallIndex ibmCollision.cu:5-19
+    return 7 + (1 - (int)n[0]) - 2 * (1 - (int)n[1]) - 3 * (1 - (int)n[2]);
+}
+__device__ void upd(DPart& p, int idx, const double d[3], int step, double out[3]) {
+    if (idx < 0) { out[0] = d[0]; out[1] = d[1]; out[2] = d[2]; return; }
+    for (int a = 0; a < 3; ++a) p.tdisp[idx][a] += d[a];
+    p.last[idx] = step;
+    for (int a = 0; a < 3; ++a) out[a] = p.tdisp[idx][a];
+}
+
+// sphereWallCollision ibmCollision.cu:393-508
+__device__ void wall_contact(const IbmParams& P, DPart& p, const double wn[3], double disp, double accF[3],
+                             double accM[3]) {
+    const int step = P.step;
+    const double m = p.volume * p.density, r = p.radius;
+    const double n[3] = {-wn[0], -wn[1], -wn[2]};
+    const double* G = p.vel;
+    const double kn = P.sw_n * sqrt(fabs(r));
+    const double kt = P.sw_t * sqrt(r) * sqrt(fabs(disp));
+    const double etan = P.dpw * sqrt(m * kn), etat = P.dpw * sqrt(m * kt);
+    const double fkn = -kn * sqrt(fabs(disp * disp * disp));
+    const double Gn = G[0] * n[0] + G[1] * n[1] + G[2] * n[2];
+    const double q = pow(fabs(disp), 0.25);
+    double fnv[3];
+    for (int a = 0; a < 3; ++a) fnv[a] = fkn * n[a] - etan * Gn * n[a] * q;
+    const double fn = sqrt(fnv[0] * fnv[0] + fnv[1] * fnv[1] + fnv[2] * fnv[2]);
+    double wxn[3];
+    dcross(p.w, n, wxn);
+    double Gct[3];
+    for (int a = 0; a < 3; ++a) Gct[a] = G[a] + r * wxn[a] - Gn * n[a];
+    double mag = sqrt(Gct[0] * Gct[0] + Gct[1] * Gct[1] + Gct[2] * Gct[2]);
+    double t[3] = {0, 0, 0};
+    if (mag != 0) for (int a = 0; a < 3; ++a) t[a] = Gct[a] / mag;
+    const int idx = wall_index(n);
+    double td[3];
+    if (step - p.last[idx] > 1) {
+        p.tdisp[idx][0] = p.tdisp[idx][1] = p.tdisp[idx][2] = 0.0;
+        p.last[idx] = step;
+        for (int a = 0; a < 3; ++a) td[a] = Gct[a];
+    } else {
+        upd(p, idx, Gct, step, td);
+    }
+    double ft[3];
+    for (int a = 0; a < 3; ++a) ft[a] = -kt * td[a] - etat * Gct[a] * pow(fabs(td[a]), 0.25);
+    mag = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+    if (mag > P.mu_pw * fabs(fn)) {
+        const double mg[3] = {-Gct[0], -Gct[1], -Gct[2]};
+        upd(p, idx, mg, step, td);
+        for (int a = 0; a < 3; ++a) ft[a] = -P.mu_pw * fn * t[a];
+    }
+    double nxf[3];
+    dcross(n, ft, nxf);
+    for (int a = 0; a < 3; ++a) { accF[a] += fnv[a] + ft[a]; accM[a] += r * nxf[a]; }
+}
+
+// sphereSphereCollision ibmCollision.cu:1718-1913; slots kept in the lower
+// index i, so one thread per i serialises all slot updates of that particle.
+__device__ void pair_contact(const IbmParams& P, DPart& pi, const DPart& pj, int j, double accF[3], double accM[3],
+                             double* out6) {
+    const int step = P.step;
+    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
+    double d[3];
+    for (int a = 0; a < 3; ++a) {
+        d[a] = pi.pos[a] - pj.pos[a];
+        if (!P.wall[a]) d[a] = pdelta(d[a], L[a]);
+    }
+    const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (dist > pi.radius + pj.radius) return;
+    const double n[3] = {d[0] / dist, d[1] / dist, d[2] / dist};
+    const double disp = pi.radius + pj.radius - dist;
+    const double G[3] = {pi.vel[0] - pj.vel[0], pi.vel[1] - pj.vel[1], pi.vel[2] - pj.vel[2]};
+    const double mi = pi.volume * pi.density, mj = pj.volume * pj.density;
+    const double reff = 1.0 / ((pi.radius + pj.radius) / (pi.radius * pj.radius));
+    const double meff = 1.0 / ((mi + mj) / (mi * mj));
+    const double kn = P.ss_n * sqrt(reff);
+    const double kt = P.ss_t * sqrt(reff) * sqrt(fabs(disp));
+    const double etan = P.dpp * sqrt(meff * kn), etat = P.dpp * sqrt(meff * kt);
+    const double fkn = -kn * sqrt(fabs(disp * disp * disp));
+    const double Gn = G[0] * n[0] + G[1] * n[1] + G[2] * n[2];
+    const double q = pow(fabs(disp), 0.25);
+    double fnv[3];
+    for (int a = 0; a < 3; ++a) fnv[a] = fkn * n[a] - etan * Gn * n[a] * q;
+    const double fn = sqrt(fnv[0] * fnv[0] + fnv[1] * fnv[1] + fnv[2] * fnv[2]);
+    double wi[3], wj[3];
+    dcross(pi.w, n, wi);
+    dcross(pj.w, n, wj);
+    double Gct[3];
+    for (int a = 0; a < 3; ++a) Gct[a] = G[a] + pi.radius * wi[a] + pj.radius * wj[a] - Gn * n[a];
+    double mag = sqrt(Gct[0] * Gct[0] + Gct[1] * Gct[1] + Gct[2] * Gct[2]);
+    double t[3] = {0, 0, 0};
+    if (mag != 0) for (int a = 0; a < 3; ++a) t[a] = Gct[a] / mag;
+    double td[3];
+    int idx = -1;
+    for (int s = 7; s < IBM_MAX_SLOTS; ++s)
+        if (pi.partner[s] == j && step - pi.last[s] <= 1) { idx = s; break; }
+    if (idx == -1) {
+        // startCollision (ibmCollision.cu:32-53); ended contacts free their slot
+        for (int s = 7; s < IBM_MAX_SLOTS; ++s)
+            if (pi.last[s] == -1 || step - pi.last[s] > 1) {
+                pi.partner[s] = j;
+                pi.tdisp[s][0] = pi.tdisp[s][1] = pi.tdisp[s][2] = 0.0;
+                pi.last[s] = step;
+                idx = s;
+                break;
+            }
+        for (int a = 0; a < 3; ++a) td[a] = Gct[a];
+    } else {
+        upd(pi, idx, G, step, td);  // the reference accumulates G here (ibmCollision.cu:1851)
+    }
+    double ft[3];
+    for (int a = 0; a < 3; ++a) ft[a] = -kt * td[a] - etat * Gct[a] * pow(fabs(td[a]), 0.25);
+    mag = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+    if (mag > P.mu_pp * fabs(fn)) {
+        const double mg[3] = {-Gct[0], -Gct[1], -Gct[2]};
+        upd(pi, idx, mg, step, td);
+        for (int a = 0; a < 3; ++a) ft[a] = -P.mu_pp * fn * t[a];
+    }
+    double nxf[3];
+    dcross(n, ft, nxf);
+    for (int a = 0; a < 3; ++a) {
+        const double fd = fnv[a] + ft[a];
+        accF[a] -= fd;
+        accM[a] += pi.radius * nxf[a];
+        out6[a] += fd;
+        out6[3 + a] += pj.radius * nxf[a];
+    }
+}
+
+// gpuUpdateParticleCenterVelocityAndRotation ibm.cu:755-897
+__device__ void update_center(const IbmParams& P, DPart& p) {
+    if (!p.movable) return;
+    const double al = P.alpha;
+    const double inv_v = 1.0 / p.volume;
+    for (int a = 0; a < 3; ++a)
+        p.vel[a] = p.vel_old[a] + ((p.f_old[a] * (1.0 - al) + p.f[a] * al + p.dP[a]) * inv_v +
+                                   (p.density - P.rho_f) * P.g[a]) / p.density;
+    const double Ixx = p.I[0], Iyy = p.I[1], Izz = p.I[2], Ixy = p.I[3], Ixz = p.I[4], Iyz = p.I[5];
+    const double det = Izz * Ixy * Ixy + Iyy * Ixz * Ixz + Ixx * Iyz * Iyz - Ixx * Iyy * Izz - 2 * Ixy * Ixz * Iyz;
+    const double inv = 1.0 / det;
+    double wa[3], LM[3];
+    for (int a = 0; a < 3; ++a) {
+        wa[a] = p.w_old[a] * (1.0 - al) + p.w_old[a] * al;
+        LM[a] = p.dL[a] + (p.M[a] * al + p.M_old[a] * (1.0 - al));
+    }
+    const double Lx = Ixx * wa[0] + Ixy * wa[1] + Ixz * wa[2];
+    const double Ly = Ixy * wa[0] + Iyy * wa[1] + Iyz * wa[2];
+    const double Lz = Ixz * wa[0] + Iyz * wa[1] + Izz * wa[2];
+    const double bx = LM[0] + wa[2] * Ly - wa[1] * Lz;
+    const double by = LM[1] + wa[0] * Lz - wa[2] * Lx;
+    const double bz = LM[2] + wa[1] * Lx - wa[0] * Ly;
+    double wn[3];
+    wn[0] = p.w_old[0] + ((Iyz * Iyz - Iyy * Izz) * bx - (Ixy * Iyz - Ixz * Iyy) * bz - (Ixz * Iyz - Ixy * Izz) * by) * inv;
+    wn[1] = p.w_old[1] + ((Ixz * Ixz - Ixx * Izz) * by - (Ixy * Ixz - Ixx * Iyz) * bz - (Ixz * Iyz - Ixy * Izz) * bx) * inv;
+    wn[2] = p.w_old[2] + ((Ixy * Ixy - Ixx * Iyy) * bz - (Ixy * Ixz - Ixx * Iyz) * by - (Ixy * Iyz - Ixz * Iyy) * bx) * inv;
+    const double th = sqrt(wa[0] * wa[0] + wa[1] * wa[1] + wa[2] * wa[2]);
+    if (th > 0.0 && isfinite(1.0 / th)) {  // I <- R I R^T, R of the quaternion of w_avg
+        const double h = sin(th / 2.0) / th;
+        const double qw = cos(th / 2.0), qx = wa[0] * h, qy = wa[1] * h, qz = wa[2] * h;
+        const double R[3][3] = {
+            {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)},
+            {2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)},
+            {2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)}};
+        const double M3[3][3] = {{Ixx, Ixy, Ixz}, {Ixy, Iyy, Iyz}, {Ixz, Iyz, Izz}};
+        double T[3][3], O[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                double s = 0;
+                for (int c = 0; c < 3; ++c) s += R[a][c] * M3[c][b];
+                T[a][b] = s;
+            }
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                double s = 0;
+                for (int c = 0; c < 3; ++c) s += T[a][c] * R[b][c];
+                O[a][b] = s;
+            }
+        p.I[0] = O[0][0]; p.I[1] = O[1][1]; p.I[2] = O[2][2];
+        p.I[3] = O[0][1]; p.I[4] = O[0][2]; p.I[5] = O[1][2];
+    }
+    for (int a = 0; a < 3; ++a) p.w[a] = wn[a];
+}
+
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_contacts(IbmParams P, DPart* parts, double* contrib) {
+    const int np = P.np;
+    // gpuUpdateParticleOldValues ibm.cu:995-1042
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        DPart& p = parts[i];
+        for (int a = 0; a < 3; ++a) {
+            p.dP[a] = 0; p.dL[a] = 0;
+            p.pos_old[a] = p.pos[a]; p.vel_old[a] = p.vel[a]; p.w_old[a] = p.w[a];
+            p.f_old[a] = p.f[a]; p.f[a] = 0; p.M[a] = 0;
+        }
+    }
+    __syncthreads();
+    // contacts: thread i owns particle i's slots and its walls
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        DPart& pi = parts[i];
+        double F[3] = {0, 0, 0}, Mo[3] = {0, 0, 0};
+        for (int j = i + 1; j < np; ++j) {
+            double* o = contrib + ((size_t)i * np + j) * 6;
+            for (int a = 0; a < 6; ++a) o[a] = 0.0;
+            if (!pi.movable && !parts[j].movable) continue;
+            pair_contact(P, pi, parts[j], j, F, Mo, o);
+        }
+        if (pi.movable) {
+            const int Li[3] = {P.nx, P.ny, P.nz};
+            for (int a = 0; a < 3; ++a) {
+                if (!P.wall[a]) continue;
+                double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+                lo[a] = 1;
+                hi[a] = -1;
+                const double dlo = pi.pos[a];
+                if (dlo < pi.radius) wall_contact(P, pi, lo, pi.radius - dlo, F, Mo);
+                const double dhi = (Li[a] - 1) - pi.pos[a];
+                if (dhi < pi.radius) wall_contact(P, pi, hi, pi.radius - dhi, F, Mo);
+            }
+        }
+        for (int a = 0; a < 3; ++a) { pi.f[a] += F[a]; pi.M[a] += Mo[a]; }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < np; j += blockDim.x) {
+        DPart& pj = parts[j];
+        for (int i = 0; i < j; ++i) {
+            const double* o = contrib + ((size_t)i * np + j) * 6;
+            for (int a = 0; a < 3; ++a) { pj.f[a] += o[a]; pj.M[a] += o[3 + a]; }
+        }
+        update_center(P, pj);  // predictor (ibm.cu:98-103)
+    }
+}
+
+// -------------------------------------------------- interpolation/spread --
+// Stencil of one Lagrangian node: base index and validity range per axis.
+struct NodeStencil {
+    int base[3], lo[3], hi[3];
+    float w[3][4];
+    bool skip;
+};
+
+__device__ __forceinline__ NodeStencil node_stencil(const IbmParams& P, const DPart& p, double X, double Y, double Z) {
+    NodeStencil s;
+    const double pos[3] = {X, Y, Z};
+    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
+    const int Li[3] = {P.nx, P.ny, P.nz};
+    s.skip = false;
+    for (int a = 0; a < 3; ++a) {
+        double xu = P.wall[a] ? pos[a] : p.pos[a] + pdelta(pos[a] - p.pos[a], L[a]);
+        if (!(fabs(xu) < 4.0 * L[a] + 8.0)) {  // non-finite or diverged position: no stencil
+            s.skip = true;
+            xu = 0.0;
+        }
+        // int(x) - P_DIST + 1 of the stored coordinate (ibm.cu:236-240): truncation,
+        // which differs from floor for the negative coordinates a sphere's nodes
+        // have across x=0 before their first movement wraps them; for periodic
+        // axes the base is then shifted into the sphere-centred frame
+        const double raw = s.skip ? 0.0 : pos[a];
+        const int braw = (int)raw - 1;
+        const double fr_raw = raw - (double)braw;
+        if (P.wall[a]) {
+            s.base[a] = braw;
+        } else {
+            const int k = (int)rint((xu - raw) / L[a]);
+            s.base[a] = braw + k * Li[a];
+        }
+        s.lo[a] = 0;
+        s.hi[a] = 3;
+        if (P.wall[a]) {
+            s.hi[a] = (s.base[a] + 3 < Li[a]) ? 3 : (Li[a] - 1 - s.base[a]);
+            s.lo[a] = (s.base[a] >= 0) ? 0 : -s.base[a];
+        }
+        if (s.hi[a] <= 0 || s.lo[a] >= 4) s.skip = true;  // ibm.cu:300-305
+        const float fr = (float)fr_raw;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) s.w[a][j] = stencil4((float)j - fr);
+    }
+    return s;
+}
+
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_interp_spread(IbmParams P, DPart* parts, const double* X,
+                                                                    const double* Y, const double* Z, const double* S,
+                                                                    double* nfx, double* nfy, double* nfz, double* ndx,
+                                                                    double* ndy, double* ndz, float* fields, int smem_nodes) {
+    extern __shared__ float sm[];
+    __shared__ double red[32];
+    DPart& p = parts[blockIdx.x];
+    const size_t N = (size_t)P.nx * P.ny * P.nz;
+    const int bx = p.box_n[0], by = p.box_n[1], bz = p.box_n[2];
+    const int tot = bx * by * bz;
+    const bool staged = tot <= smem_nodes;
+    const float* rho_g = fields;
+    const float* ux_g = fields + N;
+    const float* uy_g = fields + 2 * N;
+    const float* uz_g = fields + 3 * N;
+    float* faux = fields + 4 * N;
+    auto gidx = [&](int ix, int iy, int iz) -> size_t {
+        const int x = wrapi(p.box_lo[0] + ix, P.nx), y = wrapi(p.box_lo[1] + iy, P.ny), z = wrapi(p.box_lo[2] + iz, P.nz);
+        return ((size_t)z * P.ny + y) * P.nx + x;
+    };
+    if (staged) {  // stage rho,u of the box (x fastest: coalesced rows)
+        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
+            const int ix = k % bx, iy = (k / bx) % by, iz = k / (bx * by);
+            const size_t g = gidx(ix, iy, iz);
+            sm[k] = rho_g[g];
+            sm[tot + k] = ux_g[g];
+            sm[2 * tot + k] = uy_g[g];
+            sm[3 * tot + k] = uz_g[g];
+        }
+    }
+    __syncthreads();
+    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
+    double accF[3] = {0, 0, 0}, accM[3] = {0, 0, 0};
+    const int nb = p.node_count;
+    // interpolation and direct forcing (ibm.cu:307-475)
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        const int j = p.node_begin + k;
+        const NodeStencil st = node_stencil(P, p, X[j], Y[j], Z[j]);
+        if (st.skip) { ndx[j] = ndy[j] = ndz[j] = 0.0; continue; }
+        float rho = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
+        for (int zk = st.lo[2]; zk <= st.hi[2]; ++zk)
+            for (int yj = st.lo[1]; yj <= st.hi[1]; ++yj) {
+                const float wzy = st.w[2][zk] * st.w[1][yj];
+                for (int xi = st.lo[0]; xi <= st.hi[0]; ++xi) {
+                    const float d = wzy * st.w[0][xi];
+                    // inside [0, box) by construction; the wrap matters only when a
+                    // periodic axis is shorter than the box and the box spans it
+                    const int ix = wrapi(st.base[0] + xi - p.box_lo[0], bx),
+                              iy = wrapi(st.base[1] + yj - p.box_lo[1], by),
+                              iz = wrapi(st.base[2] + zk - p.box_lo[2], bz);
+                    if (staged) {
+                        const int b = (iz * by + iy) * bx + ix;
+                        rho += sm[b] * d; ux += sm[tot + b] * d; uy += sm[2 * tot + b] * d; uz += sm[3 * tot + b] * d;
+                    } else {
+                        const size_t g = gidx(ix, iy, iz);
+                        rho += rho_g[g] * d; ux += ux_g[g] * d; uy += uy_g[g] * d; uz += uz_g[g] * d;
+                    }
+                }
+            }
+        double dr[3] = {X[j] - p.pos[0], Y[j] - p.pos[1], Z[j] - p.pos[2]};
+        for (int a = 0; a < 3; ++a)
+            if (!P.wall[a]) dr[a] = pdelta(dr[a], L[a]);
+        double uc[3] = {0, 0, 0};
+        if (p.movable) {
+            double wxr[3];
+            dcross(p.w, dr, wxr);
+            for (int a = 0; a < 3; ++a) uc[a] = p.vel[a] + wxr[a];
+        }
+        const double aux = 2.0 * (double)rho * S[j] * P.thickness;
+        const double dF[3] = {aux * ((double)ux - uc[0]), aux * ((double)uy - uc[1]), aux * ((double)uz - uc[2])};
+        nfx[j] += dF[0]; nfy[j] += dF[1]; nfz[j] += dF[2];
+        ndx[j] = dF[0]; ndy[j] = dF[1]; ndz[j] = dF[2];
+        double m[3];
+        dcross(dr, dF, m);
+        for (int a = 0; a < 3; ++a) { accF[a] += dF[a]; accM[a] += m[a]; }
+    }
+    __syncthreads();
+    if (staged)
+        for (int k = threadIdx.x; k < 3 * tot; k += blockDim.x) sm[k] = 0.f;
+    __syncthreads();
+    // spreading: fAux -= dF * delta (ibm.cu:478-512)
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        const int j = p.node_begin + k;
+        const NodeStencil st = node_stencil(P, p, X[j], Y[j], Z[j]);
+        if (st.skip) continue;
+        const float dF[3] = {(float)ndx[j], (float)ndy[j], (float)ndz[j]};
+        for (int zk = st.lo[2]; zk <= st.hi[2]; ++zk)
+            for (int yj = st.lo[1]; yj <= st.hi[1]; ++yj) {
+                const float wzy = st.w[2][zk] * st.w[1][yj];
+                for (int xi = st.lo[0]; xi <= st.hi[0]; ++xi) {
+                    const float d = wzy * st.w[0][xi];
+                    // inside [0, box) by construction; the wrap matters only when a
+                    // periodic axis is shorter than the box and the box spans it
+                    const int ix = wrapi(st.base[0] + xi - p.box_lo[0], bx),
+                              iy = wrapi(st.base[1] + yj - p.box_lo[1], by),
+                              iz = wrapi(st.base[2] + zk - p.box_lo[2], bz);
+                    if (staged) {
+                        const int b = (iz * by + iy) * bx + ix;
+                        atomicAdd(&sm[b], -dF[0] * d);
+                        atomicAdd(&sm[tot + b], -dF[1] * d);
+                        atomicAdd(&sm[2 * tot + b], -dF[2] * d);
+                    } else {
+                        const size_t g = gidx(ix, iy, iz);
+                        atomicAdd(&faux[g], -dF[0] * d);
+                        atomicAdd(&faux[N + g], -dF[1] * d);
+                        atomicAdd(&faux[2 * N + g], -dF[2] * d);
+                    }
+                }
+            }
+    }
+    __syncthreads();
+    if (staged) {  // one flush of the box into the global auxiliary field
+        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
+            const float a0 = sm[k], a1 = sm[tot + k], a2 = sm[2 * tot + k];
+            if (a0 == 0.f && a1 == 0.f && a2 == 0.f) continue;
+            const int ix = k % bx, iy = (k / bx) % by, iz = k / (bx * by);
+            const size_t g = gidx(ix, iy, iz);
+            atomicAdd(&faux[g], a0);
+            atomicAdd(&faux[N + g], a1);
+            atomicAdd(&faux[2 * N + g], a2);
+        }
+    }
+    // sphere force and torque: block sums, one writer per sphere (ibm.cu:526-541)
+    double tot6[6];
+    for (int a = 0; a < 3; ++a) { tot6[a] = block_sum(accF[a], red); tot6[3 + a] = block_sum(accM[a], red); }
+    if (threadIdx.x == 0)
+        for (int a = 0; a < 3; ++a) { p.f[a] += tot6[a]; p.M[a] += tot6[3 + a]; }
+}
+
+__global__ void k_ibm_update(IbmParams P, DPart* parts) {
+    for (int i = threadIdx.x; i < P.np; i += blockDim.x) update_center(P, parts[i]);
+}
+
+// gpuEulerSumIBMAuxsReset restricted to the touched nodes
+__global__ void k_ibm_euler(IbmParams P, float* fields, float* fibm, uint8_t* cls, const int* list, const int* count) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *count) return;
+    const size_t N = (size_t)P.nx * P.ny * P.nz;
+    const int n = list[k];
+    float* faux = fields + 4 * N;
+    const float rho = fields[n];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float v = faux[a * N + n];
+        fields[(1 + a) * N + n] += 0.5f * v / rho;
+        fibm[a * N + n] += v;
+        faux[a * N + n] = 0.f;
+    }
+    cls[n] = cls[n] | NODE_IBM_FORCE;
+}
+
+// gpuParticleMovement ibm.cu:899-993
+__global__ void k_ibm_move(IbmParams P, DPart* parts) {
+    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
+    for (int i = threadIdx.x; i < P.np; i += blockDim.x) {
+        DPart& p = parts[i];
+        if (!p.movable) continue;
+        for (int a = 0; a < 3; ++a) {
+            const double dx = p.vel[a] * P.alpha + p.vel_old[a] * (1.0 - P.alpha);
+            if (P.wall[a]) p.pos[a] += dx;
+            else p.pos[a] = fmod(p.pos[a] + dx + L[a], L[a]);
+            p.w_avg[a] = p.w[a] * P.alpha + p.w_old[a] * (1.0 - P.alpha);
+            p.w_pos[a] += p.w_avg[a];
+        }
+    }
+}
+
+// gpuParticleNodeMovement ibm.cu:1044-1197
+__global__ void k_ibm_move_nodes(IbmParams P, const DPart* parts, const int* pid, double* X, double* Y, double* Z) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.nnodes) return;
+    const DPart& p = parts[pid[k]];
+    if (!p.movable) return;
+    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
+    double* Pp[3] = {&X[k], &Y[k], &Z[k]};
+    const double wn = sqrt(p.w_avg[0] * p.w_avg[0] + p.w_avg[1] * p.w_avg[1] + p.w_avg[2] * p.w_avg[2]);
+    if (wn <= 1e-8) {
+        for (int a = 0; a < 3; ++a) {
+            double d = p.pos[a] - p.pos_old[a];
+            if (P.wall[a]) { *Pp[a] += d; continue; }
+            if (fabs(d) > L[a] / 2.0) d = (p.pos[a] < p.pos_old[a]) ? p.pos[a] + L[a] - p.pos_old[a] : p.pos[a] - L[a] - p.pos_old[a];
+            *Pp[a] = fmod(*Pp[a] + d + L[a], L[a]);
+        }
+        return;
+    }
+    double v[3];
+    for (int a = 0; a < 3; ++a) {
+        if (!P.wall[a] && fabs(*Pp[a] - p.pos_old[a]) > L[a] / 2.0) *Pp[a] += (*Pp[a] < p.pos_old[a]) ? L[a] : -L[a];
+        v[a] = *Pp[a] - p.pos_old[a];
+    }
+    const double q0 = cos(0.5 * wn);
+    const double qi = (p.w_avg[0] / wn) * sin(0.5 * wn), qj = (p.w_avg[1] / wn) * sin(0.5 * wn),
+                 qk = (p.w_avg[2] / wn) * sin(0.5 * wn);
+    const double t = q0 * q0 - 0.5;
+    // rows as the reference writes them (third row: qi*qj - q0*qj, ibm.cu:1172)
+    double np3[3];
+    np3[0] = p.pos[0] + 2 * ((t + qi * qi) * v[0] + (qi * qj - q0 * qk) * v[1] + (qi * qk + q0 * qj) * v[2]);
+    np3[1] = p.pos[1] + 2 * ((qi * qj + q0 * qk) * v[0] + (t + qj * qj) * v[1] + (qj * qk - q0 * qi) * v[2]);
+    np3[2] = p.pos[2] + 2 * ((qi * qj - q0 * qj) * v[0] + (qj * qk + q0 * qi) * v[1] + (t + qk * qk) * v[2]);
+    for (int a = 0; a < 3; ++a) *Pp[a] = P.wall[a] ? np3[a] : fmod(np3[a] + L[a], L[a]);
+}
+
+__global__ void k_ibm_fixup(const float* fields, long long N, const int* list, const int* count, float* rho, float* ux,
+                            float* uy, float* uz) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *count) return;
+    const int n = list[k];
+    if (rho) rho[n] = fields[n];
+    if (ux) ux[n] = fields[N + n];
+    if (uy) uy[n] = fields[2 * N + n];
+    if (uz) uz[n] = fields[3 * N + n];
+}
+
+// ---------------------------------------------------------------- host --
+static void host_mesh(double diameter, double mesh_scale, double breugem, std::vector<double>& px,
+                      std::vector<double>& py, std::vector<double>& pz, std::vector<double>& pS) {
+    // Particle::makeSpherePolar (IBM/structs/particle.cpp:698-995), no Coulomb step
+    const double r = diameter / 2.0 - breugem;
+    const unsigned nLayer = (unsigned)(2.0 * std::sqrt(2.0) * r / mesh_scale + 1.0);
+    std::vector<unsigned> nl(nLayer + 1);
+    std::vector<double> theta(nLayer + 1), zeta(nLayer + 1), S(nLayer + 1);
+    unsigned total = 0;
+    for (unsigned i = 0; i <= nLayer; ++i) {
+        theta[i] = M_PI * ((double)i / (double)nLayer - 0.5);
+        nl[i] = (unsigned)(1.5 + std::cos(theta[i]) * nLayer * std::sqrt(3.0));
+        total += nl[i];
+        zeta[i] = r * std::sin(theta[i]);
+    }
+    for (unsigned i = 0; i < nLayer; ++i) S[i] = (zeta[i] + zeta[i + 1]) / 2.0 - zeta[0];
+    S[nLayer] = 2 * r;
+    for (unsigned i = 0; i <= nLayer; ++i) S[i] *= 2 * M_PI * r;
+    for (unsigned i = nLayer; i > 0; --i) S[i] -= S[i - 1];
+    S[0] = S[nLayer];
+    px.assign(total, 0); py.assign(total, 0); pz.assign(total, 0); pS.assign(total, 0);
+    pz[0] = r * std::sin(theta[0]);
+    pS[0] = S[0];
+    unsigned k = 1;
+    double phase = 0.0;
+    for (unsigned i = 1; i < nLayer; ++i) {
+        if (i % 2 == 1) phase += M_PI / nl[i];
+        for (unsigned j = 0; j < nl[i]; ++j, ++k) {
+            const double a = (double)j * 2.0 * M_PI / nl[i] + phase;
+            px[k] = r * std::cos(theta[i]) * std::cos(a);
+            py[k] = r * std::cos(theta[i]) * std::sin(a);
+            pz[k] = r * std::sin(theta[i]);
+            pS[k] = S[i] / nl[i];
+        }
+    }
+    pz[total - 1] = r * std::sin(theta[nLayer]);
+    pS[total - 1] = S[nLayer];
+}
+
+#define IBM_CUDA(call)                                          \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cuda_status(e_, #call);   \
+    } while (0)
+
+template <int Q, int ST>
+static cudaError_t launch_gather(vlbm_sim* s, IbmState* st) {
+    const StepParams sp = make_params(s);
+    if (s->parity == 1)
+        k_ibm_gather<Q, ST, true><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+    else
+        k_ibm_gather<Q, ST, false><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+    return cudaGetLastError();
+}
+
+static cudaError_t gather_dispatch(vlbm_sim* s, IbmState* st) {
+    const int sto = s->cfg.storage;
+    if (s->Q == 19) {
+        if (sto == VLBM_STORE_F32) return launch_gather<19, VLBM_STORE_F32>(s, st);
+        if (sto == VLBM_STORE_F16) return launch_gather<19, VLBM_STORE_F16>(s, st);
+        return launch_gather<19, VLBM_STORE_BF16>(s, st);
+    }
+    if (sto == VLBM_STORE_F32) return launch_gather<27, VLBM_STORE_F32>(s, st);
+    if (sto == VLBM_STORE_F16) return launch_gather<27, VLBM_STORE_F16>(s, st);
+    return launch_gather<27, VLBM_STORE_BF16>(s, st);
+}
+
+vlbm_status ibm_step(vlbm_sim* s) {
+    IbmState* st = s->ibm;
+    if (!st || st->np == 0) return VLBM_OK;
+    st->prm.step = (int)(s->step - 1);  // index of the fluid step just taken (main.cu:270)
+    const IbmParams& P = st->prm;
+    cudaStream_t cs = s->stream;
+    IBM_CUDA(cudaMemsetAsync(st->count, 0, sizeof(int), cs));
+    k_ibm_box<<<st->np, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nfx, st->nfy, st->nfz, st->ndx,
+                                              st->ndy, st->ndz);
+    IBM_CUDA(cudaGetLastError());
+    IBM_CUDA(gather_dispatch(s, st));
+    k_ibm_contacts<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->contrib);
+    IBM_CUDA(cudaGetLastError());
+    const size_t smem = (size_t)st->smem_nodes * 4 * sizeof(float);
+    const int euler_blocks = (int)((s->N + 255) / 256);
+    for (int it = 0; it < st->cfg.max_iterations; ++it) {
+        k_ibm_interp_spread<<<st->np, IBM_THREADS, smem, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nS, st->nfx,
+                                                               st->nfy, st->nfz, st->ndx, st->ndy, st->ndz, st->fields,
+                                                               st->smem_nodes);
+        IBM_CUDA(cudaGetLastError());
+        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts);
+        IBM_CUDA(cudaGetLastError());
+        // the list never exceeds N; launch over N's block count, threads past *count exit
+        k_ibm_euler<<<euler_blocks, 256, 0, cs>>>(P, st->fields, s->fibm, s->cls, st->list, st->count);
+        IBM_CUDA(cudaGetLastError());
+    }
+    k_ibm_move<<<1, IBM_THREADS, 0, cs>>>(P, st->parts);
+    k_ibm_move_nodes<<<(st->nnodes + 255) / 256, 256, 0, cs>>>(P, st->parts, st->npid, st->nx, st->ny, st->nz);
+    IBM_CUDA(cudaGetLastError());
+    return VLBM_OK;
+}
+
+void ibm_counts(const vlbm_sim* s, int* np, int* nn) {
+    *np = s->ibm ? s->ibm->np : 0;
+    *nn = s->ibm ? s->ibm->nnodes : 0;
+}
+
+vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz) {
+    IbmState* st = s->ibm;
+    if (!st || st->np == 0 || s->step == 0) return VLBM_OK;
+    k_ibm_fixup<<<(int)((s->N + 255) / 256), 256, 0, s->stream>>>(st->fields, s->N, st->list, st->count, rho, ux, uy, uz);
+    return cuda_status(cudaGetLastError(), "ibm macroscopics fixup");
+}
+
+void ibm_destroy(IbmState* st) {
+    if (!st) return;
+    cudaFree(st->parts);
+    for (double* p : {st->nx, st->ny, st->nz, st->nS, st->nfx, st->nfy, st->nfz, st->ndx, st->ndy, st->ndz, st->contrib})
+        cudaFree(p);
+    cudaFree(st->npid); cudaFree(st->fields); cudaFree(st->list); cudaFree(st->count);
+    delete st;
+}
+
+void ibm_reset(vlbm_sim* s) {
+    IbmState* st = s->ibm;
+    if (!st) return;
+    cudaMemcpyAsync(st->parts, st->initial.data(), st->initial.size() * sizeof(DPart), cudaMemcpyHostToDevice, s->stream);
+    const size_t nn = (size_t)st->nnodes;
+    cudaMemcpyAsync(st->nx, st->init_nodes.data(), nn * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    cudaMemcpyAsync(st->ny, st->init_nodes.data() + nn, nn * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    cudaMemcpyAsync(st->nz, st->init_nodes.data() + 2 * nn, nn * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    cudaMemsetAsync(st->fields, 0, (size_t)7 * s->N * sizeof(float), s->stream);
+    cudaMemsetAsync(st->count, 0, sizeof(int), s->stream);
+}
 
 }  // namespace vlbm
 
@@ -21,7 +834,7 @@ extern "C" {
 
 vlbm_status vlbm_ibm_config_default(vlbm_ibm_config* c) {
     if (!c) return VLBM_ERR_INVALID;
-    *c = vlbm_ibm_config{};
+    std::memset(c, 0, sizeof(*c));
     c->max_iterations = 1;       // ibmVar.h:23 IBM_MAX_ITERATION
     c->stencil = 4;              // ibmVar.h:136 STENCIL_4
     c->thickness = 1.0;          // ibmVar.h:33 IBM_THICKNESS
@@ -38,9 +851,170 @@ vlbm_status vlbm_ibm_config_default(vlbm_ibm_config* c) {
     return VLBM_OK;
 }
 
-vlbm_status vlbm_add_spheres(vlbm_sim*, const vlbm_ibm_config*, const vlbm_sphere*, int32_t) {
-    set_last_error("IBM spheres are not available in this build");
-    return VLBM_ERR_UNSUPPORTED;
+vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_sphere* sp, int32_t n) {
+    if (!s || !ib || (n > 0 && !sp)) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    IBM_CUDA(cudaSetDevice(s->device));
+    if (s->ibm) { set_last_error("spheres were already added to this simulation"); return VLBM_ERR_STATE; }
+    if (n <= 0 || n > IBM_MAX_PARTICLES) { set_last_error("sphere count must be in 1..1024"); return VLBM_ERR_INVALID; }
+    if (ib->stencil != 4) {
+        set_last_error("only the Peskin 4-point stencil (STENCIL_4) is supported");
+        return VLBM_ERR_UNSUPPORTED;
+    }
+    if (ib->max_iterations < 1 || !(ib->mesh_scale > 0)) { set_last_error("max_iterations >= 1 and mesh_scale > 0 required"); return VLBM_ERR_INVALID; }
+    IbmState* st = new IbmState();
+    st->cfg = *ib;
+    const vlbm_config& c = s->cfg;
+    IbmParams& P = st->prm;
+    P.np = n;
+    P.nx = c.nx; P.ny = c.ny; P.nz = c.nz;
+    P.wall[0] = ib->wall_x; P.wall[1] = ib->wall_y; P.wall[2] = ib->wall_z;
+    P.alpha = ib->movement_alpha;
+    P.rho_f = ib->fluid_density;
+    P.g[0] = ib->gx; P.g[1] = ib->gy; P.g[2] = ib->gz;
+    P.thickness = ib->thickness;
+    {   // contact constants, ibmBoundaryCondition.h:93-107 and the damping factor of :441
+        const double Gp = ib->particle_young / (2.0 + 2.0 * ib->particle_poisson);
+        const double Gw = ib->wall_young / (2.0 + 2.0 * ib->wall_poisson);
+        const double np2 = ib->particle_poisson * ib->particle_poisson, nw2 = ib->wall_poisson * ib->wall_poisson;
+        P.ss_n = (4.0 / 3.0) / ((1 - np2) / ib->particle_young + (1 - np2) / ib->particle_young);
+        P.sw_n = (4.0 / 3.0) / ((1 - np2) / ib->particle_young + (1 - nw2) / ib->wall_young);
+        P.ss_t = 4.0 * std::sqrt(2.0) / ((2 - ib->particle_poisson) / Gp + (2 - ib->particle_poisson) / Gp);
+        P.sw_t = 4.0 * std::sqrt(2.0) / ((2 - ib->particle_poisson) / Gp + (2 - ib->wall_poisson) / Gw);
+        const double lpp = std::log(ib->pp_restitution), lpw = std::log(ib->pw_restitution);
+        P.dpp = -2.0 * lpp / std::sqrt(M_PI * M_PI + lpp * lpp);
+        P.dpw = -2.0 * lpw / std::sqrt(M_PI * M_PI + lpw * lpw);
+        P.mu_pp = ib->pp_friction;
+        P.mu_pw = ib->pw_friction;
+    }
+    P.fx = (float)c.fx; P.fy = (float)c.fy; P.fz = (float)c.fz;
+    std::vector<DPart> parts(n);
+    std::vector<double> X, Y, Z, S;
+    std::vector<int> pid;
+    for (int k = 0; k < n; ++k) {
+        DPart& p = parts[k];
+        std::memset(&p, 0, sizeof(p));
+        const double r = sp[k].diameter / 2.0;
+        p.radius = r;
+        p.volume = r * r * r * 4 * M_PI / 3;
+        p.S = 4.0 * M_PI * r * r;
+        p.density = sp[k].density;
+        const double cc[3] = {sp[k].cx, sp[k].cy, sp[k].cz}, v[3] = {sp[k].vx, sp[k].vy, sp[k].vz},
+                     w[3] = {sp[k].wx, sp[k].wy, sp[k].wz};
+        for (int a = 0; a < 3; ++a) {
+            p.pos[a] = p.pos_old[a] = cc[a];
+            p.vel[a] = p.vel_old[a] = v[a];
+            p.w[a] = p.w_avg[a] = p.w_old[a] = w[a];
+        }
+        p.I[0] = p.I[1] = p.I[2] = 2.0 * p.volume * p.density * r * r / 5.0;  // particle.cpp:745-751
+        p.movable = sp[k].movable;
+        for (int i = 0; i < IBM_MAX_SLOTS; ++i) { p.partner[i] = -1; p.last[i] = -1; }
+        std::vector<double> px, py, pz, pS;
+        host_mesh(sp[k].diameter, ib->mesh_scale, ib->breugem, px, py, pz, pS);
+        p.node_begin = (int)X.size();
+        p.node_count = (int)px.size();
+        for (size_t j = 0; j < px.size(); ++j) {
+            X.push_back(px[j] + cc[0]); Y.push_back(py[j] + cc[1]); Z.push_back(pz[j] + cc[2]);
+            S.push_back(pS[j]);
+            pid.push_back(k);
+        }
+    }
+    st->np = n;
+    st->nnodes = (int)X.size();
+    P.nnodes = st->nnodes;
+    const size_t nn = X.size(), N = (size_t)s->N;
+    auto dalloc = [&](void** p, size_t b) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, b);
+        if (e == cudaSuccess) st->bytes += b;
+        return e;
+    };
+    cudaError_t e = dalloc((void**)&st->parts, parts.size() * sizeof(DPart));
+    double** dp[] = {&st->nx, &st->ny, &st->nz, &st->nS, &st->nfx, &st->nfy, &st->nfz, &st->ndx, &st->ndy, &st->ndz};
+    for (double** d : dp)
+        if (e == cudaSuccess) e = dalloc((void**)d, nn * sizeof(double));
+    if (e == cudaSuccess) e = dalloc((void**)&st->npid, nn * sizeof(int));
+    if (e == cudaSuccess) e = dalloc((void**)&st->fields, 7 * N * sizeof(float));
+    if (e == cudaSuccess) e = dalloc((void**)&st->list, N * sizeof(int));
+    if (e == cudaSuccess) e = dalloc((void**)&st->count, sizeof(int));
+    if (e == cudaSuccess) e = dalloc((void**)&st->contrib, (size_t)n * n * 6 * sizeof(double));
+    if (e == cudaSuccess && !s->fibm) {
+        e = cudaMalloc((void**)&s->fibm, 3 * N * sizeof(float));
+        if (e == cudaSuccess) s->device_bytes += 3 * N * sizeof(float);
+    }
+    if (e != cudaSuccess) { ibm_destroy(st); return cuda_status(e, "IBM allocation"); }
+    e = cudaMemcpy(st->parts, parts.data(), parts.size() * sizeof(DPart), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(st->nx, X.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(st->ny, Y.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(st->nz, Z.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(st->nS, S.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(st->npid, pid.data(), nn * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(st->fields, 0, 7 * N * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(st->count, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s->fibm, 0, 3 * N * sizeof(float));
+    // staged box capacity: largest sphere box, capped by the shared memory limit
+    int maxbox = 0;
+    for (int k = 0; k < n; ++k) {
+        const int side = (int)std::ceil(sp[k].diameter) + 5;
+        const int bx = std::min(side, c.nx), by = std::min(side, c.ny), bz = std::min(side, c.nz);
+        maxbox = std::max(maxbox, bx * by * bz);
+    }
+    st->smem_nodes = std::min(maxbox, IBM_SMEM_MAX_NODES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ibm_interp_spread, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 st->smem_nodes * 4 * (int)sizeof(float));
+    if (e != cudaSuccess) { ibm_destroy(st); return cuda_status(e, "IBM setup"); }
+    st->initial = parts;
+    st->init_nodes.resize(3 * nn);
+    std::memcpy(st->init_nodes.data(), X.data(), nn * sizeof(double));
+    std::memcpy(st->init_nodes.data() + nn, Y.data(), nn * sizeof(double));
+    std::memcpy(st->init_nodes.data() + 2 * nn, Z.data(), nn * sizeof(double));
+    s->device_bytes += st->bytes;
+    s->ibm = st;
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_get_particles(vlbm_sim* s, vlbm_particle_state* out, int32_t n) {
+    if (!s || !out) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    if (!s->ibm) { set_last_error("no spheres in this simulation"); return VLBM_ERR_STATE; }
+    IBM_CUDA(cudaSetDevice(s->device));
+    IbmState* st = s->ibm;
+    std::vector<DPart> h(st->np);
+    IBM_CUDA(cudaMemcpyAsync(h.data(), st->parts, h.size() * sizeof(DPart), cudaMemcpyDeviceToHost, s->stream));
+    IBM_CUDA(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < n && k < st->np; ++k) {
+        const DPart& p = h[k];
+        vlbm_particle_state& o = out[k];
+        std::memset(&o, 0, sizeof(o));
+        for (int a = 0; a < 3; ++a) {
+            o.pos[a] = p.pos[a]; o.vel[a] = p.vel[a]; o.w[a] = p.w[a]; o.f[a] = p.f[a]; o.M[a] = p.M[a];
+            o.pos_old[a] = p.pos_old[a]; o.vel_old[a] = p.vel_old[a]; o.w_old[a] = p.w_old[a];
+            o.f_old[a] = p.f_old[a]; o.M_old[a] = p.M_old[a]; o.w_avg[a] = p.w_avg[a]; o.w_pos[a] = p.w_pos[a];
+        }
+        for (int a = 0; a < 6; ++a) o.I[a] = p.I[a];
+        o.radius = p.radius; o.volume = p.volume; o.density = p.density; o.S = p.S;
+        o.movable = p.movable; o.n_nodes = p.node_count;
+    }
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_get_lagrangian_nodes(vlbm_sim* s, double* pos, double* force, size_t n) {
+    if (!s) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    if (!s->ibm) { set_last_error("no spheres in this simulation"); return VLBM_ERR_STATE; }
+    IbmState* st = s->ibm;
+    if (n != (size_t)st->nnodes) { set_last_error("node count mismatch"); return VLBM_ERR_INVALID; }
+    IBM_CUDA(cudaSetDevice(s->device));
+    const size_t b = n * sizeof(double);
+    if (pos) {
+        IBM_CUDA(cudaMemcpyAsync(pos, st->nx, b, cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(pos + n, st->ny, b, cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(pos + 2 * n, st->nz, b, cudaMemcpyDeviceToHost, s->stream));
+    }
+    if (force) {
+        IBM_CUDA(cudaMemcpyAsync(force, st->nfx, b, cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(force + n, st->nfy, b, cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(force + 2 * n, st->nfz, b, cudaMemcpyDeviceToHost, s->stream));
+    }
+    IBM_CUDA(cudaStreamSynchronize(s->stream));
+    return VLBM_OK;
 }
 
 }  // extern "C"

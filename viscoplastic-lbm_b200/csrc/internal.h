@@ -12,6 +12,7 @@ namespace vlbm {
 enum : uint8_t {
     NODE_BULK = 0,       // plain periodic streaming, no boundary rule
     NODE_BC = 1,         // boundary node: look up bc_slot / BcRec
+    NODE_IBM_SET = 0x20,  // node listed by this step's IBM gather
     NODE_IBM_FORCE = 0x40 // IBM force present in the dense force field
 };
 
@@ -44,7 +45,7 @@ struct StepParams {
     const BcRec* bc;            // [nbc]
     const float* side_prev;     // post-collision of boundary nodes, previous step [Q][nbc]
     float* side_next;           // same, this step
-    float* omega;               // Power-Law omega state [N] (nullptr otherwise)
+    float* omega;               // Power-Law state: apparent viscosity eta of the last step [N]
     float* fibm;                // IBM force [3][N] (nullptr without spheres)
     unsigned int* err;          // device error word (bit 0: bad density)
     int nx, ny, nz;

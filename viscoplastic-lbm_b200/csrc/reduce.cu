@@ -1,0 +1,134 @@
+// reduce.cu -- FP64 global mass and momentum of the current state.
+//
+// Sums rho and rho*u = sum_i f_i c_i + F/2 over every node in double precision
+// (the reference's only global reduction is the FP32 density mean of
+// AuxFunctions/reduction.cu:36-98 used for DENSITY_CORRECTION; treatData.cpp
+// sums on the host).  Two passes with a fixed partition: each block owns a
+// chunk of REDUCE_CHUNK consecutive nodes and writes four partial sums, a
+// single block then adds the partials in block order, so the result is
+// bit-reproducible for a given lattice size.
+#include <cuda_runtime.h>
+#include "sim.h"
+#include "step_impl.cuh"
+
+namespace vlbm {
+
+constexpr int REDUCE_THREADS = 256;
+constexpr int REDUCE_CHUNK = 4096;   // nodes per block
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int Q, int ST, bool ODD>
+__global__ void __launch_bounds__(REDUCE_THREADS) k_moment_partials(const StepParams p, double* partials) {
+    const long long base = (long long)blockIdx.x * REDUCE_CHUNK;
+    const long long end = base + REDUCE_CHUNK < p.N ? base + REDUCE_CHUNK : p.N;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long nn = base + threadIdx.x; nn < end; nn += REDUCE_THREADS) {
+        const unsigned n = (unsigned)nn;
+        const int x = (int)(n % (unsigned)p.nx);
+        const unsigned t = n / (unsigned)p.nx;
+        const int y = (int)(t % (unsigned)p.ny);
+        const int z = (int)(t / (unsigned)p.ny);
+        Nbr nb;
+        nb.init(x, y, z, p.nx, p.ny, p.nz);
+        float f[Q];
+        uint8_t cls;
+        gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
+        double rho = 0.0, jx = 0.5 * p.fx, jy = 0.5 * p.fy, jz = 0.5 * p.fz;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            rho += f[i];
+            if (lat_cx(i)) jx += lat_cx(i) * (double)f[i];
+            if (lat_cy(i)) jy += lat_cy(i) * (double)f[i];
+            if (lat_cz(i)) jz += lat_cz(i) * (double)f[i];
+        }
+        acc[0] += rho; acc[1] += jx; acc[2] += jy; acc[3] += jz;
+    }
+    __shared__ double sh[4][REDUCE_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double v = warp_sum(acc[k]);
+        if (lane == 0) sh[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double s = 0.0;
+        for (int w = 0; w < REDUCE_THREADS / 32; ++w) s += sh[threadIdx.x][w];
+        partials[(size_t)blockIdx.x * 4 + threadIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(REDUCE_THREADS) k_moment_finalize(const double* partials, int nblocks, double* out) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nblocks; b += REDUCE_THREADS)
+        for (int k = 0; k < 4; ++k) acc[k] += partials[(size_t)b * 4 + k];
+    __shared__ double sh[4][REDUCE_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double v = warp_sum(acc[k]);
+        if (lane == 0) sh[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double s = 0.0;
+        for (int w = 0; w < REDUCE_THREADS / 32; ++w) s += sh[threadIdx.x][w];
+        out[threadIdx.x] = s;
+    }
+}
+
+int reduce_blocks(long long N) { return (int)((N + REDUCE_CHUNK - 1) / REDUCE_CHUNK); }
+
+// Launch both passes: partials[4*reduce_blocks(N)] doubles, out[4] doubles (device).
+cudaError_t launch_moments_sum(vlbm_sim* s, double* partials, double* out) {
+    const StepParams p = make_params(s);
+    const int nb = reduce_blocks(s->N);
+    const bool odd = s->parity == 1;
+#define VLBM_RED(QQ, SS)                                                                                   \
+    do {                                                                                                   \
+        if (odd) k_moment_partials<QQ, SS, true><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials);       \
+        else k_moment_partials<QQ, SS, false><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials);          \
+    } while (0)
+    const int st = s->cfg.storage;
+    if (s->Q == 19) {
+        if (st == VLBM_STORE_F32) VLBM_RED(19, VLBM_STORE_F32);
+        else if (st == VLBM_STORE_F16) VLBM_RED(19, VLBM_STORE_F16);
+        else VLBM_RED(19, VLBM_STORE_BF16);
+    } else {
+        if (st == VLBM_STORE_F32) VLBM_RED(27, VLBM_STORE_F32);
+        else if (st == VLBM_STORE_F16) VLBM_RED(27, VLBM_STORE_F16);
+        else VLBM_RED(27, VLBM_STORE_BF16);
+    }
+#undef VLBM_RED
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_moment_finalize<<<1, REDUCE_THREADS, 0, s->stream>>>(partials, nb, out);
+    return cudaGetLastError();
+}
+
+}  // namespace vlbm
+
+using namespace vlbm;
+
+extern "C" vlbm_status vlbm_moments_sum(vlbm_sim* s, double* out4) {
+    if (!s || !out4) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
+    const size_t need = (size_t)4 * reduce_blocks(s->N) + 4;
+    if (!s->red_scratch) {
+        e = cudaMalloc(&s->red_scratch, need * sizeof(double));
+        if (e != cudaSuccess) { s->red_scratch = nullptr; return cuda_status(e, "cudaMalloc reduction scratch"); }
+        s->device_bytes += need * sizeof(double);
+    }
+    double* partials = s->red_scratch;
+    double* out = s->red_scratch + (need - 4);
+    e = launch_moments_sum(s, partials, out);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out4, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return cuda_status(e, "vlbm_moments_sum");
+}

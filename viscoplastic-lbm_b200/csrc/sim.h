@@ -38,6 +38,7 @@ struct vlbm_sim {
     float* fibm = nullptr;           // [3][N] IBM force (allocated with spheres)
     unsigned int* err = nullptr;     // device error word
     float* scratch = nullptr;        // [5][N] macroscopic output scratch (lazy)
+    double* red_scratch = nullptr;   // FP64 reduction partials + result (lazy)
     size_t device_bytes = 0;
 
     // host state
@@ -63,10 +64,15 @@ vlbm_status fluid_step(vlbm_sim* s);   // one fused step (no IBM)
 vlbm_status sim_macroscopics_device(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz, float* omega);
 vlbm_status sim_validate_config(const vlbm_config& c, std::string& why);
 
+// FP64 mass/momentum reduction (reduce.cu)
+int reduce_blocks(long long N);
+cudaError_t launch_moments_sum(vlbm_sim* s, double* partials, double* out);
+
 // IBM hooks (ibm.cu)
 vlbm_status ibm_step(vlbm_sim* s);
 vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz);
 void ibm_destroy(IbmState* st);
 void ibm_reset(vlbm_sim* s);
+void ibm_counts(const vlbm_sim* s, int* np, int* nn);
 
 }  // namespace vlbm

@@ -284,15 +284,18 @@ __device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr
                                       float (&f)[Q], uint8_t& cls) {
     using S = Store<ST>;
     using T = typename S::T;
-    const T* A = static_cast<const T*>(p.pop);
     const size_t N = (size_t)p.N;
+    // walk the planes with one running pointer: plane j holds population j in
+    // the natural layout (even steps) and population opp(j) after an even step
+    const T* plane = static_cast<const T*>(p.pop);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
+    for (int j = 0; j < Q; ++j, plane += N) {
         if (!ODD) {
-            f[i] = S::ld(A + (size_t)i * N + n, Lattice<Q>::w(i), p);
+            f[j] = S::ld(plane + n, Lattice<Q>::w(j), p);
         } else {
+            const int i = lat_opp(j);
             const unsigned src = n + nb.off(-lat_cx(i), -lat_cy(i), -lat_cz(i));
-            f[i] = S::ld(A + (size_t)lat_opp(i) * N + src, Lattice<Q>::w(i), p);
+            f[i] = S::ld(plane + src, Lattice<Q>::w(i), p);
         }
     }
     cls = p.cls[n];
@@ -360,16 +363,21 @@ __device__ __forceinline__ float stress_aux(const Mom& m, float fx, float fy, fl
     return sqrtf(0.5f * (a * a + b * b + c * c + 2.f * (d * d + e * e + g * g)));
 }
 
-// nnf.h:32-87 calcOmega.
+// nnf.h:32-87 calcOmega.  For Power-Law the per-node state is the apparent
+// viscosity eta of the previous step (the reference stores omega,
+// lbm.cu:215-219); with omega_old = 1/(1/2 + 3 eta_old) the reference's
+//   eta_old = (1/omega_old - 1/2)/3,  gamma_dot = (1 - omega_old/2) |S| / eta_old
+// is the same number as gamma_dot = 3 |S| / (1/2 + 3 eta_old), which stays
+// finite where FP32 would round omega_old to exactly 2 (eta_old -> 0) and
+// needs eta_old = +inf for the reference's initial omega = 0.
 template <int RHEO>
-__device__ __forceinline__ float relax(const StepParams& p, float omega_old, float aux) {
+__device__ __forceinline__ float relax(const StepParams& p, float eta_old, float aux, float& eta_new) {
     if (RHEO == VLBM_BINGHAM) {
         return p.omega_p * fmaxf(0.f, 1.f - p.yield / aux);
     } else if (RHEO == VLBM_POWERLAW) {
-        float eta = ((1.f / omega_old) - 0.5f) / 3.f;
-        const float gd = (1.f - 0.5f * omega_old) * aux / eta;
-        eta = (gd <= p.gamma0) ? p.k_cons : p.k_cons * powf(gd, p.n_index - 1.f);
-        return 1.f / (0.5f + 3.f * eta);
+        const float gd = 3.f * aux / (0.5f + 3.f * eta_old);
+        eta_new = (gd <= p.gamma0) ? p.k_cons : p.k_cons * powf(gd, p.n_index - 1.f);
+        return 1.f / (0.5f + 3.f * eta_new);
     }
     return p.omega_newt;
 }
@@ -422,6 +430,9 @@ __device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega
 }
 
 // ------------------------------------------------------------ kernels --
+// Occupancy: the odd (neighbour) step needs more address registers; capping it
+// at 4 resident 256-thread blocks per SM (64 registers) keeps enough loads in
+// flight to saturate HBM.
 template <int Q, int OP, int RHEO, int ST, bool ODD>
 __global__ void __launch_bounds__(256) k_step(const StepParams p) {
     using S = Store<ST>;
@@ -444,7 +455,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
         const size_t N = (size_t)p.N;
         fx += p.fibm[n]; fy += p.fibm[N + n]; fz += p.fibm[2 * N + n];
         p.fibm[n] = 0.f; p.fibm[N + n] = 0.f; p.fibm[2 * N + n] = 0.f;
-        p.cls[n] = cls & (uint8_t)~NODE_IBM_FORCE;
+        p.cls[n] = cls & (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
     }
     constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
     const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz);
@@ -453,8 +464,9 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
     if (RHEO != VLBM_NEWTONIAN) {
         const float aux = stress_aux(m, fx, fy, fz);
         const float old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;
-        omega = relax<RHEO>(p, old, aux);
-        if (RHEO == VLBM_POWERLAW) p.omega[n] = omega;  // lbm.cu:215-219
+        float eta = 0.f;
+        omega = relax<RHEO>(p, old, aux, eta);
+        if (RHEO == VLBM_POWERLAW) p.omega[n] = eta;  // state update, lbm.cu:215-219
     }
     collide<Q, OP>(f, m, omega, fx, fy, fz);
 
@@ -463,15 +475,16 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
 #pragma unroll
         for (int i = 0; i < Q; ++i) p.side_next[(size_t)i * nbc + slot] = f[i];
     }
-    T* A = static_cast<T*>(p.pop);
+    T* plane = static_cast<T*>(p.pop);
     const size_t N = (size_t)p.N;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        if (!ODD) {
-            S::st(A + (size_t)lat_opp(i) * N + n, f[i], Lattice<Q>::w(i), p);
-        } else {
-            const unsigned dst = n + nb.off(lat_cx(i), lat_cy(i), lat_cz(i));
-            S::st(A + (size_t)i * N + dst, f[i], Lattice<Q>::w(i), p);
+    for (int j = 0; j < Q; ++j, plane += N) {
+        if (!ODD) {  // plane j receives the post-collision value of opp(j) at this node
+            const int i = lat_opp(j);
+            S::st(plane + n, f[i], Lattice<Q>::w(i), p);
+        } else {     // plane j receives population j streamed to the downstream node
+            const unsigned dst = n + nb.off(lat_cx(j), lat_cy(j), lat_cz(j));
+            S::st(plane + dst, f[j], Lattice<Q>::w(j), p);
         }
     }
 }
@@ -507,7 +520,8 @@ __global__ void __launch_bounds__(256) k_macro(const MacroParams mp) {
         if (RHEO != VLBM_NEWTONIAN) {
             const float aux = stress_aux(m, fx, fy, fz);
             const float old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;
-            omega = relax<RHEO>(p, old, aux);
+            float eta = 0.f;
+            omega = relax<RHEO>(p, old, aux, eta);
         }
         mp.omega_out[n] = omega;
     }
@@ -553,7 +567,7 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
         }
         S::st(A + (size_t)i * N + n, v, Lattice<Q>::w(i), p);
     }
-    if (p.omega) p.omega[n] = 0.f;  // lbmInitialization.cu:111
+    if (p.omega) p.omega[n] = __int_as_float(0x7f800000);  // eta = +inf <=> omega = 0 (lbmInitialization.cu:111)
 }
 
 }  // namespace vlbm

@@ -180,6 +180,7 @@ _SIGS = {
     "vlbm_set_populations": [_P, _F32P, C.c_size_t],
     "vlbm_get_forces": [_P, _F32P, C.c_size_t],
     "vlbm_get_info": [_P, C.POINTER(Info)],
+    "vlbm_moments_sum": [_P, _F64P],
     "vlbm_add_spheres": [_P, C.POINTER(IbmConfig), C.POINTER(Sphere), C.c_int32],
     "vlbm_get_particles": [_P, C.POINTER(ParticleState), C.c_int32],
     "vlbm_get_lagrangian_nodes": [_P, _F64P, _F64P, C.c_size_t],
@@ -306,6 +307,12 @@ class Simulation:
         out = np.empty(3 * self.n, dtype=np.float32)
         _check(_lib.vlbm_get_forces(self._h, _fptr(out), out.size), "vlbm_get_forces")
         return out.reshape(3, self.cfg.nz, self.cfg.ny, self.cfg.nx)
+
+    def moments_sum(self):
+        """FP64 (sum rho, sum rho ux, sum rho uy, sum rho uz) of the current state."""
+        out = np.zeros(4, dtype=np.float64)
+        _check(_lib.vlbm_moments_sum(self._h, out.ctypes.data_as(_F64P)), "vlbm_moments_sum")
+        return out
 
     def info(self):
         i = Info()
