@@ -1,7 +1,7 @@
 """Immersed-boundary step for spheres on the GPU against the FP64 oracle.
 
 Tolerances (FP32 Eulerian fields and interpolation vs FP64, <= 60 steps):
-  sphere position   |dx| <= 1e-7 + 1e-3 * |x - x0|
+  sphere position   |dx| <= 2e-6 + 1e-3 * |x - x0|  (lattice units; sphere radius >= 3)
   sphere velocity   |dv| <= 2e-3 * max|v| + 1e-9 (and the same for the rotation)
   fluid velocity    relative L2 <= 5e-3, max abs <= 5e-6 (settling flows are
                     ~1e-4, so FP32 rounding of rho*u weighs in)
@@ -60,7 +60,7 @@ def test_ibm_step_matches_oracle(vlbm, oracle, case):
     pos = np.array([list(p.pos) for p in pg])
     vel = np.array([list(p.vel) for p in pg])
     w = np.array([list(p.w) for p in pg])
-    assert np.all(np.abs(pos - po["pos"]) <= 1e-7 + 1e-3 * np.abs(po["pos"] - x0)), (name, pos - po["pos"])
+    assert np.all(np.abs(pos - po["pos"]) <= 2e-6 + 1e-3 * np.abs(po["pos"] - x0)), (name, pos - po["pos"])
     vscale = max(np.abs(po["vel"]).max(), 1e-12)
     assert np.abs(vel - po["vel"]).max() <= 2e-3 * vscale + 1e-9, (name, vel - po["vel"])
     wscale = max(np.abs(po["w"]).max(), 1e-12)
