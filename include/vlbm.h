@@ -181,6 +181,19 @@ vlbm_status vlbm_set_populations(vlbm_sim* sim, const float* pops, size_t n);
  * treatData.cpp:25-449.  Allocates its partial-sum buffer on first use. */
 vlbm_status vlbm_moments_sum(vlbm_sim* sim, double* out4);
 
+/* Same sums as vlbm_moments_sum, for callers that cannot allocate device
+ * memory when they need them (a serving process whose HBM is all committed to
+ * admitted simulations, a monitor thread in a process whose allocator belongs
+ * to another framework).  It allocates nothing: it uses a fixed 512 KiB scratch
+ * array in the library's device globals, which every GPU that loads the
+ * library keeps until exit.  No counterpart in the reference.  Limit: lattices
+ * of at most 67,108,864 nodes (larger ones return VLBM_ERR_INVALID).  The
+ * first call on a device looks up the array's device address, so make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: calls that overlap on the GPU race, so serialise them.  out4 is a
+ * host array of 4 doubles; results are bit-identical to vlbm_moments_sum. */
+vlbm_status vlbm_moments_sum_noalloc(vlbm_sim* sim, double* out4);
+
 /* Per-node IBM force (macr.f, macroscopics.h) of the current state, [3][nz][ny][nx]. */
 vlbm_status vlbm_get_forces(vlbm_sim* sim, float* fxyz, size_t n);
 

@@ -8,6 +8,8 @@
 // single block then adds the partials in block order, so the result is
 // bit-reproducible for a given lattice size.
 #include <cuda_runtime.h>
+#include <mutex>
+#include <string>
 #include "sim.h"
 #include "step_impl.cuh"
 
@@ -131,4 +133,70 @@ extern "C" vlbm_status vlbm_moments_sum(vlbm_sim* s, double* out4) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(out4, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     return cuda_status(e, "vlbm_moments_sum");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of vlbm_moments_sum.
+//
+// Some callers cannot call cudaMalloc when they want these sums: a serving
+// process that has handed its whole HBM budget to admitted simulations, a
+// host thread sampling mass and momentum between steps while the allocator is
+// owned by another framework, or code that must not grow the device footprint
+// after start-up.  This variant uses a fixed scratch array in the library's
+// device globals instead of the per-simulation buffer that vlbm_moments_sum
+// allocates on first use.  It runs the same two kernels on the same partition,
+// so both entry points return bit-identical sums.
+//
+// The array below holds REDUCE_NOALLOC_MAX_BLOCKS partial-sum slots (4 doubles
+// each) plus the 4-double result: 512 KiB + 32 B that every GPU which loads the
+// library keeps until the process exits.  That caps the lattice at
+// REDUCE_NOALLOC_MAX_BLOCKS * REDUCE_CHUNK = 67,108,864 nodes.  Every slot the
+// finalize pass reads is written by the partial pass of the same call, so no
+// part of the array has to start at zero; the array keeps the last call's
+// contents.  All calls on a device share it: calls whose kernels overlap on
+// the GPU (different streams, or several host threads) race and return wrong
+// sums, so callers must serialise them.
+constexpr int REDUCE_NOALLOC_MAX_BLOCKS = 16384;
+static __device__ __align__(256) double g_reduce_noalloc_scratch[4 * REDUCE_NOALLOC_MAX_BLOCKS + 4];
+
+namespace {
+// Device address of g_reduce_noalloc_scratch per device ordinal.  In host code
+// the array's name is only a host-side stand-in, so the address is taken with
+// cudaGetSymbolAddress once per device, with that device current.
+constexpr int kMaxDevices = 64;
+double* g_noalloc_addr[kMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+cudaError_t noalloc_scratch_address(int device, double** out) {
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_reduce_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[device] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[device];
+    return cudaSuccess;
+}
+}  // namespace
+
+extern "C" vlbm_status vlbm_moments_sum_noalloc(vlbm_sim* s, double* out4) {
+    if (!s || !out4) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    const int nb = reduce_blocks(s->N);
+    if (nb > REDUCE_NOALLOC_MAX_BLOCKS) {
+        set_last_error("vlbm_moments_sum_noalloc: the lattice has " + std::to_string(s->N) +
+                       " nodes, more than the 67108864 its built-in scratch covers; use vlbm_moments_sum");
+        return VLBM_ERR_INVALID;
+    }
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
+    double* scratch = nullptr;
+    e = noalloc_scratch_address(s->device, &scratch);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_reduce_noalloc_scratch)");
+    double* out = scratch + 4 * REDUCE_NOALLOC_MAX_BLOCKS;
+    e = launch_moments_sum(s, scratch, out);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out4, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return cuda_status(e, "vlbm_moments_sum_noalloc");
 }

@@ -181,6 +181,7 @@ _SIGS = {
     "vlbm_get_forces": [_P, _F32P, C.c_size_t],
     "vlbm_get_info": [_P, C.POINTER(Info)],
     "vlbm_moments_sum": [_P, _F64P],
+    "vlbm_moments_sum_noalloc": [_P, _F64P],
     "vlbm_add_spheres": [_P, C.POINTER(IbmConfig), C.POINTER(Sphere), C.c_int32],
     "vlbm_get_particles": [_P, C.POINTER(ParticleState), C.c_int32],
     "vlbm_get_lagrangian_nodes": [_P, _F64P, _F64P, C.c_size_t],
