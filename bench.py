@@ -156,6 +156,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="vlbm", choices=["vlbm", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--layout", default="auto", choices=["auto", "natural", "zpair"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -178,6 +179,7 @@ def main():
 
     storage = {"f32": vlbm.STORE_F32, "f16": vlbm.STORE_F16, "bf16": vlbm.STORE_BF16}[args.storage]
     cfg = make_cfg(vlbm, storage)
+    cfg.layout = {"auto": vlbm.LAYOUT_AUTO, "natural": vlbm.LAYOUT_NATURAL, "zpair": vlbm.LAYOUT_ZPAIR}[args.layout]
     cfg.device = local
     sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
     stream = torch.cuda.Stream()
@@ -253,7 +255,7 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": dtype[args.storage], "data": "synthetic",
-            "config": config_dict(args.storage),
+            "config": dict(config_dict(args.storage), layout=args.layout),
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak, "traffic": traffic,
                          "peak_source": peak_kind,

@@ -113,8 +113,16 @@ typedef struct vlbm_config {
     double gamma0;               /* nnf.h:118 GAMMA_0 (truncation)                  */
     double ux_bc[8], uy_bc[8], uz_bc[8], rho_bc[8]; /* var.h:114-117 UX_BC..RHO_BC */
     double storage_scale;        /* F16/BF16 deviation scale; 0 = library default   */
-    int32_t reserved[8];
+    int32_t layout;              /* VLBM_LAYOUT_*: population storage order          */
+    int32_t reserved[7];
 } vlbm_config;
+
+/* Population storage order.  NATURAL: planes [Q][z][y][x].  ZPAIR: nodes z and
+ * z+NZ/2 of the same (x, y) are adjacent, so every stencil access of the fused
+ * step is one aligned two-node vector (requires even NZ).  AUTO picks ZPAIR for
+ * FP16/BF16 storage with even NZ and NATURAL otherwise.  The layout is
+ * internal: every entry point takes and returns the [z][y][x] order. */
+enum { VLBM_LAYOUT_AUTO = 0, VLBM_LAYOUT_NATURAL = 1, VLBM_LAYOUT_ZPAIR = 2 };
 
 /* Fill `cfg` with the reference defaults (var.h / nnf.h values, D3Q19, FP32,
  * regularized, Newtonian, tau=0.6, rho0=1, zero force, UX_BC etc. from var.h:114-117). */

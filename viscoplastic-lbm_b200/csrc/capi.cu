@@ -38,6 +38,7 @@ vlbm_status sim_validate_config(const vlbm_config& c, std::string& why) {
     if (c.collision != VLBM_OP_REGULARIZED && c.collision != VLBM_OP_BGK) { why = "unknown collision operator"; return VLBM_ERR_INVALID; }
     if (c.rheology < VLBM_NEWTONIAN || c.rheology > VLBM_POWERLAW) { why = "unknown rheology"; return VLBM_ERR_INVALID; }
     if (c.storage < VLBM_STORE_F32 || c.storage > VLBM_STORE_BF16) { why = "unknown storage"; return VLBM_ERR_INVALID; }
+    if (c.layout < VLBM_LAYOUT_AUTO || c.layout > VLBM_LAYOUT_ZPAIR) { why = "unknown layout"; return VLBM_ERR_INVALID; }
     if (c.rheology == VLBM_NEWTONIAN && !(c.tau > 0.5)) { why = "tau must be > 0.5"; return VLBM_ERR_INVALID; }
     if (c.rheology == VLBM_BINGHAM && !(c.eta_p > 0.0 && c.yield_stress >= 0.0)) { why = "Bingham needs eta_p > 0, yield_stress >= 0"; return VLBM_ERR_INVALID; }
     if (c.rheology == VLBM_POWERLAW && !(c.n_index > 0.0 && c.k_consistency > 0.0)) { why = "Power-Law needs n_index > 0, k_consistency > 0"; return VLBM_ERR_INVALID; }
@@ -61,6 +62,7 @@ StepParams make_params(vlbm_sim* s) {
     p.nx = c.nx; p.ny = c.ny; p.nz = c.nz;
     p.N = s->N;
     p.nbc = s->nbc;
+    p.pairH = s->pairH;
     p.apply_bc = s->apply_bc;
     p.omega_newt = (float)(1.0 / c.tau);                 // var.h:105 OMEGA
     p.fx = (float)c.fx; p.fy = (float)c.fy; p.fz = (float)c.fz;
@@ -193,6 +195,16 @@ vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) {
     s->N = (long long)cfg->nx * cfg->ny * cfg->nz;
     s->store_bytes = cfg->storage == VLBM_STORE_F32 ? 4 : 2;
     s->device = cfg->device;
+    {   // population layout
+        const bool even_z = cfg->nz % 2 == 0;
+        int lay = cfg->layout;
+        // two-node threads pay off where the per-node state is small: D3Q19 with
+        // 2-byte storage (the D3Q27 pair kernel needs over 110 registers)
+        if (lay == VLBM_LAYOUT_AUTO)
+            lay = (cfg->storage != VLBM_STORE_F32 && cfg->vel_set == 19 && even_z) ? VLBM_LAYOUT_ZPAIR : VLBM_LAYOUT_NATURAL;
+        if (lay == VLBM_LAYOUT_ZPAIR && !even_z) { delete s; set_last_error("the z-paired layout needs an even nz"); return VLBM_ERR_INVALID; }
+        s->pairH = lay == VLBM_LAYOUT_ZPAIR ? cfg->nz / 2 : 0;
+    }
     e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete s; return cuda_status(e, "cudaStreamCreate"); }
     s->own_stream = true;

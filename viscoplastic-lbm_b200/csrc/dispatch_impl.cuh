@@ -9,6 +9,12 @@ inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block 
 
 template <int Q, int OP, int RHEO, int ST>
 cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s) {
+    if (p.pairH > 0) {  // z-paired layout: one thread per node pair
+        const unsigned g = grid_for(p.N / 2, ls.block);
+        if (odd) k_step2<Q, OP, RHEO, ST, true><<<g, ls.block, 0, s>>>(p);
+        else k_step2<Q, OP, RHEO, ST, false><<<g, ls.block, 0, s>>>(p);
+        return cudaGetLastError();
+    }
     const unsigned g = grid_for(p.N, ls.block);
     if (odd) k_step<Q, OP, RHEO, ST, true><<<g, ls.block, 0, s>>>(p);
     else k_step<Q, OP, RHEO, ST, false><<<g, ls.block, 0, s>>>(p);
@@ -34,8 +40,14 @@ cudaError_t launch_step_st(const StepParams& p, int op, int rheo, bool odd, Laun
 template <int Q, int RHEO, int ST>
 cudaError_t macro_t(const MacroParams& mp, bool odd, cudaStream_t s) {
     const unsigned g = grid_for(mp.s.N, 256);
-    if (odd) k_macro<Q, RHEO, ST, true><<<g, 256, 0, s>>>(mp);
-    else k_macro<Q, RHEO, ST, false><<<g, 256, 0, s>>>(mp);
+    const bool pr = mp.s.pairH > 0;
+    if (odd) {
+        if (pr) k_macro<Q, RHEO, ST, true, true><<<g, 256, 0, s>>>(mp);
+        else k_macro<Q, RHEO, ST, true, false><<<g, 256, 0, s>>>(mp);
+    } else {
+        if (pr) k_macro<Q, RHEO, ST, false, true><<<g, 256, 0, s>>>(mp);
+        else k_macro<Q, RHEO, ST, false, false><<<g, 256, 0, s>>>(mp);
+    }
     return cudaGetLastError();
 }
 
@@ -52,8 +64,14 @@ cudaError_t launch_macro_st(const MacroParams& mp, int rheo, bool odd, cudaStrea
 template <int Q, int ST>
 cudaError_t get_pops_t(const StepParams& p, bool odd, float* out, cudaStream_t s) {
     const unsigned g = grid_for(p.N, 256);
-    if (odd) k_get_pops<Q, ST, true><<<g, 256, 0, s>>>(p, out);
-    else k_get_pops<Q, ST, false><<<g, 256, 0, s>>>(p, out);
+    const bool pr = p.pairH > 0;
+    if (odd) {
+        if (pr) k_get_pops<Q, ST, true, true><<<g, 256, 0, s>>>(p, out);
+        else k_get_pops<Q, ST, true, false><<<g, 256, 0, s>>>(p, out);
+    } else {
+        if (pr) k_get_pops<Q, ST, false, true><<<g, 256, 0, s>>>(p, out);
+        else k_get_pops<Q, ST, false, false><<<g, 256, 0, s>>>(p, out);
+    }
     return cudaGetLastError();
 }
 
@@ -66,7 +84,8 @@ template <int Q, int ST>
 cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, float ux, float uy, float uz,
                                cudaStream_t s) {
     const unsigned g = grid_for(p.N, 256);
-    k_set_pops<Q, ST><<<g, 256, 0, s>>>(p, in, rho, ux, uy, uz);
+    if (p.pairH > 0) k_set_pops<Q, ST, true><<<g, 256, 0, s>>>(p, in, rho, ux, uy, uz);
+    else k_set_pops<Q, ST, false><<<g, 256, 0, s>>>(p, in, rho, ux, uy, uz);
     return cudaGetLastError();
 }
 

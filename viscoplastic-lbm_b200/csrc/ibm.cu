@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_box(IbmParams P, DPart* par
 }
 
 // -------------------------------------------------------------- gather --
-template <int Q, int ST, bool ODD>
+template <int Q, int ST, bool ODD, bool PAIRED>
 __global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmParams P, const DPart* parts,
                                                              float* fields, int* list, int* count) {
     const DPart& p = parts[blockIdx.x];
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmPa
         nb.init(x, y, z, sp.nx, sp.ny, sp.nz);
         float f[Q];
         uint8_t cls;
-        gather<Q, ST, ODD>(sp, n, nb, x, y, z, f, cls);
+        gather<Q, ST, ODD, PAIRED>(sp, n, nb, x, y, z, f, cls);
         const Mom m = moments<Q, false>(f, P.fx, P.fy, P.fz);
         fields[n] = m.rho;
         fields[N + n] = m.ux;
@@ -742,10 +742,14 @@ static void host_mesh(double diameter, double mesh_scale, double breugem, std::v
 template <int Q, int ST>
 static cudaError_t launch_gather(vlbm_sim* s, IbmState* st) {
     const StepParams sp = make_params(s);
-    if (s->parity == 1)
-        k_ibm_gather<Q, ST, true><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
-    else
-        k_ibm_gather<Q, ST, false><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+    const bool pr = sp.pairH > 0;
+    if (s->parity == 1) {
+        if (pr) k_ibm_gather<Q, ST, true, true><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+        else k_ibm_gather<Q, ST, true, false><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+    } else {
+        if (pr) k_ibm_gather<Q, ST, false, true><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+        else k_ibm_gather<Q, ST, false, false><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+    }
     return cudaGetLastError();
 }
 

@@ -51,6 +51,7 @@ struct StepParams {
     int nx, ny, nz;
     long long N;
     int nbc;
+    int pairH;                  // z-paired population layout: NZ/2, or 0 for the natural layout
     int apply_bc;               // 0 on the first step after (re)initialisation
     float omega_newt;           // 1/tau
     float fx, fy, fz;           // body force

@@ -24,7 +24,7 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-template <int Q, int ST, bool ODD>
+template <int Q, int ST, bool ODD, bool PAIRED>
 __global__ void __launch_bounds__(REDUCE_THREADS) k_moment_partials(const StepParams p, double* partials) {
     const long long base = (long long)blockIdx.x * REDUCE_CHUNK;
     const long long end = base + REDUCE_CHUNK < p.N ? base + REDUCE_CHUNK : p.N;
@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_moment_partials(const StepPa
         nb.init(x, y, z, p.nx, p.ny, p.nz);
         float f[Q];
         uint8_t cls;
-        gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
+        gather<Q, ST, ODD, PAIRED>(p, n, nb, x, y, z, f, cls);
         double rho = 0.0, jx = 0.5 * p.fx, jy = 0.5 * p.fy, jz = 0.5 * p.fz;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -93,8 +93,13 @@ cudaError_t launch_moments_sum(vlbm_sim* s, double* partials, double* out) {
     const bool odd = s->parity == 1;
 #define VLBM_RED(QQ, SS)                                                                                   \
     do {                                                                                                   \
-        if (odd) k_moment_partials<QQ, SS, true><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials);       \
-        else k_moment_partials<QQ, SS, false><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials);          \
+        if (p.pairH > 0) {                                                                                 \
+            if (odd) k_moment_partials<QQ, SS, true, true><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials); \
+            else k_moment_partials<QQ, SS, false, true><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials);    \
+        } else {                                                                                           \
+            if (odd) k_moment_partials<QQ, SS, true, false><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials); \
+            else k_moment_partials<QQ, SS, false, false><<<nb, REDUCE_THREADS, 0, s->stream>>>(p, partials);   \
+        }                                                                                                  \
     } while (0)
     const int st = s->cfg.storage;
     if (s->Q == 19) {

@@ -34,6 +34,7 @@ struct vlbm_sim {
     vlbm::BcRec* bc = nullptr;       // [nbc]
     float* side[2] = {nullptr, nullptr};  // [Q][nbc] post-collision at boundary nodes
     int nbc = 0;
+    int pairH = 0;                   // z-paired layout (NZ/2) or 0
     float* omega = nullptr;          // [N] Power-Law state
     float* fibm = nullptr;           // [3][N] IBM force (allocated with spheres)
     unsigned int* err = nullptr;     // device error word

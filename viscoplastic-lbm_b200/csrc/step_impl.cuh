@@ -81,6 +81,12 @@ struct Nbr {
         zm = (z == 0) ? (nz - 1) * nxy : -nxy;
         zp = (z == nz - 1) ? -(nz - 1) * nxy : nxy;
     }
+    // Hide the offsets from common-subexpression elimination: the store loop
+    // then recomputes its sums (a few integer adds) instead of keeping the
+    // load loop's 18 sums live across the collision.
+    __device__ __forceinline__ void launder() {
+        asm volatile("" : "+r"(xm), "+r"(xp), "+r"(ym), "+r"(yp), "+r"(zm), "+r"(zp));
+    }
     // offset of the node at (x+dx, y+dy, z+dz), dx,dy,dz in {-1,0,1}
     __device__ __forceinline__ int off(int dx, int dy, int dz) const {
         return (dx > 0 ? xp : (dx < 0 ? xm : 0)) + (dy > 0 ? yp : (dy < 0 ? ym : 0)) +
@@ -277,14 +283,43 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int
     (void)x; (void)y; (void)z;
 }
 
+// Storage index of node (x, y, z) in the z-paired layout: nodes z and z+H
+// (H = NZ/2) of one (x, y) column are neighbours in memory.
+__device__ __forceinline__ size_t pair_index(const StepParams& p, int x, int y, int z) {
+    const int lane = z >= p.pairH ? 1 : 0;
+    const int zp = z - lane * p.pairH;
+    return ((((size_t)zp * p.ny + y) * p.nx + x) << 1) | (size_t)lane;
+}
+__device__ __forceinline__ int wrap1(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
 // Gather f_i(x, t) of node n (after boundary rules).  Returns the side-store
 // slot of a boundary node, -1 for bulk nodes.
-template <int Q, int ST, bool ODD>
+template <int Q, int ST, bool ODD, bool PAIRED = false>
 __device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr& nb, int x, int y, int z,
                                       float (&f)[Q], uint8_t& cls) {
     using S = Store<ST>;
     using T = typename S::T;
     const size_t N = (size_t)p.N;
+    if (PAIRED) {
+        const T* A = static_cast<const T*>(p.pop);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            if (!ODD) {
+                f[i] = S::ld(A + (size_t)i * N + pair_index(p, x, y, z), Lattice<Q>::w(i), p);
+            } else {
+                const size_t src = pair_index(p, wrap1(x - lat_cx(i), p.nx), wrap1(y - lat_cy(i), p.ny),
+                                              wrap1(z - lat_cz(i), p.nz));
+                f[i] = S::ld(A + (size_t)lat_opp(i) * N + src, Lattice<Q>::w(i), p);
+            }
+        }
+        cls = p.cls[n];
+        int slot = -1;
+        if (cls & NODE_BC) {
+            slot = p.bc_slot[n];
+            if (p.apply_bc) apply_bc<Q>(f, p, slot, x, y, z, nb, n);
+        }
+        return slot;
+    }
     // walk the planes with one running pointer: plane j holds population j in
     // the natural layout (even steps) and population opp(j) after an even step
     const T* plane = static_cast<const T*>(p.pop);
@@ -317,26 +352,29 @@ struct Mom {
 
 template <int Q, bool NEED_PI>
 __device__ __forceinline__ Mom moments(const float (&f)[Q], float fx, float fy, float fz) {
+    // Sums over opposite pairs: e = f_i + f_opp feeds the even moments (rho,
+    // second moments), o = f_i - f_opp the odd ones (momentum).
     Mom m;
-    float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    float rho = f[0], jx = 0.f, jy = 0.f, jz = 0.f;
     float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
+    for (int i = 1; i < Q; i += 2) {
         const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
-        rho += f[i];
-        if (cx) jx += cx * f[i];
-        if (cy) jy += cy * f[i];
-        if (cz) jz += cz * f[i];
+        const float e = f[i] + f[i + 1], o = f[i] - f[i + 1];
+        rho += e;
+        if (cx) jx += cx * o;
+        if (cy) jy += cy * o;
+        if (cz) jz += cz * o;
         if (NEED_PI) {
-            if (cx) sxx += f[i];
-            if (cy) syy += f[i];
-            if (cz) szz += f[i];
-            if (cx && cy) sxy += cx * cy * f[i];
-            if (cx && cz) sxz += cx * cz * f[i];
-            if (cy && cz) syz += cy * cz * f[i];
+            if (cx) sxx += e;
+            if (cy) syy += e;
+            if (cz) szz += e;
+            if (cx && cy) sxy += cx * cy * e;
+            if (cx && cz) sxz += cx * cz * e;
+            if (cy && cz) syz += cy * cz * e;
         }
     }
-    const float inv = 1.f / rho;
+    const float inv = __fdividef(1.f, rho);  // hardware reciprocal (<= 2 ulp)
     m.rho = rho;
     m.ux = (jx + 0.5f * fx) * inv;
     m.uy = (jy + 0.5f * fy) * inv;
@@ -360,7 +398,8 @@ __device__ __forceinline__ float stress_aux(const Mom& m, float fx, float fy, fl
     const float d = m.pxy + 0.5f * (m.ux * fy + m.uy * fx);
     const float e = m.pxz + 0.5f * (m.ux * fz + m.uz * fx);
     const float g = m.pyz + 0.5f * (m.uy * fz + m.uz * fy);
-    return sqrtf(0.5f * (a * a + b * b + c * c + 2.f * (d * d + e * e + g * g)));
+    const float q = 0.5f * (a * a + b * b + c * c + 2.f * (d * d + e * e + g * g));
+    return q > 0.f ? q * rsqrtf(q) : 0.f;  // hardware reciprocal square root (<= 2 ulp)
 }
 
 // nnf.h:32-87 calcOmega.  For Power-Law the per-node state is the apparent
@@ -373,7 +412,7 @@ __device__ __forceinline__ float stress_aux(const Mom& m, float fx, float fy, fl
 template <int RHEO>
 __device__ __forceinline__ float relax(const StepParams& p, float eta_old, float aux, float& eta_new) {
     if (RHEO == VLBM_BINGHAM) {
-        return p.omega_p * fmaxf(0.f, 1.f - p.yield / aux);
+        return p.omega_p * fmaxf(0.f, 1.f - __fdividef(p.yield, aux));
     } else if (RHEO == VLBM_POWERLAW) {
         const float gd = 3.f * aux / (0.5f + 3.f * eta_old);
         eta_new = (gd <= p.gamma0) ? p.k_cons : p.k_cons * powf(gd, p.n_index - 1.f);
@@ -389,6 +428,9 @@ __device__ __forceinline__ float relax(const StepParams& p, float eta_old, float
 //  BGK (collisionForceNoReg.txt): f*_i = (1-omega) f_i + omega f_eq_i + B F_i
 template <int Q, int OP>
 __device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega, float fx, float fy, float fz) {
+    // Populations i (odd index) and opp(i) = i+1 have opposite velocities: they
+    // share Q_i:Pi, while c.u and c.F change sign.  Each pair is evaluated as an
+    // even part E and an odd part O with f*_i = w (E + O), f*_opp = w (E - O).
     const float B = 1.f - 0.5f * omega;
     const float uu = m.ux * m.ux + m.uy * m.uy + m.uz * m.uz;
     const float uF = m.ux * fx + m.uy * fy + m.uz * fz;
@@ -398,34 +440,82 @@ __device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega
         const float K0 = m.rho * (1.f - 1.5f * uu) - 3.f * B * uF - A * tr;
         const float alpha = 3.f * B - A * (1.f / 3.f);
         const float r3 = 3.f * m.rho, r45 = 4.5f * m.rho, b9 = 9.f * B;
+        f[0] = Lattice<Q>::w(0) * K0;
+        // coefficients with the weight of each velocity class folded in
+        float cK[3], cA[3], cr45[3], cb9[3], cal[3], cr3[3];
 #pragma unroll
-        for (int i = 0; i < Q; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            // representative population of the class: 1 (axis), 7 (face), 19 (body, D3Q27 only)
+            const float w = Lattice<Q>::w(k == 0 ? 1 : (k == 1 ? 7 : (Q == 27 ? 19 : 1)));
+            cK[k] = w * K0; cA[k] = w * A; cr45[k] = w * r45; cb9[k] = w * b9; cal[k] = w * alpha; cr3[k] = w * r3;
+        }
+        const float pxy2 = 2.f * m.pxy, pxz2 = 2.f * m.pxz, pyz2 = 2.f * m.pyz;
+#pragma unroll
+        for (int i = 1; i < Q; i += 2) {
             const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
+            const int k = lat_norm1(i) - 1;   // 0 axis, 1 face diagonal, 2 body diagonal
             float S = 0.f, cu = 0.f, cF = 0.f;
             if (cx) { S += m.pxx; cu += cx * m.ux; cF += cx * fx; }
             if (cy) { S += m.pyy; cu += cy * m.uy; cF += cy * fy; }
             if (cz) { S += m.pzz; cu += cz * m.uz; cF += cz * fz; }
-            if (cx && cy) S += 2.f * cx * cy * m.pxy;
-            if (cx && cz) S += 2.f * cx * cz * m.pxz;
-            if (cy && cz) S += 2.f * cy * cz * m.pyz;
-            const float v = K0 + A * S + alpha * cF + cu * (r3 + r45 * cu + b9 * cF);
-            f[i] = Lattice<Q>::w(i) * v;
+            if (cx && cy) S += cx * cy * pxy2;
+            if (cx && cz) S += cx * cz * pxz2;
+            if (cy && cz) S += cy * cz * pyz2;
+            const float E = cK[k] + cA[k] * S + cu * (cr45[k] * cu + cb9[k] * cF);
+            const float O = cal[k] * cF + cr3[k] * cu;
+            f[i] = E + O;
+            f[i + 1] = E - O;
         }
     } else {
         const float om1 = 1.f - omega;
-        const float base = 1.f - 1.5f * uu;
+        const float base = omega * m.rho * (1.f - 1.5f * uu) - 3.f * B * uF;
+        const float r45 = 4.5f * omega * m.rho, r3 = 3.f * omega * m.rho, b9 = 9.f * B, b3 = 3.f * B;
+        f[0] = om1 * f[0] + Lattice<Q>::w(0) * base;
 #pragma unroll
-        for (int i = 0; i < Q; ++i) {
+        for (int i = 1; i < Q; i += 2) {
             const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
             float cu = 0.f, cF = 0.f;
             if (cx) { cu += cx * m.ux; cF += cx * fx; }
             if (cy) { cu += cy * m.uy; cF += cy * fy; }
             if (cz) { cu += cz * m.uz; cF += cz * fz; }
             const float w = Lattice<Q>::w(i);
-            const float feq = w * m.rho * (base + 3.f * cu + 4.5f * cu * cu);
-            const float frc = w * (3.f * cF - 3.f * uF + 9.f * cu * cF);
-            f[i] = om1 * f[i] + omega * feq + B * frc;
+            const float E = w * (base + cu * (r45 * cu + b9 * cF));
+            const float O = w * (r3 * cu + b3 * cF);
+            f[i] = om1 * f[i] + (E + O);
+            f[i + 1] = om1 * f[i + 1] + (E - O);
         }
+    }
+}
+
+// Everything after the gather for one node: IBM force read and reset
+// (lbm.cu:45-58), moments, relaxation (lbm.cu:192-222), collision, and the
+// post-collision copy of boundary nodes (lbm.cu:463-470).
+template <int Q, int OP, int RHEO>
+__device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned n, uint8_t cls, int slot,
+                                                  float (&f)[Q]) {
+    float fx = p.fx, fy = p.fy, fz = p.fz;
+    if (cls & NODE_IBM_FORCE) {
+        const size_t N = (size_t)p.N;
+        fx += p.fibm[n]; fy += p.fibm[N + n]; fz += p.fibm[2 * N + n];
+        p.fibm[n] = 0.f; p.fibm[N + n] = 0.f; p.fibm[2 * N + n] = 0.f;
+        p.cls[n] = cls & (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
+    }
+    constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
+    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz);
+    if (!(m.rho > 0.f && m.rho < 1e30f)) atomicOr(p.err, 1u);
+    float omega = p.omega_newt;
+    if (RHEO != VLBM_NEWTONIAN) {
+        const float aux = stress_aux(m, fx, fy, fz);
+        const float old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;
+        float eta = 0.f;
+        omega = relax<RHEO>(p, old, aux, eta);
+        if (RHEO == VLBM_POWERLAW) p.omega[n] = eta;  // state update, lbm.cu:215-219
+    }
+    collide<Q, OP>(f, m, omega, fx, fy, fz);
+    if (slot >= 0) {
+        const size_t nbc = (size_t)p.nbc;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) p.side_next[(size_t)i * nbc + slot] = f[i];
     }
 }
 
@@ -449,32 +539,8 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
     float f[Q];
     uint8_t cls;
     const int slot = gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
-
-    float fx = p.fx, fy = p.fy, fz = p.fz;
-    if (cls & NODE_IBM_FORCE) {  // IBM force read and reset (lbm.cu:45-58)
-        const size_t N = (size_t)p.N;
-        fx += p.fibm[n]; fy += p.fibm[N + n]; fz += p.fibm[2 * N + n];
-        p.fibm[n] = 0.f; p.fibm[N + n] = 0.f; p.fibm[2 * N + n] = 0.f;
-        p.cls[n] = cls & (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
-    }
-    constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
-    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz);
-    if (!(m.rho > 0.f && m.rho < 1e30f)) atomicOr(p.err, 1u);
-    float omega = p.omega_newt;
-    if (RHEO != VLBM_NEWTONIAN) {
-        const float aux = stress_aux(m, fx, fy, fz);
-        const float old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;
-        float eta = 0.f;
-        omega = relax<RHEO>(p, old, aux, eta);
-        if (RHEO == VLBM_POWERLAW) p.omega[n] = eta;  // state update, lbm.cu:215-219
-    }
-    collide<Q, OP>(f, m, omega, fx, fy, fz);
-
-    if (slot >= 0) {
-        const size_t nbc = (size_t)p.nbc;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) p.side_next[(size_t)i * nbc + slot] = f[i];
-    }
+    relax_and_collide<Q, OP, RHEO>(p, n, cls, slot, f);
+    nb.launder();
     T* plane = static_cast<T*>(p.pop);
     const size_t N = (size_t)p.N;
 #pragma unroll
@@ -490,7 +556,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
 }
 
 // Macroscopics of the current state (what gpuMacrCollisionStream saves).
-template <int Q, int RHEO, int ST, bool ODD>
+template <int Q, int RHEO, int ST, bool ODD, bool PAIRED>
 __global__ void __launch_bounds__(256) k_macro(const MacroParams mp) {
     const StepParams& p = mp.s;
     const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -503,7 +569,7 @@ __global__ void __launch_bounds__(256) k_macro(const MacroParams mp) {
     nb.init(x, y, z, p.nx, p.ny, p.nz);
     float f[Q];
     uint8_t cls;
-    gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
+    gather<Q, ST, ODD, PAIRED>(p, n, nb, x, y, z, f, cls);
     float fx = p.fx, fy = p.fy, fz = p.fz;
     if (mp.fibm_const) {
         const size_t N = (size_t)p.N;
@@ -528,7 +594,7 @@ __global__ void __launch_bounds__(256) k_macro(const MacroParams mp) {
 }
 
 // Populations f_i(x,t) after boundary rules, natural [Q][N] float layout.
-template <int Q, int ST, bool ODD>
+template <int Q, int ST, bool ODD, bool PAIRED>
 __global__ void __launch_bounds__(256) k_get_pops(const StepParams p, float* out) {
     const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= (unsigned)p.N) return;
@@ -540,13 +606,13 @@ __global__ void __launch_bounds__(256) k_get_pops(const StepParams p, float* out
     nb.init(x, y, z, p.nx, p.ny, p.nz);
     float f[Q];
     uint8_t cls;
-    gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
+    gather<Q, ST, ODD, PAIRED>(p, n, nb, x, y, z, f, cls);
 #pragma unroll
     for (int i = 0; i < Q; ++i) out[(size_t)i * (size_t)p.N + n] = f[i];
 }
 
 // Natural-layout store of given populations (equilibrium init or user state).
-template <int Q, int ST>
+template <int Q, int ST, bool PAIRED>
 __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const float* in, float rho, float ux,
                                                   float uy, float uz) {
     using S = Store<ST>;
@@ -555,6 +621,12 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
     if (n >= (unsigned)p.N) return;
     T* A = static_cast<T*>(p.pop);
     const size_t N = (size_t)p.N;
+    size_t sidx = n;
+    if (PAIRED) {
+        const int x = (int)(n % (unsigned)p.nx);
+        const unsigned t = n / (unsigned)p.nx;
+        sidx = pair_index(p, x, (int)(t % (unsigned)p.ny), (int)(t / (unsigned)p.ny));
+    }
     const float uu = ux * ux + uy * uy + uz * uz;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
@@ -565,9 +637,113 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
             const float cu = lat_cx(i) * ux + lat_cy(i) * uy + lat_cz(i) * uz;
             v = Lattice<Q>::w(i) * rho * (1.f - 1.5f * uu + 3.f * cu * (1.f + 1.5f * cu));
         }
-        S::st(A + (size_t)i * N + n, v, Lattice<Q>::w(i), p);
+        S::st(A + (size_t)i * N + sidx, v, Lattice<Q>::w(i), p);
     }
     if (p.omega) p.omega[n] = __int_as_float(0x7f800000);  // eta = +inf <=> omega = 0 (lbmInitialization.cu:111)
+}
+
+// ------------------------------------------------- z-paired two-node step --
+// Vector view of a node pair in each storage type.
+template <int ST> struct Pair;
+template <> struct Pair<VLBM_STORE_F32> {
+    using V = float2;
+    static __device__ __forceinline__ float get(const V& v, int lane, float, const StepParams&) {
+        return lane ? v.y : v.x;
+    }
+    static __device__ __forceinline__ void set(V& v, int lane, float f, float, const StepParams&) {
+        if (lane) v.y = f; else v.x = f;
+    }
+    static __device__ __forceinline__ V swap(const V& v) { return make_float2(v.y, v.x); }
+};
+template <> struct Pair<VLBM_STORE_F16> {
+    using V = __half2;
+    static __device__ __forceinline__ float get(const V& v, int lane, float w, const StepParams& s) {
+        return fmaf(lane ? __high2float(v) : __low2float(v), s.inv_scale, w * s.rho0);
+    }
+    static __device__ __forceinline__ void set(V& v, int lane, float f, float w, const StepParams& s) {
+        const __half h = __float2half_rn((f - w * s.rho0) * s.scale);
+        v = lane ? __halves2half2(__low2half(v), h) : __halves2half2(h, __high2half(v));
+    }
+    static __device__ __forceinline__ V swap(const V& v) { return __lowhigh2highlow(v); }
+};
+template <> struct Pair<VLBM_STORE_BF16> {
+    using V = __nv_bfloat162;
+    static __device__ __forceinline__ float get(const V& v, int lane, float w, const StepParams& s) {
+        return fmaf(lane ? __high2float(v) : __low2float(v), s.inv_scale, w * s.rho0);
+    }
+    static __device__ __forceinline__ void set(V& v, int lane, float f, float w, const StepParams& s) {
+        const __nv_bfloat16 h = __float2bfloat16_rn((f - w * s.rho0) * s.scale);
+        v = lane ? __halves2bfloat162(__low2bfloat16(v), h) : __halves2bfloat162(h, __high2bfloat16(v));
+    }
+    static __device__ __forceinline__ V swap(const V& v) { return __lowhigh2highlow(v); }
+};
+
+// One thread advances the node pair (x, y, zp) / (x, y, zp+H).  Every access is
+// one aligned vector of the two nodes, also for the x-shifted neighbours of
+// the odd step; crossing the periodic z seam swaps the two lanes.
+template <int Q, int OP, int RHEO, int ST, bool ODD>
+__global__ void __launch_bounds__(256) k_step2(const StepParams p) {
+    using PV = Pair<ST>;
+    using V = typename PV::V;
+    const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned M = (unsigned)(p.N >> 1);
+    if (m >= M) return;
+    const int H = p.pairH;
+    const int x = (int)(m % (unsigned)p.nx);
+    const unsigned t = m / (unsigned)p.nx;
+    const int y = (int)(t % (unsigned)p.ny);
+    const int zp = (int)(t / (unsigned)p.ny);
+    Nbr pn;                       // neighbour offsets in pair space
+    pn.init(x, y, zp, p.nx, p.ny, H);
+    const bool seam_lo = zp == 0, seam_hi = zp == H - 1;
+    const size_t Np = (size_t)p.N >> 1;   // pairs per plane
+    V in[Q];
+    const V* plane = reinterpret_cast<const V*>(p.pop);
+#pragma unroll
+    for (int j = 0; j < Q; ++j, plane += Np) {
+        if (!ODD) {
+            in[j] = plane[m];
+        } else {
+            const int i = lat_opp(j);
+            const int cz = lat_cz(i);
+            const V v = plane[m + pn.off(-lat_cx(i), -lat_cy(i), -cz)];
+            const bool sw = (cz > 0 && seam_lo) || (cz < 0 && seam_hi);
+            in[i] = sw ? PV::swap(v) : v;
+        }
+    }
+#pragma unroll
+    for (int lane = 0; lane < 2; ++lane) {
+        const int z = zp + lane * H;
+        const unsigned n = (unsigned)(((size_t)z * p.ny + y) * p.nx + x);
+        float f[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = PV::get(in[i], lane, Lattice<Q>::w(i), p);
+        const uint8_t cls = p.cls[n];
+        int slot = -1;
+        if (cls & NODE_BC) {
+            slot = p.bc_slot[n];
+            if (p.apply_bc) {
+                Nbr nb;
+                nb.init(x, y, z, p.nx, p.ny, p.nz);
+                apply_bc<Q>(f, p, slot, x, y, z, nb, n);
+            }
+        }
+        relax_and_collide<Q, OP, RHEO>(p, n, cls, slot, f);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) PV::set(in[i], lane, f[i], Lattice<Q>::w(i), p);
+    }
+    pn.launder();
+    V* out = reinterpret_cast<V*>(p.pop);
+#pragma unroll
+    for (int j = 0; j < Q; ++j, out += Np) {
+        if (!ODD) {
+            out[m] = in[lat_opp(j)];
+        } else {
+            const int cz = lat_cz(j);
+            const bool sw = (cz > 0 && seam_hi) || (cz < 0 && seam_lo);
+            out[m + pn.off(lat_cx(j), lat_cy(j), cz)] = sw ? PV::swap(in[j]) : in[j];
+        }
+    }
 }
 
 }  // namespace vlbm

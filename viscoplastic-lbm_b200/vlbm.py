@@ -28,6 +28,7 @@ D3Q19, D3Q27 = 19, 27
 OP_REGULARIZED, OP_BGK = 0, 1
 NEWTONIAN, BINGHAM, POWERLAW = 0, 1, 2
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+LAYOUT_AUTO, LAYOUT_NATURAL, LAYOUT_ZPAIR = 0, 1, 2
 (BUILDER_PERIODIC, BUILDER_PLATES_Y, BUILDER_LID_DRIVEN, BUILDER_CLOSED_BOX,
  BUILDER_SQUARE_DUCT, BUILDER_DUCT_YZ, BUILDER_LID_CAVITY_CLOSED,
  BUILDER_PLATES_Y_FREE_SLIP, BUILDER_PLATES_Y_ZOUHE) = range(9)
@@ -61,7 +62,8 @@ class Config(C.Structure):
         ("ux_bc", C.c_double * 8), ("uy_bc", C.c_double * 8),
         ("uz_bc", C.c_double * 8), ("rho_bc", C.c_double * 8),
         ("storage_scale", C.c_double),
-        ("reserved", C.c_int32 * 8),
+        ("layout", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
     @classmethod
