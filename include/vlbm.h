@@ -120,7 +120,7 @@ typedef struct vlbm_config {
 /* Population storage order.  NATURAL: planes [Q][z][y][x].  ZPAIR: nodes z and
  * z+NZ/2 of the same (x, y) are adjacent, so every stencil access of the fused
  * step is one aligned two-node vector (requires even NZ).  AUTO picks ZPAIR for
- * FP16/BF16 storage with even NZ and NATURAL otherwise.  The layout is
+ * D3Q19 with FP16/BF16 storage and even NZ, NATURAL otherwise.  The layout is
  * internal: every entry point takes and returns the [z][y][x] order. */
 enum { VLBM_LAYOUT_AUTO = 0, VLBM_LAYOUT_NATURAL = 1, VLBM_LAYOUT_ZPAIR = 2 };
 
