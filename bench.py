@@ -134,6 +134,121 @@ def cpu_baseline(vlbm, seconds_budget=15.0):
             "sample": f"{NX}x{NY}x{nz} slab of the workload, {steps} steps, FP64 oracle, {dt:.1f} s"}
 
 
+def serving_requests(vlbm, n, step_scale, seed=2024):
+    """A seeded sample of the Bingham-duct serving stream.
+
+    Per request: nx uniform in [32, 256], ny = nz uniform in [16, 96], D3Q19 or
+    D3Q27 at 50/50, tau_p uniform in [0.6, 1.2], Bingham number log-uniform in
+    [0.1, 10], 2,000-20,000 steps (times step_scale), 20 % carrying 1-4
+    movable spheres of radius 4-6 lattice units, FP16-deviation storage.  The
+    duct has walls in y and z and is periodic in x; the body force gives a
+    plane-Poiseuille centre-line speed of 0.02 across the duct width, and the
+    yield stress follows from the Bingham number with that speed and width.
+    """
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for tag in range(n):
+        nx = int(rng.integers(32, 257))
+        ny = int(rng.integers(16, 97))
+        q = 19 if rng.random() < 0.5 else 27
+        tau = float(rng.uniform(0.6, 1.2))
+        nu = (tau - 0.5) / 3.0
+        bn = float(10 ** rng.uniform(-1, 1))
+        u, h = 0.02, ny - 2
+        cfg = vlbm.Config.default(nx=nx, ny=ny, nz=ny, vel_set=q, collision=vlbm.OP_REGULARIZED,
+                                  rheology=vlbm.BINGHAM, eta_p=nu, yield_stress=bn * nu * u / h,
+                                  fx=8.0 * nu * u / (h * h), storage=vlbm.STORE_F16)
+        steps = max(1, int(round(int(rng.integers(2000, 20001)) * step_scale)))
+        spheres = []
+        if rng.random() < 0.2:
+            for _ in range(int(rng.integers(1, 5))):
+                r = float(rng.uniform(4, 6))
+                if ny - 2 * r - 5 <= 0:   # the duct is too narrow for this sphere
+                    continue
+                for _try in range(50):
+                    c = (float(rng.uniform(0, nx)), float(rng.uniform(r + 2, ny - r - 3)),
+                         float(rng.uniform(r + 2, ny - r - 3)))
+                    if all((c[0] - o.cx) ** 2 + (c[1] - o.cy) ** 2 + (c[2] - o.cz) ** 2 > (r + o.diameter / 2 + 1) ** 2
+                           for o in spheres):
+                        spheres.append(vlbm.Sphere(diameter=2 * r, cx=c[0], cy=c[1], cz=c[2], density=1.5, movable=1))
+                        break
+        out.append(dict(tag=tag, cfg=cfg, steps=steps, spheres=spheres, nodes=nx * ny * ny))
+    return out
+
+
+SERVING_IBM = dict(max_iterations=1, gx=0.0, gy=0.0, gz=-1e-5, wall_x=0, wall_y=1, wall_z=1)
+
+
+def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_resident=64, seed=2024):
+    """Continuous batching against plain one-at-a-time solves on one arrival stream.
+
+    Both arms see the same Poisson arrivals (rate requests/s).  The plain arm
+    serves them first-in first-out with one simulation at a time through the
+    public API (create, node map, spheres, step, read ux, destroy); the batched
+    arm submits each request to a vlbm_server when it arrives and pumps it.
+    Latency = time the result is handed back - arrival time; solves/s =
+    requests / (last completion - first arrival).
+    """
+    import numpy as np
+    reqs = serving_requests(vlbm, n_req, step_scale, seed)
+    arrivals = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / rate, n_req))
+    arrivals -= arrivals[0]
+    ibm = vlbm.IbmConfig.default(**SERVING_IBM)
+    lu = float(sum(r["nodes"] * r["steps"] for r in reqs))
+
+    t0 = time.perf_counter()
+    plain_lat, plain_mean = [], {}
+    for r, a in zip(reqs, arrivals):
+        now = time.perf_counter() - t0
+        if now < a:
+            time.sleep(a - now)
+        sim = vlbm.Simulation(vlbm.Config.from_buffer_copy(r["cfg"]), builder=vlbm.BUILDER_DUCT_YZ)
+        if r["spheres"]:
+            sim.add_spheres(ibm, r["spheres"])
+        sim.step(r["steps"])
+        sim.sync()
+        plain_mean[r["tag"]] = float(sim.macroscopics()["ux"].astype(np.float64).mean())
+        sim.close()
+        plain_lat.append(time.perf_counter() - t0 - a)
+    plain_span = time.perf_counter() - t0
+
+    srv = vlbm.Server(device=0, hbm_budget_bytes=int(budget_gb * 2 ** 30), max_resident=max_resident)
+    t0 = time.perf_counter()
+    nxt, done, arrive_at = 0, [], {}
+    while len(done) < n_req:
+        now = time.perf_counter() - t0
+        while nxt < n_req and arrivals[nxt] <= now:
+            r = reqs[nxt]
+            srv.submit(vlbm.Config.from_buffer_copy(r["cfg"]), vlbm.BUILDER_DUCT_YZ, r["steps"], r["tag"],
+                       r["spheres"], ibm)
+            arrive_at[r["tag"]] = arrivals[nxt]
+            nxt += 1
+        st = srv.stats()
+        if st["resident"] == 0 and st["queued"] == 0:
+            time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
+            continue
+        for c in srv.pump(200):
+            if c.status != vlbm.OK:
+                raise RuntimeError(f"serving request {c.tag} failed with status {c.status}")
+            done.append((c, time.perf_counter() - t0))
+    batched_span = time.perf_counter() - t0
+    srv.close()
+    batched_lat = [t_ret - arrive_at[c.tag] for c, t_ret in done]
+    dev = max(abs(c.mean_ux - plain_mean[c.tag]) / max(1e-30, abs(plain_mean[c.tag])) for c, _ in done)
+
+    def arm(span, lat):
+        return {"solves_per_s": n_req / span, "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "mlups": lu / span / 1e6, "makespan_s": span}
+
+    batched, plain = arm(batched_span, batched_lat), arm(plain_span, plain_lat)
+    return {"requests": n_req, "step_scale": step_scale, "arrival_rate_per_s": rate, "seed": seed,
+            "with_spheres": sum(1 for r in reqs if r["spheres"]), "lattice_updates": lu,
+            "batched": batched, "plain": plain, "speedup_solves": batched["solves_per_s"] / plain["solves_per_s"],
+            "max_rel_diff_mean_ux": dev,
+            "sample": f"{n_req} requests of the Bingham-duct serving stream, step counts x{step_scale}"}
+
+
 def run_reference(args, rank, world):
     import vlbm
     if rank != 0:
@@ -158,6 +273,10 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--layout", default="auto", choices=["auto", "natural", "zpair"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=48)
+    ap.add_argument("--serving-step-scale", type=float, default=0.25)
+    ap.add_argument("--serving-rate", type=float, default=20.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -248,6 +367,9 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(vlbm)
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        serving = serving_leg(vlbm, args.serving_requests, args.serving_step_scale, args.serving_rate)
 
     if rank == 0:
         dtype = {"f32": "f32", "f16": "f32 arithmetic, f16 storage", "bf16": "f32 arithmetic, bf16 storage"}
@@ -268,6 +390,7 @@ def main():
             "gpu_launches": args.steps,
             "kernel_variant": variant,
             "clocks": clk,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     sim.close()

@@ -2,7 +2,9 @@
 
 Tolerances (FP32 arithmetic and storage vs FP64, after <= 100 steps):
   populations  max |f_gpu - f_oracle|            <= 5e-6
-  density      max |rho_gpu - rho_oracle|         <= 1e-5
+  density      max |rho_gpu - rho_oracle|         <= 2e-5  (a sum of Q populations,
+               each within the bound above; the step takes 1/rho and |S| with the
+               hardware reciprocal and reciprocal square root, <= 2 ulp)
   velocity     relative L2 ||u_gpu - u_or||/||u_or|| <= 1e-3  (flows with |u| >~ 1e-3)
                and max abs error                  <= 2e-6 + 2e-4 * max|u|
   omega        median |d omega| <= 1e-4 * omega_p, mean <= 3e-3 * omega_p,
@@ -18,7 +20,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 POP_TOL = 5e-6
-RHO_TOL = 1e-5
+RHO_TOL = 2e-5
 U_ABS_TOL = 2e-6
 U_REL_TOL = 1e-3
 

@@ -1,0 +1,136 @@
+"""Continuous-batching server: results alone and in the mix, HBM-budget admission.
+
+Tolerance: lattices without spheres advance with the same per-node code in both
+paths (the batched kernel and the single-lattice kernel share it) and must
+match bit for bit; lattices with spheres spread their force with float atomics
+whose order differs between runs, so their velocity field must match to
+relative L2 1e-5.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REQS = [
+    # (tag, config, builder, steps, spheres)
+    (1, dict(nx=40, ny=20, nz=20, vel_set=19, rheology=1, eta_p=0.1, yield_stress=1e-5, fx=2e-5, storage=1), 5, 301, []),
+    (2, dict(nx=24, ny=24, nz=24, vel_set=27, tau=0.7, fx=1e-5, fz=-2e-5), 3, 250, []),
+    (3, dict(nx=32, ny=16, nz=16, vel_set=19, collision=1, tau=0.9, fx=1e-5), 1, 420, []),
+    (4, dict(nx=20, ny=20, nz=20, vel_set=19, tau=0.8), 3, 120,
+     [dict(diameter=6, cx=10.0, cy=10.2, cz=11.0, density=1.5, movable=1)]),
+    (5, dict(nx=33, ny=18, nz=17, vel_set=27, rheology=1, eta_p=0.2, yield_stress=1e-6, fx=3e-5, storage=1), 5, 77,
+     []),
+    # smaller spheres admitted after request 4: the staged-box shared memory of
+    # the interpolation kernel must still cover request 4's larger boxes
+    (6, dict(nx=16, ny=16, nz=16, vel_set=27, tau=0.9, storage=1), 3, 90,
+     [dict(diameter=5, cx=5.5, cy=8.0, cz=8.5, density=1.5, movable=1),
+      dict(diameter=4, cx=11.0, cy=9.0, cz=7.0, density=2.0, movable=1)]),
+    (7, dict(nx=30, ny=10, nz=14, vel_set=19, rheology=2, n_index=0.7, k_consistency=0.05, fx=2e-5, storage=2), 1,
+     33, []),
+]
+IBM_KW = dict(max_iterations=2, gx=0.0, gy=0.0, gz=-1e-5, wall_x=1, wall_y=1, wall_z=1)
+
+
+def cfg_of(vlbm, kw):
+    c = vlbm.Config.default(**kw)
+    c.layout = vlbm.LAYOUT_NATURAL
+    return c
+
+
+def alone(vlbm, kw, builder, steps, spheres):
+    sim = vlbm.Simulation(cfg_of(vlbm, kw), builder=builder)
+    if spheres:
+        sim.add_spheres(vlbm.IbmConfig.default(**IBM_KW), [vlbm.Sphere(**s) for s in spheres])
+    sim.step(steps)
+    sim.sync()
+    ux = sim.macroscopics()["ux"].ravel().copy()
+    sim.close()
+    return ux
+
+
+def drain(srv, chunk=64, limit=100000):
+    out = []
+    for _ in range(limit):
+        out += srv.pump(chunk)
+        st = srv.stats()
+        if st["resident"] == 0 and st["queued"] == 0:
+            return out + srv.pump(1)
+    raise AssertionError("server did not drain")
+
+
+def test_results_same_alone_and_in_the_mix(vlbm):
+    srv = vlbm.Server(device=0, hbm_budget_bytes=4 << 30, max_resident=8)
+    for tag, kw, builder, steps, spheres in REQS:
+        srv.submit(cfg_of(vlbm, kw), builder, steps, tag, [vlbm.Sphere(**s) for s in spheres],
+                   vlbm.IbmConfig.default(**IBM_KW))
+    done = {c.tag: c for c in drain(srv)}
+    assert sorted(done) == [r[0] for r in REQS]
+    for tag, kw, builder, steps, spheres in REQS:
+        c = done[tag]
+        assert c.status == vlbm.OK and c.steps == steps
+        assert c.submit_time_s <= c.start_time_s <= c.finish_time_s
+        n = kw["nx"] * kw["ny"] * kw["nz"]
+        mix = srv.fetch(tag, n)
+        ref = alone(vlbm, kw, builder, steps, spheres)
+        if spheres:
+            assert np.linalg.norm(mix - ref) <= 1e-5 * np.linalg.norm(ref), tag
+        else:
+            np.testing.assert_array_equal(mix, ref, err_msg=f"request {tag}")
+        assert abs(c.mean_ux - ref.astype(np.float64).mean()) <= 1e-7 + 1e-5 * abs(ref.mean())
+    srv.close()
+
+
+def test_late_arrivals_join_running_batch(vlbm):
+    """Requests submitted while others are on the GPU give the same results."""
+    srv = vlbm.Server(device=0, hbm_budget_bytes=4 << 30, max_resident=4)
+    a = dict(nx=24, ny=12, nz=12, vel_set=19, rheology=1, eta_p=0.15, yield_stress=1e-5, fx=3e-5, storage=1)
+    b = dict(nx=18, ny=14, nz=10, vel_set=27, tau=0.75, fx=2e-5)
+    srv.submit(cfg_of(vlbm, a), 5, 200, 10)
+    got = srv.pump(37)
+    srv.submit(cfg_of(vlbm, b), 5, 101, 11)
+    got += srv.pump(13)
+    srv.submit(cfg_of(vlbm, a), 5, 55, 12)
+    got += drain(srv, chunk=17)
+    assert sorted(c.tag for c in got) == [10, 11, 12]
+    for tag, kw, steps in [(10, a, 200), (11, b, 101), (12, a, 55)]:
+        ref = alone(vlbm, kw, 5, steps, [])
+        np.testing.assert_array_equal(srv.fetch(tag, ref.size), ref, err_msg=f"request {tag}")
+    srv.close()
+
+
+def request_bytes(q, nx, ny, nz, store_bytes=4):
+    """The server's admission estimate for a sphere-free Newtonian/Bingham lattice."""
+    n = nx * ny * nz
+    walls = 2 * (nx * ny + ny * nz + nx * nz)
+    return q * n * store_bytes + 25 * n + (1 << 20) + walls * (2 * q * 4 + 24)
+
+
+def test_budget_admission_limits_residency(vlbm):
+    one = request_bytes(19, 32, 32, 32)
+    srv = vlbm.Server(device=0, hbm_budget_bytes=int(one * 1.5), max_resident=8)
+    kw = dict(nx=32, ny=32, nz=32, tau=0.8, fx=1e-5)
+    for tag in range(4):
+        srv.submit(cfg_of(vlbm, kw), vlbm.BUILDER_PLATES_Y, 50 + 10 * tag, tag)
+    peak, done = 0, []
+    for _ in range(1000):
+        done += srv.pump(7)
+        st = srv.stats()
+        peak = max(peak, st["resident"])
+        assert st["bytes"] <= one * 1.5
+        if st["resident"] == 0 and st["queued"] == 0:
+            break
+    assert peak == 1
+    assert sorted(c.tag for c in done) == [0, 1, 2, 3]
+    assert srv.stats()["bytes"] == 0
+    srv.close()
+
+
+def test_oversized_and_invalid_requests_rejected(vlbm):
+    srv = vlbm.Server(device=0, hbm_budget_bytes=64 << 20, max_resident=2)
+    with pytest.raises(vlbm.VlbmError):
+        srv.submit(cfg_of(vlbm, dict(nx=128, ny=128, nz=128)), vlbm.BUILDER_PLATES_Y, 10, 1)
+    with pytest.raises(vlbm.VlbmError):
+        srv.submit(cfg_of(vlbm, dict(nx=8, ny=8, nz=8, tau=0.3)), vlbm.BUILDER_PLATES_Y, 10, 2)
+    with pytest.raises(vlbm.VlbmError):
+        srv.submit(cfg_of(vlbm, dict(nx=8, ny=8, nz=8)), vlbm.BUILDER_PLATES_Y, 0, 3)
+    srv.close()

@@ -38,4 +38,29 @@ cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in,
 #undef C_
 }
 
+cudaError_t launch_batched(int Q, int st, const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid,
+                           int op, int rheo, cudaStream_t s) {
+#define C_(QQ, SS) launch_batched_st<QQ, SS>(slots, table, ntiles, grid, op, rheo, s)
+    VLBM_SELECT(C_)
+#undef C_
+}
+
+#define VLBM_SELECT_INT(CALL)                                                      \
+    if (Q == 19) {                                                                 \
+        if (st == VLBM_STORE_F32) return CALL(19, VLBM_STORE_F32);                 \
+        if (st == VLBM_STORE_F16) return CALL(19, VLBM_STORE_F16);                 \
+        if (st == VLBM_STORE_BF16) return CALL(19, VLBM_STORE_BF16);               \
+    } else if (Q == 27) {                                                          \
+        if (st == VLBM_STORE_F32) return CALL(27, VLBM_STORE_F32);                 \
+        if (st == VLBM_STORE_F16) return CALL(27, VLBM_STORE_F16);                 \
+        if (st == VLBM_STORE_BF16) return CALL(27, VLBM_STORE_BF16);               \
+    }                                                                              \
+    return 0;
+
+int batched_blocks_per_sm(int Q, int st, int op, int rheo) {
+#define C_(QQ, SS) batched_occupancy_st<QQ, SS>(op, rheo)
+    VLBM_SELECT_INT(C_)
+#undef C_
+}
+
 }  // namespace vlbm

@@ -89,11 +89,52 @@ cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, 
     return cudaGetLastError();
 }
 
+template <int Q, int OP, int ST>
+cudaError_t batched_rh(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, int rheo,
+                       cudaStream_t s) {
+    switch (rheo) {
+    case VLBM_NEWTONIAN: k_step_batched<Q, OP, VLBM_NEWTONIAN, ST><<<grid, 256, 0, s>>>(slots, table, ntiles); break;
+    case VLBM_BINGHAM: k_step_batched<Q, OP, VLBM_BINGHAM, ST><<<grid, 256, 0, s>>>(slots, table, ntiles); break;
+    case VLBM_POWERLAW: k_step_batched<Q, OP, VLBM_POWERLAW, ST><<<grid, 256, 0, s>>>(slots, table, ntiles); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <int Q, int ST>
+cudaError_t launch_batched_st(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, int op,
+                              int rheo, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    if (op == VLBM_OP_BGK) return batched_rh<Q, VLBM_OP_BGK, ST>(slots, table, ntiles, grid, rheo, s);
+    return batched_rh<Q, VLBM_OP_REGULARIZED, ST>(slots, table, ntiles, grid, rheo, s);
+}
+
+template <int Q, int OP, int ST>
+int occ_rh(int rheo) {
+    int nb = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (rheo) {
+    case VLBM_NEWTONIAN: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_batched<Q, OP, VLBM_NEWTONIAN, ST>, 256, 0); break;
+    case VLBM_BINGHAM: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_batched<Q, OP, VLBM_BINGHAM, ST>, 256, 0); break;
+    case VLBM_POWERLAW: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_batched<Q, OP, VLBM_POWERLAW, ST>, 256, 0); break;
+    }
+    return e == cudaSuccess ? nb : 0;
+}
+
+template <int Q, int ST>
+int batched_occupancy_st(int op, int rheo) {
+    if (op == VLBM_OP_BGK) return occ_rh<Q, VLBM_OP_BGK, ST>(rheo);
+    return occ_rh<Q, VLBM_OP_REGULARIZED, ST>(rheo);
+}
+
 #define VLBM_INSTANTIATE(QQ, SS)                                                                              \
     template cudaError_t launch_step_st<QQ, SS>(const StepParams&, int, int, bool, LaunchShape, cudaStream_t); \
     template cudaError_t launch_macro_st<QQ, SS>(const MacroParams&, int, bool, cudaStream_t);                 \
     template cudaError_t launch_get_pops_st<QQ, SS>(const StepParams&, bool, float*, cudaStream_t);            \
     template cudaError_t launch_set_pops_st<QQ, SS>(const StepParams&, const float*, float, float, float, float, \
-                                                    cudaStream_t);
+                                                    cudaStream_t);                                              \
+    template cudaError_t launch_batched_st<QQ, SS>(const BatchSlot*, const BatchBlock*, int, int, int, int,      \
+                                                   cudaStream_t);                                               \
+    template int batched_occupancy_st<QQ, SS>(int, int);
 
 }  // namespace vlbm

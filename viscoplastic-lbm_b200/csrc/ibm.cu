@@ -962,9 +962,12 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
         maxbox = std::max(maxbox, bx * by * bz);
     }
     st->smem_nodes = std::min(maxbox, IBM_SMEM_MAX_NODES);
+    // the attribute is one value per kernel and device, shared by every
+    // simulation in the process: always allow the largest box, so a later
+    // simulation with smaller spheres cannot lower the limit under an earlier one
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_ibm_interp_spread, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 st->smem_nodes * 4 * (int)sizeof(float));
+                                 IBM_SMEM_MAX_NODES * 4 * (int)sizeof(float));
     if (e != cudaSuccess) { ibm_destroy(st); return cuda_status(e, "IBM setup"); }
     st->initial = parts;
     st->init_nodes.resize(3 * nn);

@@ -524,11 +524,9 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned 
 // at 4 resident 256-thread blocks per SM (64 registers) keeps enough loads in
 // flight to saturate HBM.
 template <int Q, int OP, int RHEO, int ST, bool ODD>
-__global__ void __launch_bounds__(256) k_step(const StepParams p) {
+__device__ __forceinline__ void step_node(const StepParams& p, unsigned n) {
     using S = Store<ST>;
     using T = typename S::T;
-    const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= (unsigned)p.N) return;
     const int x = (int)(n % (unsigned)p.nx);
     const unsigned t = n / (unsigned)p.nx;
     const int y = (int)(t % (unsigned)p.ny);
@@ -551,6 +549,64 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
         } else {     // plane j receives population j streamed to the downstream node
             const unsigned dst = n + nb.off(lat_cx(j), lat_cy(j), lat_cz(j));
             S::st(plane + dst, f[j], Lattice<Q>::w(j), p);
+        }
+    }
+}
+
+template <int Q, int OP, int RHEO, int ST, bool ODD>
+__global__ void __launch_bounds__(256) k_step(const StepParams p) {
+    const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= (unsigned)p.N) return;
+    step_node<Q, OP, RHEO, ST, ODD>(p, n);
+}
+
+// ------------------------------------------------------- batched step --
+// Many lattices of one (velocity set, operator, rheology, storage) group
+// advance in one launch.  The launch walks a table of tiles (lattice slot,
+// first node; BATCH_TILE consecutive nodes each) with a grid-stride loop, so a
+// grid of a few blocks per SM is persistent over all lattices.  The step state
+// of every lattice (AA parity, which side-store buffer is current, whether the
+// boundary rule applies) lives in its slot in device memory and is advanced by
+// k_batch_advance after the group launches, so one captured step can be
+// replayed any number of times.
+constexpr int BATCH_TILE = 256;
+
+struct BatchSlot {
+    StepParams p;
+    float* side[2];
+    int parity, side_cur, apply_bc, pad;
+};
+struct BatchBlock {
+    int slot;           // lattice of this tile
+    unsigned first;     // first node of this tile
+};
+
+template <int Q, int OP, int RHEO, int ST>
+__global__ void __launch_bounds__(256) k_step_batched(const BatchSlot* __restrict__ slots,
+                                                      const BatchBlock* __restrict__ table, int ntiles) {
+    __shared__ StepParams sp;
+    __shared__ int odd;
+    constexpr int WORDS = (int)(sizeof(StepParams) / 4);
+    static_assert(sizeof(StepParams) % 4 == 0, "StepParams is copied as 32-bit words");
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchBlock e = table[t];
+        const BatchSlot* s = slots + e.slot;
+        __syncthreads();   // the previous tile is done with sp
+        if (threadIdx.x < WORDS)
+            reinterpret_cast<unsigned*>(&sp)[threadIdx.x] = reinterpret_cast<const unsigned*>(&s->p)[threadIdx.x];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int cur = s->side_cur;
+            sp.side_prev = s->side[cur];
+            sp.side_next = s->side[cur ^ 1];
+            sp.apply_bc = s->apply_bc;
+            odd = s->parity;
+        }
+        __syncthreads();
+        const unsigned n = e.first + threadIdx.x;
+        if (n < (unsigned)sp.N) {
+            if (odd) step_node<Q, OP, RHEO, ST, true>(sp, n);
+            else step_node<Q, OP, RHEO, ST, false>(sp, n);
         }
     }
 }
