@@ -183,10 +183,12 @@ SERVING_IBM = dict(max_iterations=1, gx=0.0, gy=0.0, gz=-1e-5, wall_x=0, wall_y=
 def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_resident=64, seed=2024):
     """Continuous batching against plain one-at-a-time solves on one arrival stream.
 
-    Both arms see the same Poisson arrivals (rate requests/s).  The plain arm
-    serves them first-in first-out with one simulation at a time through the
-    public API (create, node map, spheres, step, read ux, destroy); the batched
-    arm submits each request to a vlbm_server when it arrives and pumps it.
+    Both arms see the same Poisson arrivals (rate requests/s) and use the same
+    population layout, so they compute the same numbers (checked: ux fields
+    compared bit for bit).  The plain arm serves the requests first-in
+    first-out with one simulation at a time through the public API (create,
+    node map, spheres, step, read ux, destroy); the batched arm submits each
+    request to a vlbm_server when it arrives and pumps it.
     Latency = time the result is handed back - arrival time; solves/s =
     requests / (last completion - first arrival).
     """
@@ -197,18 +199,23 @@ def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_
     ibm = vlbm.IbmConfig.default(**SERVING_IBM)
     lu = float(sum(r["nodes"] * r["steps"] for r in reqs))
 
+    def natural(cfg):
+        c = vlbm.Config.from_buffer_copy(cfg)
+        c.layout = vlbm.LAYOUT_NATURAL   # the server's layout: both arms compute the same numbers
+        return c
+
     t0 = time.perf_counter()
-    plain_lat, plain_mean = [], {}
+    plain_lat, plain_ux = [], {}
     for r, a in zip(reqs, arrivals):
         now = time.perf_counter() - t0
         if now < a:
             time.sleep(a - now)
-        sim = vlbm.Simulation(vlbm.Config.from_buffer_copy(r["cfg"]), builder=vlbm.BUILDER_DUCT_YZ)
+        sim = vlbm.Simulation(natural(r["cfg"]), builder=vlbm.BUILDER_DUCT_YZ)
         if r["spheres"]:
             sim.add_spheres(ibm, r["spheres"])
         sim.step(r["steps"])
         sim.sync()
-        plain_mean[r["tag"]] = float(sim.macroscopics()["ux"].astype(np.float64).mean())
+        plain_ux[r["tag"]] = sim.macroscopics()["ux"].ravel().copy()
         sim.close()
         plain_lat.append(time.perf_counter() - t0 - a)
     plain_span = time.perf_counter() - t0
@@ -220,8 +227,7 @@ def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_
         now = time.perf_counter() - t0
         while nxt < n_req and arrivals[nxt] <= now:
             r = reqs[nxt]
-            srv.submit(vlbm.Config.from_buffer_copy(r["cfg"]), vlbm.BUILDER_DUCT_YZ, r["steps"], r["tag"],
-                       r["spheres"], ibm)
+            srv.submit(natural(r["cfg"]), vlbm.BUILDER_DUCT_YZ, r["steps"], r["tag"], r["spheres"], ibm)
             arrive_at[r["tag"]] = arrivals[nxt]
             nxt += 1
         st = srv.stats()
@@ -233,9 +239,21 @@ def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_
                 raise RuntimeError(f"serving request {c.tag} failed with status {c.status}")
             done.append((c, time.perf_counter() - t0))
     batched_span = time.perf_counter() - t0
+    host_profile = srv.profile()
+    same, dev, differing = 0, 0.0, []
+    by_tag = {r["tag"]: r for r in reqs}
+    for c, _ in done:
+        ref = plain_ux[c.tag]
+        got = srv.fetch(c.tag, ref.size)
+        same += int(np.array_equal(got, ref))
+        rel = float(np.linalg.norm(got - ref) / max(1e-30, np.linalg.norm(ref)))
+        dev = max(dev, rel)
+        if rel > 0:
+            r = by_tag[c.tag]
+            differing.append({"tag": c.tag, "q": r["cfg"].vel_set, "nodes": r["nodes"], "steps": r["steps"],
+                              "spheres": len(r["spheres"]), "rel_l2": rel})
     srv.close()
     batched_lat = [t_ret - arrive_at[c.tag] for c, t_ret in done]
-    dev = max(abs(c.mean_ux - plain_mean[c.tag]) / max(1e-30, abs(plain_mean[c.tag])) for c, _ in done)
 
     def arm(span, lat):
         return {"solves_per_s": n_req / span, "p50_s": float(np.percentile(lat, 50)),
@@ -245,7 +263,7 @@ def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_
     return {"requests": n_req, "step_scale": step_scale, "arrival_rate_per_s": rate, "seed": seed,
             "with_spheres": sum(1 for r in reqs if r["spheres"]), "lattice_updates": lu,
             "batched": batched, "plain": plain, "speedup_solves": batched["solves_per_s"] / plain["solves_per_s"],
-            "max_rel_diff_mean_ux": dev,
+            "server_host_seconds": host_profile, "results_bitwise_equal": same, "max_rel_l2_diff_ux": dev, "differing": differing,
             "sample": f"{n_req} requests of the Bingham-duct serving stream, step counts x{step_scale}"}
 
 

@@ -306,6 +306,11 @@ vlbm_status vlbm_server_stats(vlbm_server* srv, int32_t* resident, int32_t* queu
                               int64_t* bytes_in_use, double* lattice_updates);
 /* Copy the macroscopics of the finished request `tag` (kept until fetched). */
 vlbm_status vlbm_server_fetch(vlbm_server* srv, uint64_t tag, float* ux, size_t n);
+/* Host seconds the server spent, since creation, in: [0] admission (building
+ * new lattices), [1] table rebuilds and graph captures, [2] enqueuing steps,
+ * [3] waiting for the GPU (queue depth limit, idle read-outs), [4] completing
+ * read-outs.  Writes min(n, 5) values. */
+vlbm_status vlbm_server_profile(vlbm_server* srv, double* seconds, int32_t n);
 vlbm_status vlbm_server_destroy(vlbm_server* srv);
 
 /* --------------------------------------------------------------- misc --- */

@@ -91,9 +91,20 @@ vlbm_status fluid_step(vlbm_sim* s) {
     return VLBM_OK;
 }
 
+cudaError_t alloc_with(DeviceAllocator* a, void** p, size_t bytes) {
+    return a ? a->allocate(p, bytes) : cudaMalloc(p, bytes);
+}
+void free_with(DeviceAllocator* a, void* p) {
+    if (!p) return;
+    if (a) a->release(p);
+    else cudaFree(p);
+}
+cudaError_t sim_malloc(vlbm_sim* s, void** p, size_t bytes) { return alloc_with(s->allocator, p, bytes); }
+void sim_free(vlbm_sim* s, void* p) { free_with(s->allocator, p); }
+
 static vlbm_status alloc_dev(vlbm_sim* s, void** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc");
+    cudaError_t e = sim_malloc(s, p, bytes);
+    if (e != cudaSuccess) return cuda_status(e, "device allocation");
     s->device_bytes += bytes;
     return VLBM_OK;
 }
@@ -137,9 +148,10 @@ static vlbm_status ensure_scratch(vlbm_sim* s) {
 using namespace vlbm;
 
 vlbm_sim::~vlbm_sim() {
-    if (ibm) { ibm_destroy(ibm); ibm = nullptr; }
-    cudaFree(pop); cudaFree(cls); cudaFree(bc_slot); cudaFree(bc);
-    cudaFree(side[0]); cudaFree(side[1]); cudaFree(omega); cudaFree(fibm); cudaFree(err); cudaFree(scratch); cudaFree(red_scratch);
+    if (ibm) { ibm_destroy(ibm, allocator); ibm = nullptr; }
+    for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)side[0], (void*)side[1], (void*)omega,
+                    (void*)fibm, (void*)err, (void*)scratch, (void*)red_scratch})
+        free_with(allocator, p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -181,7 +193,17 @@ vlbm_status vlbm_config_default(vlbm_config* c) {
     return VLBM_OK;
 }
 
-vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) {
+vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) { return sim_create(cfg, nullptr, out); }
+
+}  // extern "C"
+
+void vlbm::sim_release(vlbm_sim* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    delete s;
+}
+
+vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator, vlbm_sim** out) {
     if (!cfg || !out) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
     *out = nullptr;
     std::string why;
@@ -190,6 +212,7 @@ vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) {
     cudaError_t e = cudaSetDevice(cfg->device);
     if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
     vlbm_sim* s = new vlbm_sim();
+    s->allocator = allocator;
     s->cfg = *cfg;
     s->Q = cfg->vel_set;
     s->N = (long long)cfg->nx * cfg->ny * cfg->nz;
@@ -233,6 +256,8 @@ vlbm_status vlbm_create(const vlbm_config* cfg, vlbm_sim** out) {
     return VLBM_OK;
 }
 
+extern "C" {
+
 vlbm_status vlbm_destroy(vlbm_sim* s) {
     if (!s) return VLBM_OK;
     cudaSetDevice(s->device);
@@ -249,7 +274,7 @@ vlbm_status vlbm_set_node_map(vlbm_sim* s, const uint32_t* map, size_t n) {
     vlbm_status st = build_bc_tables(s->cfg, map, n, t, why);
     if (st != VLBM_OK) { set_last_error(why); return st; }
     VLBM_CUDA(cudaStreamSynchronize(s->stream));
-    cudaFree(s->bc); cudaFree(s->side[0]); cudaFree(s->side[1]);
+    sim_free(s, s->bc); sim_free(s, s->side[0]); sim_free(s, s->side[1]);
     s->bc = nullptr; s->side[0] = s->side[1] = nullptr;
     s->nbc = (int)t.recs.size();
     VLBM_CUDA(cudaMemcpy(s->cls, t.cls.data(), t.cls.size(), cudaMemcpyHostToDevice));

@@ -39,8 +39,8 @@ cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in,
 }
 
 cudaError_t launch_batched(int Q, int st, const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid,
-                           int op, int rheo, cudaStream_t s) {
-#define C_(QQ, SS) launch_batched_st<QQ, SS>(slots, table, ntiles, grid, op, rheo, s)
+                           bool odd, int op, int rheo, cudaStream_t s) {
+#define C_(QQ, SS) launch_batched_st<QQ, SS>(slots, table, ntiles, grid, odd, op, rheo, s)
     VLBM_SELECT(C_)
 #undef C_
 }

@@ -24,7 +24,7 @@ cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, 
 struct BatchSlot;
 struct BatchBlock;
 template <int Q, int ST>
-cudaError_t launch_batched_st(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, int op,
+cudaError_t launch_batched_st(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, bool odd, int op,
                               int rheo, cudaStream_t s);
 
 // Run-time selection over (Q, storage).
@@ -34,10 +34,11 @@ cudaError_t launch_macro(int Q, int st, const MacroParams& mp, int rheo, bool od
 cudaError_t launch_get_pops(int Q, int st, const StepParams& p, bool odd, float* out, cudaStream_t s);
 cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in, float rho, float ux, float uy,
                             float uz, cudaStream_t s);
-// One batched step of every lattice of a (Q, storage, op, rheology) group:
-// ntiles table entries walked by `grid` persistent blocks of 256 threads.
+// One batched step of the lattices of a (Q, storage, op, rheology) group that
+// share the AA parity `odd`: ntiles table entries walked by `grid` persistent
+// blocks of 256 threads.
 cudaError_t launch_batched(int Q, int st, const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid,
-                           int op, int rheo, cudaStream_t s);
+                           bool odd, int op, int rheo, cudaStream_t s);
 // Resident 256-thread blocks per SM of the batched kernel of a group.
 int batched_blocks_per_sm(int Q, int st, int op, int rheo);
 template <int Q, int ST>

@@ -89,36 +89,52 @@ cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, 
     return cudaGetLastError();
 }
 
-template <int Q, int OP, int ST>
-cudaError_t batched_rh(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, int rheo,
-                       cudaStream_t s) {
-    switch (rheo) {
-    case VLBM_NEWTONIAN: k_step_batched<Q, OP, VLBM_NEWTONIAN, ST><<<grid, 256, 0, s>>>(slots, table, ntiles); break;
-    case VLBM_BINGHAM: k_step_batched<Q, OP, VLBM_BINGHAM, ST><<<grid, 256, 0, s>>>(slots, table, ntiles); break;
-    case VLBM_POWERLAW: k_step_batched<Q, OP, VLBM_POWERLAW, ST><<<grid, 256, 0, s>>>(slots, table, ntiles); break;
-    default: return cudaErrorInvalidValue;
-    }
+template <int Q, int OP, int RHEO, int ST>
+cudaError_t batched_t(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, bool odd,
+                      cudaStream_t s) {
+    if (odd) k_step_batched<Q, OP, RHEO, ST, true><<<grid, 256, 0, s>>>(slots, table, ntiles);
+    else k_step_batched<Q, OP, RHEO, ST, false><<<grid, 256, 0, s>>>(slots, table, ntiles);
     return cudaGetLastError();
 }
 
+template <int Q, int OP, int ST>
+cudaError_t batched_rh(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, bool odd, int rheo,
+                       cudaStream_t s) {
+    switch (rheo) {
+    case VLBM_NEWTONIAN: return batched_t<Q, OP, VLBM_NEWTONIAN, ST>(slots, table, ntiles, grid, odd, s);
+    case VLBM_BINGHAM: return batched_t<Q, OP, VLBM_BINGHAM, ST>(slots, table, ntiles, grid, odd, s);
+    case VLBM_POWERLAW: return batched_t<Q, OP, VLBM_POWERLAW, ST>(slots, table, ntiles, grid, odd, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
 template <int Q, int ST>
-cudaError_t launch_batched_st(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, int op,
+cudaError_t launch_batched_st(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, bool odd, int op,
                               int rheo, cudaStream_t s) {
     if (ntiles <= 0) return cudaSuccess;
-    if (op == VLBM_OP_BGK) return batched_rh<Q, VLBM_OP_BGK, ST>(slots, table, ntiles, grid, rheo, s);
-    return batched_rh<Q, VLBM_OP_REGULARIZED, ST>(slots, table, ntiles, grid, rheo, s);
+    if (op == VLBM_OP_BGK) return batched_rh<Q, VLBM_OP_BGK, ST>(slots, table, ntiles, grid, odd, rheo, s);
+    return batched_rh<Q, VLBM_OP_REGULARIZED, ST>(slots, table, ntiles, grid, odd, rheo, s);
+}
+
+// resident blocks per SM: the smaller of the two parities
+template <int Q, int OP, int RHEO, int ST>
+int occ_t() {
+    int a = 0, b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_step_batched<Q, OP, RHEO, ST, false>, 256, 0) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_step_batched<Q, OP, RHEO, ST, true>, 256, 0) != cudaSuccess)
+        return 0;
+    return a < b ? a : b;
 }
 
 template <int Q, int OP, int ST>
 int occ_rh(int rheo) {
-    int nb = 0;
-    cudaError_t e = cudaErrorInvalidValue;
     switch (rheo) {
-    case VLBM_NEWTONIAN: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_batched<Q, OP, VLBM_NEWTONIAN, ST>, 256, 0); break;
-    case VLBM_BINGHAM: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_batched<Q, OP, VLBM_BINGHAM, ST>, 256, 0); break;
-    case VLBM_POWERLAW: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_batched<Q, OP, VLBM_POWERLAW, ST>, 256, 0); break;
+    case VLBM_NEWTONIAN: return occ_t<Q, OP, VLBM_NEWTONIAN, ST>();
+    case VLBM_BINGHAM: return occ_t<Q, OP, VLBM_BINGHAM, ST>();
+    case VLBM_POWERLAW: return occ_t<Q, OP, VLBM_POWERLAW, ST>();
     }
-    return e == cudaSuccess ? nb : 0;
+    return 0;
 }
 
 template <int Q, int ST>
@@ -133,7 +149,7 @@ int batched_occupancy_st(int op, int rheo) {
     template cudaError_t launch_get_pops_st<QQ, SS>(const StepParams&, bool, float*, cudaStream_t);            \
     template cudaError_t launch_set_pops_st<QQ, SS>(const StepParams&, const float*, float, float, float, float, \
                                                     cudaStream_t);                                              \
-    template cudaError_t launch_batched_st<QQ, SS>(const BatchSlot*, const BatchBlock*, int, int, int, int,      \
+    template cudaError_t launch_batched_st<QQ, SS>(const BatchSlot*, const BatchBlock*, int, int, bool, int, int, \
                                                    cudaStream_t);                                               \
     template int batched_occupancy_st<QQ, SS>(int, int);
 

@@ -15,16 +15,19 @@
 //   k_ibm_contacts   one CTA: old values, Hertz-Mindlin contacts with
 //                    deterministic slot updates and sums, predictor
 //   per multi-direct-forcing iteration:
-//     k_ibm_interp_spread  one CTA per sphere: the box's rho,u staged in shared
-//                    memory, Peskin 4-point interpolation, direct forcing, the
-//                    spread accumulated in shared memory and flushed once with
-//                    global atomics; sphere force/torque by block reduction
-//     k_ibm_update   particle velocity/rotation update
+//     k_ibm_interp_spread  several CTAs per sphere, one warp per Lagrangian
+//                    node with its 64 stencil points split over the lanes:
+//                    Peskin 4-point interpolation (warp reduction), direct
+//                    forcing, spreading with global atomics; per-CTA
+//                    force/torque partials
+//     k_ibm_update   partials added in a fixed order, particle velocity and
+//                    rotation update
 //     k_ibm_euler    over the node list: u += fAux/(2 rho), F += fAux, fAux = 0
 //   k_ibm_move / k_ibm_move_nodes   particle and Lagrangian node movement
 //
 // Particle state, contacts and integration are FP64; the Eulerian fields FP32.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -35,7 +38,8 @@ namespace vlbm {
 
 constexpr int IBM_MAX_SLOTS = 13;           // MAX_ACTIVE_COLLISIONS, ibmBoundaryCondition.h:78
 constexpr int IBM_THREADS = 256;
-constexpr int IBM_SMEM_MAX_NODES = 13312;   // 13312 * 16 B = 208 KB of staged rho,u
+constexpr int IBM_NODES_PER_CTA = 32;       // Lagrangian nodes per CTA of k_ibm_interp_spread (4 per warp)
+constexpr int IBM_MAX_SPLIT = 32;           // CTAs per sphere, at most
 constexpr int IBM_MAX_PARTICLES = 1024;   // pair buffer np*np*6 doubles <= 50 MB
 
 struct DPart {
@@ -66,11 +70,15 @@ struct IbmState {
     double *nx = nullptr, *ny = nullptr, *nz = nullptr, *nS = nullptr;
     double *nfx = nullptr, *nfy = nullptr, *nfz = nullptr, *ndx = nullptr, *ndy = nullptr, *ndz = nullptr;
     int* npid = nullptr;
-    float* fields = nullptr;      // [4][N] rho,ux,uy,uz (IBM macroscopics) + [3][N] fAux
+    float* fields = nullptr;      // [4][N] rho,ux,uy,uz (IBM macroscopics)
+    unsigned long long* faux = nullptr;   // [3][N] spread force, fixed point (IBM_FIX_SCALE)
     int* list = nullptr;          // [N] touched Eulerian nodes
-    int* count = nullptr;
+    int* count = nullptr;         // [0]: touched-node count, [1]: IBM steps taken (contact history clock)
     double* contrib = nullptr;    // [np][np][6] pair force/torque on the row particle
-    int smem_nodes = 0;           // staged box capacity of k_ibm_interp_spread
+    double* fpart = nullptr;      // [np][split][6] per-CTA force/torque partials
+    int split = 1;                // CTAs per sphere in k_ibm_interp_spread
+    int gsplit = 1;               // CTAs per sphere in k_ibm_gather
+    long long euler_blocks = 1;   // grid of k_ibm_euler (grid-stride over the node list)
     std::vector<DPart> initial;   // for vlbm_init_equilibrium
     std::vector<double> init_nodes;
     size_t bytes = 0;
@@ -178,12 +186,14 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_box(IbmParams P, DPart* par
 // -------------------------------------------------------------- gather --
 template <int Q, int ST, bool ODD, bool PAIRED>
 __global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmParams P, const DPart* parts,
-                                                             float* fields, int* list, int* count) {
-    const DPart& p = parts[blockIdx.x];
+                                                             float* fields, int* list, int* count, int split) {
+    // `split` CTAs per sphere share its box
+    const DPart& p = parts[blockIdx.x / split];
+    const int sub = blockIdx.x % split;
     const int bx = p.box_n[0], by = p.box_n[1], bz = p.box_n[2];
     const long long tot = (long long)bx * by * bz;
     const size_t N = (size_t)sp.N;
-    for (long long k = threadIdx.x; k < tot; k += blockDim.x) {
+    for (long long k = (long long)sub * blockDim.x + threadIdx.x; k < tot; k += (long long)split * blockDim.x) {
         const int ix = (int)(k % bx), iy = (int)((k / bx) % by), iz = (int)(k / ((long long)bx * by));
         const int x = wrapi(p.box_lo[0] + ix, P.nx), y = wrapi(p.box_lo[1] + iy, P.ny), z = wrapi(p.box_lo[2] + iz, P.nz);
         const unsigned n = (unsigned)(((size_t)z * P.ny + y) * P.nx + x);
@@ -386,7 +396,11 @@ __device__ void update_center(const IbmParams& P, DPart& p) {
     for (int a = 0; a < 3; ++a) p.w[a] = wn[a];
 }
 
-__global__ void __launch_bounds__(IBM_THREADS) k_ibm_contacts(IbmParams P, DPart* parts, double* contrib) {
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_contacts(IbmParams P, DPart* parts, double* contrib,
+                                                              const int* steps_taken) {
+    // index of the fluid step just taken (main.cu:270); read on the device so a
+    // captured IBM step can be replayed
+    P.step = *steps_taken;
     const int np = P.np;
     // gpuUpdateParticleOldValues ibm.cu:995-1042
     for (int i = threadIdx.x; i < np; i += blockDim.x) {
@@ -481,66 +495,92 @@ __device__ __forceinline__ NodeStencil node_stencil(const IbmParams& P, const DP
     return s;
 }
 
-__global__ void __launch_bounds__(IBM_THREADS) k_ibm_interp_spread(IbmParams P, DPart* parts, const double* X,
+// Spread force in 2^-48 fixed point, summed with 64-bit integer atomics: the
+// sum does not depend on the order of the additions, so a lattice's IBM step is
+// bit-reproducible from run to run and alone or among other lattices.
+// Resolution 3.6e-15 per contribution (below the FP32 rounding of any
+// contribution above 1e-7), range +-32768 for the sum at one node.
+constexpr double IBM_FIX_SCALE = 281474976710656.0;   // 2^48
+__device__ __forceinline__ unsigned long long to_fix(float v) {
+    return (unsigned long long)__double2ll_rn((double)v * IBM_FIX_SCALE);
+}
+__device__ __forceinline__ float from_fix(unsigned long long v) {
+    return (float)((double)(long long)v * (1.0 / IBM_FIX_SCALE));
+}
+
+// Lattice index of a box-relative offset: the offsets stay within one period
+// of the lattice except when a periodic axis is shorter than the stencil box.
+__device__ __forceinline__ int wrap_near(int v, int n) {
+    if (v < 0) v += n;
+    else if (v >= n) v -= n;
+    if ((unsigned)v >= (unsigned)n) v = wrapi(v, n);
+    return v;
+}
+
+// Interpolation, direct forcing and spreading (ibm.cu:307-541).  One warp per
+// Lagrangian node, its 4x4x4 stencil split over the lanes (points q and q+32);
+// a sphere's nodes are shared by IBM_SPLIT CTAs.  The interpolation reads the
+// IBM macroscopic fields and the spreading adds into the auxiliary force field,
+// two different arrays, so each node spreads right after its own
+// interpolation, in the same warp.  Each CTA writes its sphere force/torque
+// partial to fpart[sphere][split][6]; k_ibm_update adds the partials in a fixed
+// order.
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_interp_spread(IbmParams P, const DPart* parts, const double* X,
                                                                     const double* Y, const double* Z, const double* S,
                                                                     double* nfx, double* nfy, double* nfz, double* ndx,
-                                                                    double* ndy, double* ndz, float* fields, int smem_nodes) {
-    extern __shared__ float sm[];
+                                                                    double* ndy, double* ndz, const float* fields,
+                                                                    unsigned long long* faux, double* fpart,
+                                                                    int split) {
     __shared__ double red[32];
-    DPart& p = parts[blockIdx.x];
+    const int sphere = blockIdx.x / split, sub = blockIdx.x % split;
+    const DPart& p = parts[sphere];
     const size_t N = (size_t)P.nx * P.ny * P.nz;
-    const int bx = p.box_n[0], by = p.box_n[1], bz = p.box_n[2];
-    const int tot = bx * by * bz;
-    const bool staged = tot <= smem_nodes;
     const float* rho_g = fields;
     const float* ux_g = fields + N;
     const float* uy_g = fields + 2 * N;
     const float* uz_g = fields + 3 * N;
-    float* faux = fields + 4 * N;
-    auto gidx = [&](int ix, int iy, int iz) -> size_t {
-        const int x = wrapi(p.box_lo[0] + ix, P.nx), y = wrapi(p.box_lo[1] + iy, P.ny), z = wrapi(p.box_lo[2] + iz, P.nz);
-        return ((size_t)z * P.ny + y) * P.nx + x;
-    };
-    if (staged) {  // stage rho,u of the box (x fastest: coalesced rows)
-        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
-            const int ix = k % bx, iy = (k / bx) % by, iz = k / (bx * by);
-            const size_t g = gidx(ix, iy, iz);
-            sm[k] = rho_g[g];
-            sm[tot + k] = ux_g[g];
-            sm[2 * tot + k] = uy_g[g];
-            sm[3 * tot + k] = uz_g[g];
-        }
-    }
-    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = IBM_THREADS / 32;
     const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
     double accF[3] = {0, 0, 0}, accM[3] = {0, 0, 0};
     const int nb = p.node_count;
-    // interpolation and direct forcing (ibm.cu:307-475)
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    for (int k = sub * warps + warp; k < nb; k += split * warps) {
         const int j = p.node_begin + k;
-        const NodeStencil st = node_stencil(P, p, X[j], Y[j], Z[j]);
-        if (st.skip) { ndx[j] = ndy[j] = ndz[j] = 0.0; continue; }
+        const double xj = X[j], yj = Y[j], zj = Z[j];
+        const NodeStencil st = node_stencil(P, p, xj, yj, zj);
+        if (st.skip) {
+            if (lane == 0) ndx[j] = ndy[j] = ndz[j] = 0.0;
+            continue;
+        }
+        size_t g[2];
+        float d[2];
+        bool in[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int q = lane + 32 * h;
+            const int xi = q & 3, yi = (q >> 2) & 3, zi = q >> 4;
+            in[h] = xi >= st.lo[0] && xi <= st.hi[0] && yi >= st.lo[1] && yi <= st.hi[1] && zi >= st.lo[2] &&
+                    zi <= st.hi[2];
+            d[h] = (st.w[2][zi] * st.w[1][yi]) * st.w[0][xi];
+            const int x = wrap_near(st.base[0] + xi, P.nx), y = wrap_near(st.base[1] + yi, P.ny),
+                      z = wrap_near(st.base[2] + zi, P.nz);
+            g[h] = ((size_t)z * P.ny + y) * P.nx + x;
+        }
         float rho = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
-        for (int zk = st.lo[2]; zk <= st.hi[2]; ++zk)
-            for (int yj = st.lo[1]; yj <= st.hi[1]; ++yj) {
-                const float wzy = st.w[2][zk] * st.w[1][yj];
-                for (int xi = st.lo[0]; xi <= st.hi[0]; ++xi) {
-                    const float d = wzy * st.w[0][xi];
-                    // inside [0, box) by construction; the wrap matters only when a
-                    // periodic axis is shorter than the box and the box spans it
-                    const int ix = wrapi(st.base[0] + xi - p.box_lo[0], bx),
-                              iy = wrapi(st.base[1] + yj - p.box_lo[1], by),
-                              iz = wrapi(st.base[2] + zk - p.box_lo[2], bz);
-                    if (staged) {
-                        const int b = (iz * by + iy) * bx + ix;
-                        rho += sm[b] * d; ux += sm[tot + b] * d; uy += sm[2 * tot + b] * d; uz += sm[3 * tot + b] * d;
-                    } else {
-                        const size_t g = gidx(ix, iy, iz);
-                        rho += rho_g[g] * d; ux += ux_g[g] * d; uy += uy_g[g] * d; uz += uz_g[g] * d;
-                    }
-                }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (in[h]) {
+                rho += rho_g[g[h]] * d[h]; ux += ux_g[g[h]] * d[h];
+                uy += uy_g[g[h]] * d[h]; uz += uz_g[g[h]] * d[h];
             }
-        double dr[3] = {X[j] - p.pos[0], Y[j] - p.pos[1], Z[j] - p.pos[2]};
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            rho += __shfl_xor_sync(0xffffffffu, rho, o);
+            ux += __shfl_xor_sync(0xffffffffu, ux, o);
+            uy += __shfl_xor_sync(0xffffffffu, uy, o);
+            uz += __shfl_xor_sync(0xffffffffu, uz, o);
+        }
+        double dr[3] = {xj - p.pos[0], yj - p.pos[1], zj - p.pos[2]};
         for (int a = 0; a < 3; ++a)
             if (!P.wall[a]) dr[a] = pdelta(dr[a], L[a]);
         double uc[3] = {0, 0, 0};
@@ -551,89 +591,64 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_interp_spread(IbmParams P, 
         }
         const double aux = 2.0 * (double)rho * S[j] * P.thickness;
         const double dF[3] = {aux * ((double)ux - uc[0]), aux * ((double)uy - uc[1]), aux * ((double)uz - uc[2])};
-        nfx[j] += dF[0]; nfy[j] += dF[1]; nfz[j] += dF[2];
-        ndx[j] = dF[0]; ndy[j] = dF[1]; ndz[j] = dF[2];
-        double m[3];
-        dcross(dr, dF, m);
-        for (int a = 0; a < 3; ++a) { accF[a] += dF[a]; accM[a] += m[a]; }
-    }
-    __syncthreads();
-    if (staged)
-        for (int k = threadIdx.x; k < 3 * tot; k += blockDim.x) sm[k] = 0.f;
-    __syncthreads();
-    // spreading: fAux -= dF * delta (ibm.cu:478-512)
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-        const int j = p.node_begin + k;
-        const NodeStencil st = node_stencil(P, p, X[j], Y[j], Z[j]);
-        if (st.skip) continue;
-        const float dF[3] = {(float)ndx[j], (float)ndy[j], (float)ndz[j]};
-        for (int zk = st.lo[2]; zk <= st.hi[2]; ++zk)
-            for (int yj = st.lo[1]; yj <= st.hi[1]; ++yj) {
-                const float wzy = st.w[2][zk] * st.w[1][yj];
-                for (int xi = st.lo[0]; xi <= st.hi[0]; ++xi) {
-                    const float d = wzy * st.w[0][xi];
-                    // inside [0, box) by construction; the wrap matters only when a
-                    // periodic axis is shorter than the box and the box spans it
-                    const int ix = wrapi(st.base[0] + xi - p.box_lo[0], bx),
-                              iy = wrapi(st.base[1] + yj - p.box_lo[1], by),
-                              iz = wrapi(st.base[2] + zk - p.box_lo[2], bz);
-                    if (staged) {
-                        const int b = (iz * by + iy) * bx + ix;
-                        atomicAdd(&sm[b], -dF[0] * d);
-                        atomicAdd(&sm[tot + b], -dF[1] * d);
-                        atomicAdd(&sm[2 * tot + b], -dF[2] * d);
-                    } else {
-                        const size_t g = gidx(ix, iy, iz);
-                        atomicAdd(&faux[g], -dF[0] * d);
-                        atomicAdd(&faux[N + g], -dF[1] * d);
-                        atomicAdd(&faux[2 * N + g], -dF[2] * d);
-                    }
-                }
+        if (lane == 0) {
+            nfx[j] += dF[0]; nfy[j] += dF[1]; nfz[j] += dF[2];
+            ndx[j] = dF[0]; ndy[j] = dF[1]; ndz[j] = dF[2];
+            double m[3];
+            dcross(dr, dF, m);
+            for (int a = 0; a < 3; ++a) { accF[a] += dF[a]; accM[a] += m[a]; }
+        }
+        // spreading: fAux -= dF * delta (ibm.cu:478-512), in fixed point so the
+        // sum is the same in any order
+        const float f0 = (float)dF[0], f1 = (float)dF[1], f2 = (float)dF[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (in[h]) {
+                atomicAdd(&faux[g[h]], to_fix(-f0 * d[h]));
+                atomicAdd(&faux[N + g[h]], to_fix(-f1 * d[h]));
+                atomicAdd(&faux[2 * N + g[h]], to_fix(-f2 * d[h]));
             }
     }
-    __syncthreads();
-    if (staged) {  // one flush of the box into the global auxiliary field
-        for (int k = threadIdx.x; k < tot; k += blockDim.x) {
-            const float a0 = sm[k], a1 = sm[tot + k], a2 = sm[2 * tot + k];
-            if (a0 == 0.f && a1 == 0.f && a2 == 0.f) continue;
-            const int ix = k % bx, iy = (k / bx) % by, iz = k / (bx * by);
-            const size_t g = gidx(ix, iy, iz);
-            atomicAdd(&faux[g], a0);
-            atomicAdd(&faux[N + g], a1);
-            atomicAdd(&faux[2 * N + g], a2);
-        }
-    }
-    // sphere force and torque: block sums, one writer per sphere (ibm.cu:526-541)
+    // this CTA's part of the sphere force and torque (ibm.cu:526-541)
     double tot6[6];
     for (int a = 0; a < 3; ++a) { tot6[a] = block_sum(accF[a], red); tot6[3 + a] = block_sum(accM[a], red); }
     if (threadIdx.x == 0)
-        for (int a = 0; a < 3; ++a) { p.f[a] += tot6[a]; p.M[a] += tot6[3 + a]; }
+        for (int a = 0; a < 6; ++a) fpart[((size_t)sphere * split + sub) * 6 + a] = tot6[a];
 }
 
-__global__ void k_ibm_update(IbmParams P, DPart* parts) {
-    for (int i = threadIdx.x; i < P.np; i += blockDim.x) update_center(P, parts[i]);
+__global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int split) {
+    for (int i = threadIdx.x; i < P.np; i += blockDim.x) {
+        DPart& p = parts[i];
+        double t[6] = {0, 0, 0, 0, 0, 0};
+        for (int b = 0; b < split; ++b)
+            for (int a = 0; a < 6; ++a) t[a] += fpart[((size_t)i * split + b) * 6 + a];
+        for (int a = 0; a < 3; ++a) { p.f[a] += t[a]; p.M[a] += t[3 + a]; }
+        update_center(P, p);
+    }
 }
 
 // gpuEulerSumIBMAuxsReset restricted to the touched nodes
-__global__ void k_ibm_euler(IbmParams P, float* fields, float* fibm, uint8_t* cls, const int* list, const int* count) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= *count) return;
+__global__ void k_ibm_euler(IbmParams P, float* fields, unsigned long long* faux, float* fibm, uint8_t* cls,
+                            const int* list, const int* count) {
+    const int cnt = *count;
     const size_t N = (size_t)P.nx * P.ny * P.nz;
-    const int n = list[k];
-    float* faux = fields + 4 * N;
-    const float rho = fields[n];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const int n = list[k];
+        const float rho = fields[n];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float v = faux[a * N + n];
-        fields[(1 + a) * N + n] += 0.5f * v / rho;
-        fibm[a * N + n] += v;
-        faux[a * N + n] = 0.f;
+        for (int a = 0; a < 3; ++a) {
+            const float v = from_fix(faux[a * N + n]);
+            fields[(1 + a) * N + n] += 0.5f * v / rho;
+            fibm[a * N + n] += v;
+            faux[a * N + n] = 0ull;
+        }
+        cls[n] = cls[n] | NODE_IBM_FORCE;
     }
-    cls[n] = cls[n] | NODE_IBM_FORCE;
 }
 
 // gpuParticleMovement ibm.cu:899-993
-__global__ void k_ibm_move(IbmParams P, DPart* parts) {
+__global__ void k_ibm_move(IbmParams P, DPart* parts, int* steps_taken) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *steps_taken += 1;   // read by the next step's contacts
     const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
     for (int i = threadIdx.x; i < P.np; i += blockDim.x) {
         DPart& p = parts[i];
@@ -744,11 +759,11 @@ static cudaError_t launch_gather(vlbm_sim* s, IbmState* st) {
     const StepParams sp = make_params(s);
     const bool pr = sp.pairH > 0;
     if (s->parity == 1) {
-        if (pr) k_ibm_gather<Q, ST, true, true><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
-        else k_ibm_gather<Q, ST, true, false><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+        if (pr) k_ibm_gather<Q, ST, true, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
+        else k_ibm_gather<Q, ST, true, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
     } else {
-        if (pr) k_ibm_gather<Q, ST, false, true><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
-        else k_ibm_gather<Q, ST, false, false><<<st->np, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count);
+        if (pr) k_ibm_gather<Q, ST, false, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
+        else k_ibm_gather<Q, ST, false, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
     }
     return cudaGetLastError();
 }
@@ -768,7 +783,6 @@ static cudaError_t gather_dispatch(vlbm_sim* s, IbmState* st) {
 vlbm_status ibm_step(vlbm_sim* s) {
     IbmState* st = s->ibm;
     if (!st || st->np == 0) return VLBM_OK;
-    st->prm.step = (int)(s->step - 1);  // index of the fluid step just taken (main.cu:270)
     const IbmParams& P = st->prm;
     cudaStream_t cs = s->stream;
     IBM_CUDA(cudaMemsetAsync(st->count, 0, sizeof(int), cs));
@@ -776,22 +790,23 @@ vlbm_status ibm_step(vlbm_sim* s) {
                                               st->ndy, st->ndz);
     IBM_CUDA(cudaGetLastError());
     IBM_CUDA(gather_dispatch(s, st));
-    k_ibm_contacts<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->contrib);
+    k_ibm_contacts<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->contrib, st->count + 1);
     IBM_CUDA(cudaGetLastError());
-    const size_t smem = (size_t)st->smem_nodes * 4 * sizeof(float);
-    const int euler_blocks = (int)((s->N + 255) / 256);
+    // grid-stride over the touched-node list: enough blocks for the boxes of
+    // all spheres, at most one per 256 lattice nodes
+    const int euler_blocks = (int)std::min<long long>((s->N + 255) / 256, std::max<long long>(1, st->euler_blocks));
     for (int it = 0; it < st->cfg.max_iterations; ++it) {
-        k_ibm_interp_spread<<<st->np, IBM_THREADS, smem, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nS, st->nfx,
-                                                               st->nfy, st->nfz, st->ndx, st->ndy, st->ndz, st->fields,
-                                                               st->smem_nodes);
+        k_ibm_interp_spread<<<st->np * st->split, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nS,
+                                                                         st->nfx, st->nfy, st->nfz, st->ndx, st->ndy,
+                                                                         st->ndz, st->fields, st->faux, st->fpart,
+                                                                         st->split);
         IBM_CUDA(cudaGetLastError());
-        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts);
+        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->fpart, st->split);
         IBM_CUDA(cudaGetLastError());
-        // the list never exceeds N; launch over N's block count, threads past *count exit
-        k_ibm_euler<<<euler_blocks, 256, 0, cs>>>(P, st->fields, s->fibm, s->cls, st->list, st->count);
+        k_ibm_euler<<<euler_blocks, 256, 0, cs>>>(P, st->fields, st->faux, s->fibm, s->cls, st->list, st->count);
         IBM_CUDA(cudaGetLastError());
     }
-    k_ibm_move<<<1, IBM_THREADS, 0, cs>>>(P, st->parts);
+    k_ibm_move<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->count + 1);
     k_ibm_move_nodes<<<(st->nnodes + 255) / 256, 256, 0, cs>>>(P, st->parts, st->npid, st->nx, st->ny, st->nz);
     IBM_CUDA(cudaGetLastError());
     return VLBM_OK;
@@ -809,12 +824,14 @@ vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy
     return cuda_status(cudaGetLastError(), "ibm macroscopics fixup");
 }
 
-void ibm_destroy(IbmState* st) {
+void ibm_destroy(IbmState* st, DeviceAllocator* a) {
     if (!st) return;
-    cudaFree(st->parts);
-    for (double* p : {st->nx, st->ny, st->nz, st->nS, st->nfx, st->nfy, st->nfz, st->ndx, st->ndy, st->ndz, st->contrib})
-        cudaFree(p);
-    cudaFree(st->npid); cudaFree(st->fields); cudaFree(st->list); cudaFree(st->count);
+    free_with(a, st->parts);
+    for (double* p : {st->nx, st->ny, st->nz, st->nS, st->nfx, st->nfy, st->nfz, st->ndx, st->ndy, st->ndz, st->contrib,
+                      st->fpart})
+        free_with(a, p);
+    free_with(a, st->npid); free_with(a, st->fields); free_with(a, st->faux); free_with(a, st->list);
+    free_with(a, st->count);
     delete st;
 }
 
@@ -826,8 +843,9 @@ void ibm_reset(vlbm_sim* s) {
     cudaMemcpyAsync(st->nx, st->init_nodes.data(), nn * sizeof(double), cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(st->ny, st->init_nodes.data() + nn, nn * sizeof(double), cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(st->nz, st->init_nodes.data() + 2 * nn, nn * sizeof(double), cudaMemcpyHostToDevice, s->stream);
-    cudaMemsetAsync(st->fields, 0, (size_t)7 * s->N * sizeof(float), s->stream);
-    cudaMemsetAsync(st->count, 0, sizeof(int), s->stream);
+    cudaMemsetAsync(st->fields, 0, (size_t)4 * s->N * sizeof(float), s->stream);
+    cudaMemsetAsync(st->faux, 0, (size_t)3 * s->N * sizeof(unsigned long long), s->stream);
+    cudaMemsetAsync(st->count, 0, 2 * sizeof(int), s->stream);   // no touched nodes, step clock 0
 }
 
 }  // namespace vlbm
@@ -927,7 +945,7 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
     P.nnodes = st->nnodes;
     const size_t nn = X.size(), N = (size_t)s->N;
     auto dalloc = [&](void** p, size_t b) -> cudaError_t {
-        cudaError_t e = cudaMalloc(p, b);
+        cudaError_t e = sim_malloc(s, p, b);
         if (e == cudaSuccess) st->bytes += b;
         return e;
     };
@@ -936,39 +954,50 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
     for (double** d : dp)
         if (e == cudaSuccess) e = dalloc((void**)d, nn * sizeof(double));
     if (e == cudaSuccess) e = dalloc((void**)&st->npid, nn * sizeof(int));
-    if (e == cudaSuccess) e = dalloc((void**)&st->fields, 7 * N * sizeof(float));
+    if (e == cudaSuccess) e = dalloc((void**)&st->fields, 4 * N * sizeof(float));
+    if (e == cudaSuccess) e = dalloc((void**)&st->faux, 3 * N * sizeof(unsigned long long));
     if (e == cudaSuccess) e = dalloc((void**)&st->list, N * sizeof(int));
-    if (e == cudaSuccess) e = dalloc((void**)&st->count, sizeof(int));
+    if (e == cudaSuccess) e = dalloc((void**)&st->count, 2 * sizeof(int));
     if (e == cudaSuccess) e = dalloc((void**)&st->contrib, (size_t)n * n * 6 * sizeof(double));
+    {   // CTAs per sphere of the interpolation/spreading kernel: about
+        // IBM_NODES_PER_CTA Lagrangian nodes each for the largest sphere
+        std::vector<int> cnt(n, 0);
+        for (int pk : pid) cnt[pk] += 1;
+        int most = 1;
+        for (int c : cnt) most = std::max(most, c);
+        st->split = std::min(IBM_MAX_SPLIT, std::max(1, (most + IBM_NODES_PER_CTA - 1) / IBM_NODES_PER_CTA));
+    }
+    if (e == cudaSuccess) e = dalloc((void**)&st->fpart, (size_t)n * st->split * 6 * sizeof(double));
+    {   // CTAs per sphere of the gather: about two box nodes per thread for the largest sphere
+        long long maxbox = 1;
+        for (int k = 0; k < n; ++k) {
+            const long long side = (long long)std::ceil(sp[k].diameter) + 6;
+            maxbox = std::max(maxbox, std::min<long long>(side, c.nx) * std::min<long long>(side, c.ny) *
+                                          std::min<long long>(side, c.nz));
+        }
+        st->gsplit = (int)std::min<long long>(IBM_MAX_SPLIT, std::max<long long>(1, maxbox / (2 * IBM_THREADS)));
+        st->euler_blocks = ((long long)n * maxbox + 255) / 256;
+    }
     if (e == cudaSuccess && !s->fibm) {
-        e = cudaMalloc((void**)&s->fibm, 3 * N * sizeof(float));
+        e = sim_malloc(s, (void**)&s->fibm, 3 * N * sizeof(float));
         if (e == cudaSuccess) s->device_bytes += 3 * N * sizeof(float);
     }
-    if (e != cudaSuccess) { ibm_destroy(st); return cuda_status(e, "IBM allocation"); }
+    if (e != cudaSuccess) { ibm_destroy(st, s->allocator); return cuda_status(e, "IBM allocation"); }
     e = cudaMemcpy(st->parts, parts.data(), parts.size() * sizeof(DPart), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(st->nx, X.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(st->ny, Y.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(st->nz, Z.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(st->nS, S.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(st->npid, pid.data(), nn * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(st->fields, 0, 7 * N * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(st->fields, 0, 4 * N * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(st->faux, 0, 3 * N * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(st->count, 0, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(s->fibm, 0, 3 * N * sizeof(float));
-    // staged box capacity: largest sphere box, capped by the shared memory limit
-    int maxbox = 0;
-    for (int k = 0; k < n; ++k) {
-        const int side = (int)std::ceil(sp[k].diameter) + 5;
-        const int bx = std::min(side, c.nx), by = std::min(side, c.ny), bz = std::min(side, c.nz);
-        maxbox = std::max(maxbox, bx * by * bz);
+    if (e == cudaSuccess) {   // the contact history clock starts at the lattice's step count
+        const int clock = (int)s->step;
+        e = cudaMemcpy(st->count + 1, &clock, sizeof(int), cudaMemcpyHostToDevice);
     }
-    st->smem_nodes = std::min(maxbox, IBM_SMEM_MAX_NODES);
-    // the attribute is one value per kernel and device, shared by every
-    // simulation in the process: always allow the largest box, so a later
-    // simulation with smaller spheres cannot lower the limit under an earlier one
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_ibm_interp_spread, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 IBM_SMEM_MAX_NODES * 4 * (int)sizeof(float));
-    if (e != cudaSuccess) { ibm_destroy(st); return cuda_status(e, "IBM setup"); }
+    if (e == cudaSuccess) e = cudaMemset(s->fibm, 0, 3 * N * sizeof(float));
+    if (e != cudaSuccess) { ibm_destroy(st, s->allocator); return cuda_status(e, "IBM setup"); }
     st->initial = parts;
     st->init_nodes.resize(3 * nn);
     std::memcpy(st->init_nodes.data(), X.data(), nn * sizeof(double));

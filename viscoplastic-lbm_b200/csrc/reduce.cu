@@ -128,8 +128,8 @@ extern "C" vlbm_status vlbm_moments_sum(vlbm_sim* s, double* out4) {
     if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
     const size_t need = (size_t)4 * reduce_blocks(s->N) + 4;
     if (!s->red_scratch) {
-        e = cudaMalloc(&s->red_scratch, need * sizeof(double));
-        if (e != cudaSuccess) { s->red_scratch = nullptr; return cuda_status(e, "cudaMalloc reduction scratch"); }
+        e = sim_malloc(s, (void**)&s->red_scratch, need * sizeof(double));
+        if (e != cudaSuccess) { s->red_scratch = nullptr; return cuda_status(e, "reduction scratch allocation"); }
         s->device_bytes += need * sizeof(double);
     }
     double* partials = s->red_scratch;

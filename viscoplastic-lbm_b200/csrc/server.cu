@@ -6,22 +6,32 @@
 // while the HBM budget and the slot limit allow, kept resident, advanced
 // together, and retired at their step count:
 //
-//  * every resident lattice of one (velocity set, operator, rheology, storage)
-//    group advances in ONE persistent launch of k_step_batched over a
-//    (lattice, tile) table; the step state of each lattice (AA parity,
-//    side-store buffer, boundary flag) lives in device memory and is advanced by
-//    k_batch_advance, so a step is captured once in a CUDA graph and replayed
-//    until the membership changes.  Lattices with spheres run their IBM kernels
-//    after the batched fluid step, launched directly;
-//  * pump() runs up to the next retirement without host synchronisation, then
-//    synchronises, records completion times and the volume-mean velocity,
-//    frees the lattice and admits queued requests into the freed memory.
+//  * the small sphere-free lattices of one (velocity set, operator, rheology,
+//    storage) group that share an AA parity advance in ONE persistent launch
+//    of k_step_batched over a (lattice, tile) table; the side-store buffer and
+//    boundary flag of each lattice live in device memory and are advanced by
+//    k_batch_advance.  A sphere-free lattice that fills a wave of that kernel
+//    by itself gets its own k_step launch.  Each lattice with spheres runs its
+//    fluid and IBM launches on its own side stream (a graph branch that
+//    overlaps the others).  One step and eight steps are captured in CUDA
+//    graphs per phase (steps since the tables were built, mod 2) and replayed
+//    until the membership changes;
+//  * pump() enqueues the steps in segments of at most kSegment steps and does
+//    its host work (admission of queued requests, table rebuilds, graph
+//    captures) while the GPU runs the previous segment.  A lattice that reaches
+//    its step count is read out on the GPU (macroscopic ux and the divergence
+//    word into pinned host memory, behind an event) and leaves the batch; when
+//    the event has completed its completion is recorded and its device memory
+//    goes back to the server's cache, which hands it to the next admitted
+//    lattice without cudaFree (cudaFree would synchronise the device).
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <string>
+#include <unordered_map>
 #include <vector>
 #include "sim.h"
 #include "step_impl.cuh"
@@ -49,7 +59,9 @@ using namespace vlbm;
 
 namespace {
 
-constexpr int kGraphSteps = 8;        // steps per replay of the long graph
+constexpr int kGraphSteps = 8;        // steps per replay of the long graph (even: keeps the phase)
+constexpr int kSegment = 64;          // steps enqueued between two host bookkeeping points
+constexpr int kSegmentsInFlight = 8;  // the host waits when more segments are queued
 constexpr size_t kKeptResults = 256;  // finished fields kept for vlbm_server_fetch
 
 double now_s() {
@@ -84,15 +96,102 @@ size_t estimate_bytes(const vlbm_request& r) {
     const size_t walls = 2 * ((size_t)r.cfg.nx * r.cfg.ny + (size_t)r.cfg.ny * r.cfg.nz + (size_t)r.cfg.nx * r.cfg.nz);
     b += walls * (2 * (size_t)r.cfg.vel_set * 4 + 24);
     if (r.cfg.rheology == VLBM_POWERLAW) b += 4 * N;
-    if (r.n_spheres > 0) b += 44 * N + (size_t)r.n_spheres * 700 * 10 * 8;
+    if (r.n_spheres > 0) b += 56 * N + (size_t)r.n_spheres * 700 * 10 * 8;
     return b;
 }
 
+// The lattices of one kernel family, split by their AA parity when the tables
+// were built: part b holds the lattices whose parity was b, which at phase ph
+// (steps since the rebuild, mod 2) step with parity b ^ ph.
 struct Group {
     int Q, op, rheo, st;
-    size_t table_off;
-    int ntiles;
-    int grid;
+    size_t off[2];
+    int ntiles[2];
+    int grid[2];
+};
+
+// Device memory cache of the server.  Buffers released by retired lattices are
+// kept and handed out again (best fit, at most 25 % + 2 MiB larger than asked);
+// only trim() calls cudaFree.  A buffer is released only after the GPU has
+// finished with its lattice (its read-out event completed).
+struct DevCache final : DeviceAllocator {
+    std::multimap<size_t, void*> free_;
+    std::unordered_map<void*, size_t> size_of;
+    size_t free_bytes = 0, live_bytes = 0;
+
+    cudaError_t allocate(void** p, size_t bytes) override {
+        const size_t need = (bytes + 511) & ~(size_t)511;
+        auto it = free_.lower_bound(need);
+        if (it != free_.end() && it->first <= need + need / 4 + ((size_t)2 << 20)) {
+            *p = it->second;
+            free_bytes -= it->first;
+            live_bytes += it->first;
+            free_.erase(it);
+            return cudaSuccess;
+        }
+        cudaError_t e = cudaMalloc(p, need);
+        if (e == cudaErrorMemoryAllocation && !free_.empty()) {   // give the cached buffers back and retry
+            cudaGetLastError();
+            trim(0);
+            e = cudaMalloc(p, need);
+        }
+        if (e != cudaSuccess) { *p = nullptr; return e; }
+        size_of[*p] = need;
+        live_bytes += need;
+        return cudaSuccess;
+    }
+    void release(void* p) override {
+        auto it = size_of.find(p);
+        if (it == size_of.end()) return;
+        free_.insert({it->second, p});
+        free_bytes += it->second;
+        live_bytes -= it->second;
+    }
+    void trim(size_t keep) {
+        while (free_bytes > keep && !free_.empty()) {
+            auto it = std::prev(free_.end());
+            cudaFree(it->second);
+            size_of.erase(it->second);
+            free_bytes -= it->first;
+            free_.erase(it);
+        }
+    }
+    ~DevCache() override {
+        trim(0);
+        for (auto& kv : size_of) cudaFree(kv.first);   // nothing should be live here
+    }
+};
+
+// Pinned host buffers for read-outs, reused best fit; freed with the server.
+struct PinnedPool {
+    std::multimap<size_t, void*> free_;
+    std::vector<void*> all;
+    void* get(size_t bytes) {
+        auto it = free_.lower_bound(bytes);
+        if (it != free_.end() && it->first <= 2 * bytes + 4096) {
+            void* p = it->second;
+            free_.erase(it);
+            return p;
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+        all.push_back(p);
+        sizes[p] = bytes;
+        return p;
+    }
+    void put(void* p) { if (p) free_.insert({sizes[p], p}); }
+    std::unordered_map<void*, size_t> sizes;
+    ~PinnedPool() { for (void* p : all) cudaFreeHost(p); }
+};
+
+// A lattice that reached its step count and is being read out.
+struct Retiring {
+    Resident r;
+    float* d_ux = nullptr;        // device read-out of ux
+    float* h_ux = nullptr;        // pinned copy
+    unsigned* h_err = nullptr;    // pinned copy of the divergence word
+    cudaEvent_t done = nullptr;
+    vlbm_status status = VLBM_OK;
 };
 
 }  // namespace
@@ -103,32 +202,64 @@ struct vlbm_server {
     size_t budget = 0;
     int max_resident = 64;
     cudaStream_t stream = nullptr;
+    DevCache cache;
+    PinnedPool pinned;
     std::deque<Pending> queue;
     std::vector<Resident> res;
+    std::vector<Retiring> retiring;
+    std::deque<cudaEvent_t> segments;   // one event per queued segment
     std::deque<vlbm_completion> done;
     std::deque<std::pair<uint64_t, std::vector<float>>> results;   // finished ux fields, by tag
     size_t bytes_in_use = 0;
     double lattice_updates = 0.0;
+    double prof[5] = {0, 0, 0, 0, 0};   // admit, rebuild+capture, enqueue, wait, read-out
     // batch tables (rebuilt when the membership changes)
     bool dirty = true;
     BatchSlot* d_slots = nullptr;
     BatchBlock* d_table = nullptr;
     size_t cap_slots = 0, cap_table = 0;
+    std::vector<void*> old_tables;      // outgrown table buffers, freed with the server
+    BatchSlot* h_slots = nullptr;       // pinned staging of the tables
+    BatchBlock* h_table = nullptr;
+    cudaEvent_t upload_done = nullptr;  // staging may be rewritten once this completed
     std::vector<Group> groups;
     int nslots = 0;
-    bool any_ibm = false;
-    cudaGraphExec_t graph1 = nullptr, graphK = nullptr;   // one step, kGraphSteps steps
+    int phase = 0;                 // steps since the last rebuild, mod 2
+    std::vector<int> ibm_res;      // indices into res of lattices with spheres (side streams)
+    std::vector<int> own_res;      // indices into res of large sphere-free lattices (own launches)
+    // per phase: graphs of one step and of kGraphSteps steps
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr}, graphK[2] = {nullptr, nullptr};
+    // side streams of the lattices with spheres (graph branches)
+    std::vector<cudaStream_t> side_streams;
+    std::vector<cudaEvent_t> join_events;
+    cudaEvent_t fork_event = nullptr;
 
     void drop_graphs() {
-        if (graph1) cudaGraphExecDestroy(graph1);
-        if (graphK) cudaGraphExecDestroy(graphK);
-        graph1 = graphK = nullptr;
+        for (int p = 0; p < 2; ++p) {
+            if (graph1[p]) cudaGraphExecDestroy(graph1[p]);
+            if (graphK[p]) cudaGraphExecDestroy(graphK[p]);
+            graph1[p] = graphK[p] = nullptr;
+        }
     }
     ~vlbm_server() {
-        for (Resident& r : res) vlbm_destroy(r.sim);
+        if (stream) cudaStreamSynchronize(stream);
+        for (Resident& r : res) vlbm::sim_release(r.sim);
+        for (Retiring& t : retiring) {
+            vlbm::free_with(&cache, t.d_ux);
+            vlbm::sim_release(t.r.sim);
+            if (t.done) cudaEventDestroy(t.done);
+        }
+        for (cudaEvent_t e : segments) cudaEventDestroy(e);
         drop_graphs();
         cudaFree(d_slots);
         cudaFree(d_table);
+        for (void* p : old_tables) cudaFree(p);
+        if (h_slots) cudaFreeHost(h_slots);
+        if (h_table) cudaFreeHost(h_table);
+        if (upload_done) cudaEventDestroy(upload_done);
+        for (cudaStream_t t : side_streams) cudaStreamDestroy(t);
+        for (cudaEvent_t e : join_events) cudaEventDestroy(e);
+        if (fork_event) cudaEventDestroy(fork_event);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -138,7 +269,8 @@ namespace {
 vlbm_status server_rebuild(vlbm_server* sv) {
     sv->drop_graphs();
     sv->groups.clear();
-    sv->any_ibm = false;
+    sv->ibm_res.clear();
+    sv->phase = 0;
     std::vector<BatchSlot> slots;
     std::vector<BatchBlock> table;
     auto key = [](const vlbm_sim* s) {
@@ -147,17 +279,31 @@ vlbm_status server_rebuild(vlbm_server* sv) {
     };
     std::vector<int> order(sv->res.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return key(sv->res[a].sim) < key(sv->res[b].sim); });
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const vlbm_sim *sa = sv->res[a].sim, *sb = sv->res[b].sim;
+        return key(sa) != key(sb) ? key(sa) < key(sb) : sa->parity < sb->parity;
+    });
     int cur = -1;
+    sv->own_res.clear();
     for (int idx : order) {
         vlbm_sim* s = sv->res[idx].sim;
-        if (s->ibm) sv->any_ibm = true;
+        // Lattices with spheres step on their own side stream (fluid and IBM
+        // launches); sphere-free lattices that fill a wave of the batched
+        // kernel by themselves get their own k_step launch (parameters in the
+        // constant bank, one node per thread); the rest share the table.
+        if (s->ibm) { sv->ibm_res.push_back(idx); continue; }
+        const long long wave = (long long)std::max(1, batched_blocks_per_sm(s->Q, s->cfg.storage, s->cfg.collision,
+                                                                            s->cfg.rheology)) * sv->sms * BATCH_TILE;
+        if (s->N >= wave) { sv->own_res.push_back(idx); continue; }
         const int k = key(s);
         if (k != cur) {
-            sv->groups.push_back(Group{s->Q, s->cfg.collision, s->cfg.rheology, s->cfg.storage, table.size(), 0, 0});
+            Group g{s->Q, s->cfg.collision, s->cfg.rheology, s->cfg.storage, {table.size(), table.size()}, {0, 0}, {0, 0}};
+            sv->groups.push_back(g);
             cur = k;
         }
+        Group& g = sv->groups.back();
+        const int part = s->parity;
+        if (part == 1 && g.ntiles[1] == 0) g.off[1] = table.size();
         BatchSlot bs;
         std::memset(&bs, 0, sizeof(bs));
         bs.p = make_params(s);
@@ -170,68 +316,86 @@ vlbm_status server_rebuild(vlbm_server* sv) {
         slots.push_back(bs);
         const unsigned nt = (unsigned)((s->N + BATCH_TILE - 1) / BATCH_TILE);
         for (unsigned t = 0; t < nt; ++t) table.push_back(BatchBlock{slot, t * (unsigned)BATCH_TILE});
-        sv->groups.back().ntiles += (int)nt;
+        g.ntiles[part] += (int)nt;
     }
     for (Group& g : sv->groups) {
         const int per_sm = std::max(1, batched_blocks_per_sm(g.Q, g.st, g.op, g.rheo));
-        g.grid = std::min(g.ntiles, per_sm * sv->sms);
+        for (int b = 0; b < 2; ++b) g.grid[b] = std::min(g.ntiles[b], per_sm * sv->sms);
+    }
+    // one side stream and join event per lattice with spheres
+    while (sv->side_streams.size() < sv->ibm_res.size()) {
+        cudaStream_t t = nullptr;
+        cudaEvent_t ev = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            if (t) cudaStreamDestroy(t);
+            return cuda_status(e, "server side stream");
+        }
+        sv->side_streams.push_back(t);
+        sv->join_events.push_back(ev);
+    }
+    if (!sv->fork_event) {
+        cudaError_t e = cudaEventCreateWithFlags(&sv->fork_event, cudaEventDisableTiming);
+        if (e != cudaSuccess) { sv->fork_event = nullptr; return cuda_status(e, "server fork event"); }
     }
     sv->nslots = (int)slots.size();
+    // Grow the device tables and their pinned staging without cudaFree or
+    // cudaFreeHost (both synchronise the device): outgrown device buffers are
+    // kept until the server is destroyed, staging is replaced after the last
+    // upload from it completed.
+    if (sv->upload_done) {
+        cudaError_t e = cudaEventSynchronize(sv->upload_done);
+        if (e != cudaSuccess) return cuda_status(e, "server table upload");
+    }
     if (slots.size() > sv->cap_slots) {
-        cudaFree(sv->d_slots);
-        sv->d_slots = nullptr;
-        sv->cap_slots = 0;
-        if (cudaMalloc(&sv->d_slots, slots.size() * 2 * sizeof(BatchSlot)) != cudaSuccess) {
+        const size_t cap = std::max<size_t>(256, slots.size() * 2);
+        void* d = nullptr;
+        void* h = nullptr;
+        if (cudaMalloc(&d, cap * sizeof(BatchSlot)) != cudaSuccess ||
+            cudaHostAlloc(&h, cap * sizeof(BatchSlot), cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            if (d) cudaFree(d);
             set_last_error("server slot table allocation failed");
             return VLBM_ERR_NOMEM;
         }
-        sv->cap_slots = slots.size() * 2;
+        if (sv->d_slots) sv->old_tables.push_back(sv->d_slots);
+        if (sv->h_slots) cudaFreeHost(sv->h_slots);
+        sv->d_slots = static_cast<BatchSlot*>(d);
+        sv->h_slots = static_cast<BatchSlot*>(h);
+        sv->cap_slots = cap;
     }
     if (table.size() > sv->cap_table) {
-        cudaFree(sv->d_table);
-        sv->d_table = nullptr;
-        sv->cap_table = 0;
-        if (cudaMalloc(&sv->d_table, table.size() * 2 * sizeof(BatchBlock)) != cudaSuccess) {
+        const size_t cap = std::max<size_t>(1 << 16, table.size() * 2);
+        void* d = nullptr;
+        void* h = nullptr;
+        if (cudaMalloc(&d, cap * sizeof(BatchBlock)) != cudaSuccess ||
+            cudaHostAlloc(&h, cap * sizeof(BatchBlock), cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            if (d) cudaFree(d);
             set_last_error("server tile table allocation failed");
             return VLBM_ERR_NOMEM;
         }
-        sv->cap_table = table.size() * 2;
+        if (sv->d_table) sv->old_tables.push_back(sv->d_table);
+        if (sv->h_table) cudaFreeHost(sv->h_table);
+        sv->d_table = static_cast<BatchBlock*>(d);
+        sv->h_table = static_cast<BatchBlock*>(h);
+        sv->cap_table = cap;
     }
     if (!slots.empty()) {
-        // pageable sources: both copies are complete when the calls return
-        cudaError_t e = cudaMemcpyAsync(sv->d_slots, slots.data(), slots.size() * sizeof(BatchSlot),
+        std::memcpy(sv->h_slots, slots.data(), slots.size() * sizeof(BatchSlot));
+        std::memcpy(sv->h_table, table.data(), table.size() * sizeof(BatchBlock));
+        cudaError_t e = cudaMemcpyAsync(sv->d_slots, sv->h_slots, slots.size() * sizeof(BatchSlot),
                                         cudaMemcpyHostToDevice, sv->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(sv->d_table, table.data(), table.size() * sizeof(BatchBlock), cudaMemcpyHostToDevice,
+            e = cudaMemcpyAsync(sv->d_table, sv->h_table, table.size() * sizeof(BatchBlock), cudaMemcpyHostToDevice,
                                 sv->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(sv->stream);
+        if (e == cudaSuccess && !sv->upload_done) e = cudaEventCreateWithFlags(&sv->upload_done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(sv->upload_done, sv->stream);
         if (e != cudaSuccess) return cuda_status(e, "server table upload");
     }
     sv->dirty = false;
     return VLBM_OK;
-}
-
-// The launches of one batched fluid step (all groups, then the state advance).
-cudaError_t server_fluid_launches(vlbm_server* sv) {
-    for (const Group& g : sv->groups) {
-        cudaError_t e = launch_batched(g.Q, g.st, sv->d_slots, sv->d_table + g.table_off, g.ntiles, g.grid, g.op,
-                                       g.rheo, sv->stream);
-        if (e != cudaSuccess) return e;
-    }
-    return launch_batch_advance(sv->d_slots, sv->nslots, sv->stream);
-}
-
-cudaError_t capture(vlbm_server* sv, int steps, cudaGraphExec_t* out) {
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(sv->stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return e;
-    cudaError_t le = cudaSuccess;
-    for (int i = 0; i < steps && le == cudaSuccess; ++i) le = server_fluid_launches(sv);
-    e = cudaStreamEndCapture(sv->stream, &g);
-    if (e == cudaSuccess) e = le;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
-    if (g) cudaGraphDestroy(g);
-    return e;
 }
 
 // Host mirror of the state every lattice advanced on the device.
@@ -242,32 +406,123 @@ void advance_host(vlbm_sim* s) {
     s->step += 1;
 }
 
-vlbm_status server_steps(vlbm_server* sv, uint64_t k) {
-    if (sv->res.empty() || k == 0) return VLBM_OK;
-    if (!sv->any_ibm) {
-        cudaError_t e = cudaSuccess;
-        if (k >= (uint64_t)kGraphSteps && !sv->graphK) e = capture(sv, kGraphSteps, &sv->graphK);
-        if (e == cudaSuccess && k % kGraphSteps && !sv->graph1) e = capture(sv, 1, &sv->graph1);
-        for (uint64_t i = 0; e == cudaSuccess && i < k / kGraphSteps; ++i) e = cudaGraphLaunch(sv->graphK, sv->stream);
-        for (uint64_t i = 0; e == cudaSuccess && i < k % kGraphSteps; ++i) e = cudaGraphLaunch(sv->graph1, sv->stream);
-        if (e != cudaSuccess) return cuda_status(e, "server step graph");
-        for (Resident& r : sv->res)
-            for (uint64_t i = 0; i < k; ++i) advance_host(r.sim);
-    } else {
-        for (uint64_t i = 0; i < k; ++i) {
-            cudaError_t e = server_fluid_launches(sv);
-            if (e != cudaSuccess) return cuda_status(e, "batched step");
-            for (Resident& r : sv->res) {
-                advance_host(r.sim);
-                if (r.sim->ibm) {
-                    vlbm_status st = ibm_step(r.sim);
-                    if (st != VLBM_OK) return st;
-                }
+// Enqueue `n` steps of every resident lattice (directly or into a stream
+// capture of the server stream).  Server stream, per step: the batched launches
+// of each group and parity part, the slot-state advance, then one k_step launch
+// per large lattice.  Each lattice with spheres runs its n steps (fluid launch
+// then IBM step) on its own side stream, forked from the server stream before
+// the first step and joined after the last, so sphere lattices overlap each
+// other and the batched work.  Advances the host mirrors and the phase.
+vlbm_status enqueue_steps(vlbm_server* sv, int n) {
+    cudaError_t e = cudaSuccess;
+    if (!sv->ibm_res.empty()) {
+        e = cudaEventRecord(sv->fork_event, sv->stream);
+        if (e != cudaSuccess) return cuda_status(e, "fork event");
+    }
+    for (int i = 0; i < n; ++i) {
+        for (const Group& g : sv->groups)
+            for (int b = 0; b < 2; ++b) {
+                const bool odd = (b ^ sv->phase) != 0;
+                e = launch_batched(g.Q, g.st, sv->d_slots, sv->d_table + g.off[b], g.ntiles[b], g.grid[b], odd, g.op,
+                                   g.rheo, sv->stream);
+                if (e != cudaSuccess) return cuda_status(e, "batched step");
             }
+        e = launch_batch_advance(sv->d_slots, sv->nslots, sv->stream);
+        if (e != cudaSuccess) return cuda_status(e, "batch advance");
+        sv->phase ^= 1;
+        for (int idx : sv->own_res) {
+            vlbm_status st = fluid_step(sv->res[idx].sim);   // advances the mirror
+            if (st != VLBM_OK) return st;
         }
     }
-    for (const Resident& r : sv->res) sv->lattice_updates += (double)r.sim->N * (double)k;
+    for (size_t r = 0; r < sv->res.size(); ++r) {
+        vlbm_sim* s = sv->res[r].sim;
+        if (s->ibm) continue;
+        if (std::find(sv->own_res.begin(), sv->own_res.end(), (int)r) != sv->own_res.end()) continue;
+        for (int i = 0; i < n; ++i) advance_host(s);
+    }
+    for (size_t j = 0; j < sv->ibm_res.size(); ++j) {
+        vlbm_sim* s = sv->res[sv->ibm_res[j]].sim;
+        cudaStream_t side = sv->side_streams[j];
+        e = cudaStreamWaitEvent(side, sv->fork_event, 0);
+        if (e != cudaSuccess) return cuda_status(e, "fork wait");
+        s->stream = side;
+        vlbm_status st = VLBM_OK;
+        for (int i = 0; i < n && st == VLBM_OK; ++i) {
+            st = fluid_step(s);
+            if (st == VLBM_OK) st = ibm_step(s);
+        }
+        s->stream = sv->stream;
+        if (st != VLBM_OK) return st;
+        e = cudaEventRecord(sv->join_events[j], side);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sv->stream, sv->join_events[j], 0);
+        if (e != cudaSuccess) return cuda_status(e, "join");
+    }
     return VLBM_OK;
+}
+
+struct HostState { int parity, side_cur, apply_bc; long long step; };
+
+// Capture `steps` steps starting at the current phase; host mirrors and
+// phase are left as they were (the replay advances them).
+vlbm_status capture(vlbm_server* sv, int steps, cudaGraphExec_t* out) {
+    std::vector<HostState> saved;
+    for (const Resident& r : sv->res) saved.push_back({r.sim->parity, r.sim->side_cur, r.sim->apply_bc, r.sim->step});
+    const int phase = sv->phase;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(sv->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_status(e, "begin capture");
+    vlbm_status st = enqueue_steps(sv, steps);
+    e = cudaStreamEndCapture(sv->stream, &g);
+    for (size_t i = 0; i < sv->res.size(); ++i) {
+        vlbm_sim* s = sv->res[i].sim;
+        s->parity = saved[i].parity; s->side_cur = saved[i].side_cur;
+        s->apply_bc = saved[i].apply_bc; s->step = saved[i].step;
+    }
+    sv->phase = phase;
+    if (st != VLBM_OK) { if (g) cudaGraphDestroy(g); return st; }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
+    if (g) cudaGraphDestroy(g);
+    return cuda_status(e, "server step graph");
+}
+
+vlbm_status replay(vlbm_server* sv, cudaGraphExec_t* slot, int steps) {
+    if (!*slot) {
+        vlbm_status st = capture(sv, steps, slot);
+        if (st != VLBM_OK) return st;
+    }
+    cudaError_t e = cudaGraphLaunch(*slot, sv->stream);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGraphLaunch");
+    for (Resident& r : sv->res)
+        for (int i = 0; i < steps; ++i) advance_host(r.sim);
+    sv->phase ^= steps & 1;
+    return VLBM_OK;
+}
+
+vlbm_status server_steps(vlbm_server* sv, uint64_t k) {
+    if (sv->res.empty() || k == 0) return VLBM_OK;
+    vlbm_status st = VLBM_OK;
+    uint64_t left = k;
+    while (left > 0 && st == VLBM_OK) {
+        // Lattices with their own launches take the boundary flag from the
+        // host mirror: their first step (no boundary rule yet) runs outside
+        // the graphs, whose steps all apply the rule.
+        bool direct = false;
+        for (int idx : sv->ibm_res) direct |= sv->res[idx].sim->apply_bc == 0;
+        for (int idx : sv->own_res) direct |= sv->res[idx].sim->apply_bc == 0;
+        if (direct) {
+            st = enqueue_steps(sv, 1);
+            left -= 1;
+        } else if (left >= (uint64_t)kGraphSteps) {
+            st = replay(sv, &sv->graphK[sv->phase], kGraphSteps);
+            left -= kGraphSteps;
+        } else {
+            st = replay(sv, &sv->graph1[sv->phase], 1);
+            left -= 1;
+        }
+    }
+    for (const Resident& r : sv->res) sv->lattice_updates += (double)r.sim->N * (double)(k - left);
+    return st;
 }
 
 void fail_request(vlbm_server* sv, const Pending& p, vlbm_status st) {
@@ -280,6 +535,11 @@ void fail_request(vlbm_server* sv, const Pending& p, vlbm_status st) {
     sv->done.push_back(c);
 }
 
+// Admit queued requests in arrival order while the slot limit and the HBM
+// budget allow.  A new lattice is built on its own stream (its set-up copies
+// and kernels do not wait for the queued batch work) from the server's memory
+// cache, then moved to the server stream; it joins the batch at the next
+// table rebuild.
 vlbm_status server_admit(vlbm_server* sv) {
     while (!sv->queue.empty() && (int)sv->res.size() < sv->max_resident) {
         Pending& p = sv->queue.front();
@@ -288,7 +548,7 @@ vlbm_status server_admit(vlbm_server* sv) {
         cfg.device = sv->device;
         cfg.layout = VLBM_LAYOUT_NATURAL;   // the batched kernel streams one node per thread
         vlbm_sim* s = nullptr;
-        vlbm_status st = vlbm_create(&cfg, &s);
+        vlbm_status st = sim_create(&cfg, &sv->cache, &s);
         if (st == VLBM_OK) {
             std::vector<uint32_t> map((size_t)cfg.nx * cfg.ny * cfg.nz);
             st = vlbm_build_node_map(p.req.builder, cfg.nx, cfg.ny, cfg.nz, map.data(), map.size());
@@ -318,37 +578,103 @@ vlbm_status server_admit(vlbm_server* sv) {
     return VLBM_OK;
 }
 
-vlbm_status server_retire(vlbm_server* sv) {
-    bool any = false;
-    for (const Resident& r : sv->res) any |= (uint64_t)r.sim->step >= r.target;
-    if (!any) return VLBM_OK;
-    cudaError_t e = cudaStreamSynchronize(sv->stream);
-    if (e != cudaSuccess) return cuda_status(e, "server sync");
+// Lattices that reached their step count leave the batch: their ux and
+// divergence word are copied to pinned memory behind an event, on the server
+// stream after their last step.
+vlbm_status begin_retire(vlbm_server* sv) {
     std::vector<Resident> keep;
+    vlbm_status first_error = VLBM_OK;
     for (Resident& r : sv->res) {
         if ((uint64_t)r.sim->step < r.target) { keep.push_back(r); continue; }
-        vlbm_completion c;
-        std::memset(&c, 0, sizeof(c));
-        c.tag = r.tag;
-        c.submit_time_s = r.submit_t;
-        c.start_time_s = r.start_t;
-        c.steps = (uint64_t)r.sim->step;
-        c.status = vlbm_sync(r.sim);
-        std::vector<float> ux((size_t)r.sim->N);
-        if (c.status == VLBM_OK)
-            c.status = vlbm_get_macroscopics(r.sim, nullptr, ux.data(), nullptr, nullptr, nullptr);
-        double sum = 0.0;
-        for (float v : ux) sum += v;
-        c.mean_ux = sum / (double)r.sim->N;
-        c.finish_time_s = now_s();
-        sv->done.push_back(c);
-        sv->results.emplace_back(r.tag, std::move(ux));
-        while (sv->results.size() > kKeptResults) sv->results.pop_front();
-        sv->bytes_in_use -= r.bytes;
-        vlbm_destroy(r.sim);
+        Retiring t;
+        t.r = r;
+        vlbm_sim* s = r.sim;
+        const size_t N = (size_t)s->N;
+        cudaError_t e = sim_malloc(s, (void**)&t.d_ux, N * sizeof(float));
+        t.h_ux = static_cast<float*>(sv->pinned.get(N * sizeof(float)));
+        t.h_err = static_cast<unsigned*>(sv->pinned.get(sizeof(unsigned)));
+        if (e == cudaSuccess && (!t.h_ux || !t.h_err)) e = cudaErrorMemoryAllocation;
+        if (e == cudaSuccess) {
+            const vlbm_status st = sim_macroscopics_device(s, nullptr, t.d_ux, nullptr, nullptr, nullptr);
+            if (st != VLBM_OK) e = cudaErrorLaunchFailure;
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(t.h_ux, t.d_ux, N * sizeof(float), cudaMemcpyDeviceToHost, sv->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(t.h_err, s->err, sizeof(unsigned), cudaMemcpyDeviceToHost, sv->stream);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(t.done, sv->stream);
+        if (e != cudaSuccess) {
+            t.status = cuda_status(e, "retirement read-out");
+            if (first_error == VLBM_OK) first_error = t.status;
+        }
+        sv->retiring.push_back(t);
         sv->dirty = true;
     }
     sv->res.swap(keep);
+    return first_error;
+}
+
+// Record the completions of the read-outs that finished (all of them when
+// `wait`), release their lattices into the memory cache.
+vlbm_status poll_retiring(vlbm_server* sv, bool wait) {
+    std::vector<Retiring> still;
+    for (Retiring& t : sv->retiring) {
+        if (t.status == VLBM_OK && t.done) {
+            const cudaError_t q = wait ? cudaEventSynchronize(t.done) : cudaEventQuery(t.done);
+            if (q == cudaErrorNotReady) { still.push_back(t); continue; }
+            if (q != cudaSuccess) t.status = cuda_status(q, "retirement read-out");
+        }
+        vlbm_sim* s = t.r.sim;
+        const size_t N = (size_t)s->N;
+        vlbm_completion c;
+        std::memset(&c, 0, sizeof(c));
+        c.tag = t.r.tag;
+        c.submit_time_s = t.r.submit_t;
+        c.start_time_s = t.r.start_t;
+        c.steps = (uint64_t)s->step;
+        c.status = t.status;
+        std::vector<float> ux;
+        if (c.status == VLBM_OK) {
+            if (*t.h_err) {
+                c.status = VLBM_ERR_DIVERGED;
+            } else {
+                ux.assign(t.h_ux, t.h_ux + N);
+                double sum = 0.0;
+                for (float v : ux) sum += v;
+                c.mean_ux = sum / (double)N;
+            }
+        }
+        c.finish_time_s = now_s();
+        sv->done.push_back(c);
+        if (!ux.empty()) {
+            sv->results.emplace_back(t.r.tag, std::move(ux));
+            while (sv->results.size() > kKeptResults) sv->results.pop_front();
+        }
+        sv->pinned.put(t.h_ux);
+        sv->pinned.put(t.h_err);
+        if (t.done) cudaEventDestroy(t.done);
+        sim_free(s, t.d_ux);
+        sim_release(s);   // the GPU is done with it: its buffers go back to the cache
+        sv->bytes_in_use -= t.r.bytes;
+    }
+    sv->retiring.swap(still);
+    return VLBM_OK;
+}
+
+// Keep at most kSegmentsInFlight segments queued ahead of the GPU.
+vlbm_status end_segment(vlbm_server* sv) {
+    cudaEvent_t ev = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, sv->stream);
+    if (e != cudaSuccess) { if (ev) cudaEventDestroy(ev); return cuda_status(e, "segment event"); }
+    sv->segments.push_back(ev);
+    while ((int)sv->segments.size() > kSegmentsInFlight) {
+        e = cudaEventSynchronize(sv->segments.front());
+        cudaEventDestroy(sv->segments.front());
+        sv->segments.pop_front();
+        if (e != cudaSuccess) return cuda_status(e, "segment wait");
+    }
     return VLBM_OK;
 }
 
@@ -400,16 +726,53 @@ vlbm_status vlbm_server_pump(vlbm_server* sv, uint32_t steps, vlbm_completion* o
     cudaError_t e = cudaSetDevice(sv->device);
     if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
     uint64_t left = steps;
-    vlbm_status st = server_admit(sv);
-    while (st == VLBM_OK && left > 0 && !sv->res.empty()) {
+    double t0 = now_s();
+    vlbm_status st = poll_retiring(sv, false);
+    double t1 = now_s();
+    sv->prof[4] += t1 - t0;
+    if (st == VLBM_OK) st = server_admit(sv);
+    sv->prof[0] += now_s() - t1;
+    while (st == VLBM_OK && left > 0) {
+        if (sv->res.empty()) {
+            // nothing to step: finish the read-outs, which may free memory for the queue
+            if (sv->retiring.empty()) break;
+            const double t0 = now_s();
+            st = poll_retiring(sv, true);
+            const double t1 = now_s();
+            sv->prof[3] += t1 - t0;
+            if (st == VLBM_OK) st = server_admit(sv);
+            sv->prof[0] += now_s() - t1;
+            continue;
+        }
+        double t0 = now_s();
         if (sv->dirty && (st = server_rebuild(sv)) != VLBM_OK) break;
-        uint64_t k = left;
+        double t1 = now_s();
+        sv->prof[1] += t1 - t0;
+        uint64_t k = std::min<uint64_t>(left, kSegment);
         for (const Resident& r : sv->res) k = std::min<uint64_t>(k, r.target - (uint64_t)r.sim->step);
-        if ((st = server_steps(sv, k)) != VLBM_OK) break;
+        if ((st = server_steps(sv, k)) != VLBM_OK) break;   // graph captures count as enqueue time here
         left -= k;
-        if ((st = server_retire(sv)) != VLBM_OK) break;
-        st = server_admit(sv);
+        if ((st = begin_retire(sv)) != VLBM_OK) break;
+        t0 = now_s();
+        sv->prof[2] += t0 - t1;
+        if ((st = end_segment(sv)) != VLBM_OK) break;
+        t1 = now_s();
+        sv->prof[3] += t1 - t0;
+        // host work while the GPU runs the queued segments
+        if ((st = server_admit(sv)) != VLBM_OK) break;
+        t0 = now_s();
+        sv->prof[0] += t0 - t1;
+        st = poll_retiring(sv, false);
+        sv->prof[4] += now_s() - t0;
     }
+    // an idle server hands back everything it finished
+    if (st == VLBM_OK && sv->res.empty() && !sv->retiring.empty()) {
+        t0 = now_s();
+        st = poll_retiring(sv, true);
+        sv->prof[3] += now_s() - t0;
+    }
+    // cached memory above the budget goes back to the device
+    if (sv->cache.free_bytes + sv->cache.live_bytes > sv->budget + sv->budget / 2) sv->cache.trim(sv->budget / 2);
     int32_t n = 0;
     while (!sv->done.empty() && n < max_out) {
         out[n++] = sv->done.front();
@@ -422,7 +785,7 @@ vlbm_status vlbm_server_pump(vlbm_server* sv, uint32_t steps, vlbm_completion* o
 vlbm_status vlbm_server_stats(vlbm_server* sv, int32_t* resident, int32_t* queued, int64_t* bytes,
                               double* lattice_updates) {
     if (!sv) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
-    if (resident) *resident = (int32_t)sv->res.size();
+    if (resident) *resident = (int32_t)(sv->res.size() + sv->retiring.size());   // lattices holding device memory
     if (queued) *queued = (int32_t)sv->queue.size();
     if (bytes) *bytes = (int64_t)sv->bytes_in_use;
     if (lattice_updates) *lattice_updates = sv->lattice_updates;
@@ -440,6 +803,12 @@ vlbm_status vlbm_server_fetch(vlbm_server* sv, uint64_t tag, float* ux, size_t n
         }
     set_last_error("no finished request with that tag is kept");
     return VLBM_ERR_NOT_FOUND;
+}
+
+vlbm_status vlbm_server_profile(vlbm_server* sv, double* seconds, int32_t n) {
+    if (!sv || (n > 0 && !seconds)) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    for (int32_t i = 0; i < n && i < 5; ++i) seconds[i] = sv->prof[i];
+    return VLBM_OK;
 }
 
 vlbm_status vlbm_server_destroy(vlbm_server* sv) {

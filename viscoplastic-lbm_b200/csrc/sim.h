@@ -16,6 +16,16 @@ struct DeviceBuffer {
     size_t bytes = 0;
 };
 
+// Source of a simulation's device memory.  Without one a simulation uses
+// cudaMalloc/cudaFree; the serving loop passes a cache that recycles the
+// buffers of retired lattices, because cudaFree synchronises the whole device
+// and would drain the work queued for the other lattices.
+struct DeviceAllocator {
+    virtual cudaError_t allocate(void** p, size_t bytes) = 0;
+    virtual void release(void* p) = 0;
+    virtual ~DeviceAllocator() = default;
+};
+
 }  // namespace vlbm
 
 struct vlbm_sim {
@@ -54,12 +64,23 @@ struct vlbm_sim {
     vlbm::BcTables tables;
 
     vlbm::IbmState* ibm = nullptr;   // owned; released by ibm_destroy
+    vlbm::DeviceAllocator* allocator = nullptr;   // not owned; nullptr: cudaMalloc/cudaFree
     ~vlbm_sim();
 };
 
 namespace vlbm {
 
 StepParams make_params(vlbm_sim* s);
+// Device memory of a simulation, through its allocator (if any).
+cudaError_t sim_malloc(vlbm_sim* s, void** p, size_t bytes);
+void sim_free(vlbm_sim* s, void* p);
+cudaError_t alloc_with(DeviceAllocator* a, void** p, size_t bytes);
+void free_with(DeviceAllocator* a, void* p);
+// vlbm_create with a device-memory source (nullptr: cudaMalloc/cudaFree).
+vlbm_status sim_create(const vlbm_config* cfg, DeviceAllocator* allocator, vlbm_sim** out);
+// Free a simulation whose device work is known to be complete (no stream
+// synchronisation).
+void sim_release(vlbm_sim* s);
 vlbm_status cuda_status(cudaError_t e, const char* what);
 vlbm_status fluid_step(vlbm_sim* s);   // one fused step (no IBM)
 vlbm_status sim_macroscopics_device(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz, float* omega);
@@ -72,7 +93,7 @@ cudaError_t launch_moments_sum(vlbm_sim* s, double* partials, double* out);
 // IBM hooks (ibm.cu)
 vlbm_status ibm_step(vlbm_sim* s);
 vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz);
-void ibm_destroy(IbmState* st);
+void ibm_destroy(IbmState* st, DeviceAllocator* allocator);
 void ibm_reset(vlbm_sim* s);
 void ibm_counts(const vlbm_sim* s, int* np, int* nn);
 

@@ -564,10 +564,11 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
 // Many lattices of one (velocity set, operator, rheology, storage) group
 // advance in one launch.  The launch walks a table of tiles (lattice slot,
 // first node; BATCH_TILE consecutive nodes each) with a grid-stride loop, so a
-// grid of a few blocks per SM is persistent over all lattices.  The step state
-// of every lattice (AA parity, which side-store buffer is current, whether the
-// boundary rule applies) lives in its slot in device memory and is advanced by
-// k_batch_advance after the group launches, so one captured step can be
+// grid of a few blocks per SM is persistent over all lattices.  Lattices whose
+// AA parity differs go to different tables (the parity is a template argument,
+// as in k_step); the side-store buffer index and the boundary flag of every
+// lattice live in its slot in device memory and are advanced by
+// k_batch_advance after the group launches, so a captured step can be
 // replayed any number of times.
 constexpr int BATCH_TILE = 256;
 
@@ -581,11 +582,10 @@ struct BatchBlock {
     unsigned first;     // first node of this tile
 };
 
-template <int Q, int OP, int RHEO, int ST>
+template <int Q, int OP, int RHEO, int ST, bool ODD>
 __global__ void __launch_bounds__(256) k_step_batched(const BatchSlot* __restrict__ slots,
                                                       const BatchBlock* __restrict__ table, int ntiles) {
     __shared__ StepParams sp;
-    __shared__ int odd;
     constexpr int WORDS = (int)(sizeof(StepParams) / 4);
     static_assert(sizeof(StepParams) % 4 == 0, "StepParams is copied as 32-bit words");
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -600,14 +600,10 @@ __global__ void __launch_bounds__(256) k_step_batched(const BatchSlot* __restric
             sp.side_prev = s->side[cur];
             sp.side_next = s->side[cur ^ 1];
             sp.apply_bc = s->apply_bc;
-            odd = s->parity;
         }
         __syncthreads();
         const unsigned n = e.first + threadIdx.x;
-        if (n < (unsigned)sp.N) {
-            if (odd) step_node<Q, OP, RHEO, ST, true>(sp, n);
-            else step_node<Q, OP, RHEO, ST, false>(sp, n);
-        }
+        if (n < (unsigned)sp.N) step_node<Q, OP, RHEO, ST, ODD>(sp, n);
     }
 }
 

@@ -194,6 +194,7 @@ _SIGS = {
     "vlbm_server_stats": [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                           C.POINTER(C.c_int64), C.POINTER(C.c_double)],
     "vlbm_server_fetch": [_P, C.c_uint64, _F32P, C.c_size_t],
+    "vlbm_server_profile": [_P, _F64P, C.c_int32],
     "vlbm_server_destroy": [_P],
     "vlbm_autotune": [_P, C.POINTER(C.c_int32)],
     "vlbm_set_variant": [_P, C.c_int32],
@@ -388,6 +389,12 @@ class Server:
         _check(_lib.vlbm_server_stats(self._h, C.byref(r), C.byref(q), C.byref(b), C.byref(lu)),
                "vlbm_server_stats")
         return {"resident": r.value, "queued": q.value, "bytes": b.value, "lattice_updates": lu.value}
+
+    def profile(self):
+        """Host seconds spent in admission, rebuild+capture, enqueue, GPU waits, read-outs."""
+        out = (C.c_double * 5)()
+        _check(_lib.vlbm_server_profile(self._h, out, 5), "vlbm_server_profile")
+        return dict(zip(("admit", "rebuild", "enqueue", "wait", "readout"), list(out)))
 
     def fetch(self, tag, n):
         out = np.empty(n, dtype=np.float32)
