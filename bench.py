@@ -294,7 +294,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-step-scale", type=float, default=0.25)
-    ap.add_argument("--serving-rate", type=float, default=20.0)
+    ap.add_argument("--serving-rate", type=float, default=200.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -142,6 +142,10 @@ vlbm_status vlbm_destroy(vlbm_sim* sim);
  * map in the reference's bit layout, [nz][ny][nx] order (idxScalar,
  * globalFunctions.h:111-115).  n must equal nx*ny*nz. */
 vlbm_status vlbm_set_node_map(vlbm_sim* sim, const uint32_t* map, size_t n);
+/* Same tables as vlbm_build_node_map(builder, ...) + vlbm_set_node_map, built
+ * from the builder's rules on the domain faces only (no N-word map on the
+ * host): the set-up cost scales with the lattice surface, not its volume. */
+vlbm_status vlbm_set_builder(vlbm_sim* sim, int32_t builder);
 
 /* Host-side restatement of the named builders; writes nx*ny*nz words. */
 vlbm_status vlbm_build_node_map(int builder, int nx, int ny, int nz, uint32_t* map_out, size_t n);
@@ -306,11 +310,19 @@ vlbm_status vlbm_server_stats(vlbm_server* srv, int32_t* resident, int32_t* queu
                               int64_t* bytes_in_use, double* lattice_updates);
 /* Copy the macroscopics of the finished request `tag` (kept until fetched). */
 vlbm_status vlbm_server_fetch(vlbm_server* srv, uint64_t tag, float* ux, size_t n);
-/* Host seconds the server spent, since creation, in: [0] admission (building
- * new lattices), [1] table rebuilds and graph captures, [2] enqueuing steps,
- * [3] waiting for the GPU (queue depth limit, idle read-outs), [4] completing
- * read-outs.  Writes min(n, 5) values. */
+/* Counters since creation.  Host seconds in: [0] admission (building new
+ * lattices), [1] table rebuilds, [2] enqueuing steps (graph captures
+ * included), [3] waiting for the GPU (queue depth limit, idle read-outs),
+ * [4] completing read-outs; then [5] batch steps, [6] kernels launched
+ * directly, [7] graph launches, [8] graph captures, [9] host seconds in graph
+ * captures (part of [2]).  Writes min(n, 10) values. */
 vlbm_status vlbm_server_profile(vlbm_server* srv, double* seconds, int32_t n);
+/* Tuning: sphere-free lattices with at least `nodes` nodes get their own
+ * single-lattice launch each step instead of sharing the batched launch.
+ * -1 (the default): lattices that fill a wave of the batched kernel (148 SMs x
+ * resident blocks x 256 nodes) get one, largest first, while the estimated
+ * host launch time of a step stays below 60 % of its estimated GPU time. */
+vlbm_status vlbm_server_set_own_launch_min(vlbm_server* srv, int64_t nodes);
 vlbm_status vlbm_server_destroy(vlbm_server* srv);
 
 /* --------------------------------------------------------------- misc --- */

@@ -109,16 +109,67 @@ static vlbm_status alloc_dev(vlbm_sim* s, void** p, size_t bytes) {
     return VLBM_OK;
 }
 
+// Side store of the boundary nodes at rest equilibrium: side[b][i][slot] = w_i rho0.
+__global__ void k_fill_side(float* s0, float* s1, int nbc, int Q, float rho0) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (long long)Q * nbc) return;
+    const int i = (int)(k / nbc);
+    const float v = (float)(Q == 19 ? Lattice<19>::w(i) : Lattice<27>::w(i)) * rho0;
+    s0[k] = v;
+    s1[k] = v;
+}
+
+// Class bytes and slot indices of the boundary nodes (all others stay bulk).
+__global__ void k_scatter_bc(const int32_t* bc_node, int nbc, uint8_t* cls, int32_t* bc_slot) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nbc) return;
+    const int32_t n = bc_node[s];
+    cls[n] = NODE_BC;
+    bc_slot[n] = s;
+}
+
 static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
     if (s->nbc == 0) return VLBM_OK;
-    std::vector<float> h((size_t)s->Q * s->nbc);
-    for (int i = 0; i < s->Q; ++i) {
-        float v = (float)(lattice_weight(s->Q, i) * s->cfg.rho0);
-        for (int k = 0; k < s->nbc; ++k) h[(size_t)i * s->nbc + k] = v;
-    }
-    for (int b = 0; b < 2; ++b)
-        VLBM_CUDA(cudaMemcpyAsync(s->side[b], h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    const long long tot = (long long)s->Q * s->nbc;
+    k_fill_side<<<(unsigned)((tot + 255) / 256), 256, 0, s->stream>>>(s->side[0], s->side[1], s->nbc, s->Q,
+                                                                        (float)s->cfg.rho0);
+    VLBM_CUDA(cudaGetLastError());
     VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    return VLBM_OK;
+}
+
+// Install boundary tables: class bytes and slots (bulk everywhere, then the
+// boundary nodes scattered on the device), the records and the side store.
+static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    sim_free(s, s->bc); sim_free(s, s->side[0]); sim_free(s, s->side[1]); sim_free(s, s->bc_node);
+    s->bc = nullptr; s->side[0] = s->side[1] = nullptr; s->bc_node = nullptr;
+    s->nbc = (int)t.recs.size();
+    const size_t N = (size_t)s->N;
+    VLBM_CUDA(cudaMemsetAsync(s->cls, 0, (N + 3) & ~(size_t)3, s->stream));
+    VLBM_CUDA(cudaMemsetAsync(s->bc_slot, 0xff, N * sizeof(int32_t), s->stream));
+    if (s->nbc > 0) {
+        void* p;
+        vlbm_status st;
+        if ((st = alloc_dev(s, &p, t.recs.size() * sizeof(BcRec))) != VLBM_OK) return st;
+        s->bc = static_cast<BcRec*>(p);
+        if ((st = alloc_dev(s, &p, t.bc_nodes.size() * sizeof(int32_t))) != VLBM_OK) return st;
+        s->bc_node = static_cast<int32_t*>(p);
+        for (int b = 0; b < 2; ++b) {
+            if ((st = alloc_dev(s, &p, (size_t)s->Q * s->nbc * sizeof(float))) != VLBM_OK) return st;
+            s->side[b] = static_cast<float*>(p);
+        }
+        VLBM_CUDA(cudaMemcpyAsync(s->bc, t.recs.data(), t.recs.size() * sizeof(BcRec), cudaMemcpyHostToDevice,
+                                  s->stream));
+        VLBM_CUDA(cudaMemcpyAsync(s->bc_node, t.bc_nodes.data(), t.bc_nodes.size() * sizeof(int32_t),
+                                  cudaMemcpyHostToDevice, s->stream));
+        k_scatter_bc<<<(s->nbc + 255) / 256, 256, 0, s->stream>>>(s->bc_node, s->nbc, s->cls, s->bc_slot);
+        VLBM_CUDA(cudaGetLastError());
+        if ((st = fill_side_equilibrium(s)) != VLBM_OK) return st;   // synchronises the stream
+    } else {
+        VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    s->geometry = true;
     return VLBM_OK;
 }
 
@@ -149,8 +200,8 @@ using namespace vlbm;
 
 vlbm_sim::~vlbm_sim() {
     if (ibm) { ibm_destroy(ibm, allocator); ibm = nullptr; }
-    for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)side[0], (void*)side[1], (void*)omega,
-                    (void*)fibm, (void*)err, (void*)scratch, (void*)red_scratch})
+    for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)bc_node, (void*)side[0], (void*)side[1],
+                    (void*)omega, (void*)fibm, (void*)err, (void*)scratch, (void*)red_scratch})
         free_with(allocator, p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -273,27 +324,16 @@ vlbm_status vlbm_set_node_map(vlbm_sim* s, const uint32_t* map, size_t n) {
     BcTables t;
     vlbm_status st = build_bc_tables(s->cfg, map, n, t, why);
     if (st != VLBM_OK) { set_last_error(why); return st; }
-    VLBM_CUDA(cudaStreamSynchronize(s->stream));
-    sim_free(s, s->bc); sim_free(s, s->side[0]); sim_free(s, s->side[1]);
-    s->bc = nullptr; s->side[0] = s->side[1] = nullptr;
-    s->nbc = (int)t.recs.size();
-    VLBM_CUDA(cudaMemcpy(s->cls, t.cls.data(), t.cls.size(), cudaMemcpyHostToDevice));
-    VLBM_CUDA(cudaMemcpy(s->bc_slot, t.slot.data(), t.slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    if (s->nbc > 0) {
-        void* p;
-        if ((st = alloc_dev(s, &p, t.recs.size() * sizeof(BcRec))) != VLBM_OK) return st;
-        s->bc = static_cast<BcRec*>(p);
-        VLBM_CUDA(cudaMemcpy(s->bc, t.recs.data(), t.recs.size() * sizeof(BcRec), cudaMemcpyHostToDevice));
-        for (int b = 0; b < 2; ++b) {
-            if ((st = alloc_dev(s, &p, (size_t)s->Q * s->nbc * sizeof(float))) != VLBM_OK) return st;
-            s->side[b] = static_cast<float*>(p);
-        }
-        if ((st = fill_side_equilibrium(s)) != VLBM_OK) return st;
-    }
-    s->host_map.assign(map, map + n);
-    s->tables = std::move(t);
-    s->geometry = true;
-    return VLBM_OK;
+    return install_tables(s, t);
+}
+
+vlbm_status vlbm_set_builder(vlbm_sim* s, int32_t builder) {
+    CHECK_SIM(s);
+    std::string why;
+    BcTables t;
+    vlbm_status st = build_bc_tables_builder(s->cfg, builder, t, why);
+    if (st != VLBM_OK) { set_last_error(why); return st; }
+    return install_tables(s, t);
 }
 
 vlbm_status vlbm_init_equilibrium(vlbm_sim* s, double rho, double ux, double uy, double uz) {

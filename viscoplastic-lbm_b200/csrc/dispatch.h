@@ -21,11 +21,12 @@ template <int Q, int ST>
 cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, float ux, float uy, float uz,
                                cudaStream_t s);
 
-struct BatchSlot;
+struct BatchLaunch;
+struct BatchState;
 struct BatchBlock;
 template <int Q, int ST>
-cudaError_t launch_batched_st(const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid, bool odd, int op,
-                              int rheo, cudaStream_t s);
+cudaError_t launch_batched_st(const BatchLaunch& L, const BatchState* state, const BatchBlock* table, int ntiles,
+                              int grid, bool odd, int op, int rheo, cudaStream_t s);
 
 // Run-time selection over (Q, storage).
 cudaError_t launch_step(int Q, int st, const StepParams& p, int op, int rheo, bool odd, LaunchShape ls,
@@ -37,13 +38,13 @@ cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in,
 // One batched step of the lattices of a (Q, storage, op, rheology) group that
 // share the AA parity `odd`: ntiles table entries walked by `grid` persistent
 // blocks of 256 threads.
-cudaError_t launch_batched(int Q, int st, const BatchSlot* slots, const BatchBlock* table, int ntiles, int grid,
-                           bool odd, int op, int rheo, cudaStream_t s);
+cudaError_t launch_batched(int Q, int st, const BatchLaunch& L, const BatchState* state, const BatchBlock* table,
+                           int ntiles, int grid, bool odd, int op, int rheo, cudaStream_t s);
 // Resident 256-thread blocks per SM of the batched kernel of a group.
 int batched_blocks_per_sm(int Q, int st, int op, int rheo);
 template <int Q, int ST>
 int batched_occupancy_st(int op, int rheo);
-// Advance the per-lattice step state of nslots slots (parity, side buffer, boundary flag).
-cudaError_t launch_batch_advance(BatchSlot* slots, int nslots, cudaStream_t s);
+// Advance the per-lattice step state of nslots lattices (parity, side buffer, boundary flag).
+cudaError_t launch_batch_advance(BatchState* state, int nslots, cudaStream_t s);
 
 }  // namespace vlbm

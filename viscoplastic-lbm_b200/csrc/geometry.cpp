@@ -3,10 +3,14 @@
 // The builders restate the reference's gpuBuildBoundaryConditions variants
 // (src/CUDA/boundaryConditionsBuilders/*.cu) on the host and produce the same
 // 32-bit words (bit layout src/CUDA/structs/nodeTypeMap.h:15-133).  The table
-// builder turns such a map into what the fused kernel reads: one class byte per
-// node, a slot index for boundary nodes and one BcRec per boundary node.
+// builder turns such a map (or a named builder directly, visiting only the
+// domain faces) into what the fused kernel reads: one BcRec and the node index
+// of each boundary slot; the class bytes and slot indices are scattered on the
+// device.
+#include <algorithm>
 #include <cstring>
 #include <string>
+#include <vector>
 #include "internal.h"
 #include "lattice.cuh"
 
@@ -87,97 +91,211 @@ int bb_role(int dir, int i) {
     return (neg && pos) ? 2 : (neg ? 1 : 0);
 }
 
-vlbm_status build_bc_tables(const vlbm_config& cfg, const uint32_t* map, size_t n, BcTables& out,
-                            std::string& err) {
+// Word of node (x, y, z) for a named builder; false for an unknown builder id.
+// Only nodes on the domain faces get a non-bulk word.
+bool builder_word(int builder, int x, int y, int z, int nx, int ny, int nz, uint32_t& w) {
+    w = make_word(VLBM_BC_NULL, 0);
+    int d;
+    switch (builder) {
+    case VLBM_BUILDER_PERIODIC: break;
+    case VLBM_BUILDER_PLATES_Y:  // parallelPlatesBounceBack_Y.cu:57-159
+        if (y == 0) w = make_word(VLBM_BC_BOUNCE_BACK, VLBM_SOUTH);
+        else if (y == ny - 1) w = make_word(VLBM_BC_BOUNCE_BACK, VLBM_NORTH);
+        break;
+    case VLBM_BUILDER_PLATES_Y_FREE_SLIP:  // parallelPlatesBounceBackFreeSlip.cu
+        if (y == 0) w = make_word(VLBM_BC_BOUNCE_BACK, VLBM_SOUTH);
+        else if (y == ny - 1) w = make_word(VLBM_BC_FREE_SLIP, VLBM_NORTH);
+        break;
+    case VLBM_BUILDER_PLATES_Y_ZOUHE:  // couetteZouHe.cu
+        if (y == 0) w = make_word(VLBM_BC_VEL_ZOUHE, VLBM_SOUTH, 0, 0, 2);
+        else if (y == ny - 1) w = make_word(VLBM_BC_VEL_ZOUHE, VLBM_NORTH, 0, 0, 1);
+        break;
+    case VLBM_BUILDER_LID_DRIVEN:  // lidDrivenBounceBack.cu:57-170 (z periodic)
+    case VLBM_BUILDER_SQUARE_DUCT: {  // squareDuctBounceBack.cu (z periodic)
+        d = combine_dir(side(y, ny, true), side(x, nx, true), 0);
+        if (d < 0) break;
+        if (builder == VLBM_BUILDER_LID_DRIVEN && d == VLBM_NORTH)
+            w = make_word(VLBM_BC_VEL_BOUNCE_BACK, VLBM_NORTH, 1);
+        else
+            w = make_word(VLBM_BC_BOUNCE_BACK, d);
+        break;
+    }
+    case VLBM_BUILDER_DUCT_YZ:  // walls y and z, periodic x
+        d = combine_dir(side(y, ny, true), 0, side(z, nz, true));
+        if (d >= 0) w = make_word(VLBM_BC_BOUNCE_BACK, d);
+        break;
+    case VLBM_BUILDER_CLOSED_BOX:  // closedBoxBounceBack.cu:56-208
+    case VLBM_BUILDER_LID_CAVITY_CLOSED:
+        d = combine_dir(side(y, ny, true), side(x, nx, true), side(z, nz, true));
+        if (d < 0) break;
+        if (builder == VLBM_BUILDER_LID_CAVITY_CLOSED && d == VLBM_NORTH)
+            w = make_word(VLBM_BC_VEL_BOUNCE_BACK, VLBM_NORTH, 1);
+        else
+            w = make_word(VLBM_BC_BOUNCE_BACK, d);
+        break;
+    default:
+        return false;
+    }
+    return true;
+}
+
+namespace {
+
+bool needs_slot(uint32_t m) {
+    const int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
+    const bool save = (m >> VLBM_MAP_SAVE_POST_COL_OFFSET) & 1u;
+    return scheme != VLBM_BC_NULL || save;
+}
+
+// Boundary records from the candidate nodes (node index, map word) of the
+// nodes whose word asks for a slot, in increasing node order.  word_at(k)
+// gives the word of any node (free-slip neighbours).
+template <class WordAt>
+vlbm_status tables_from_candidates(const vlbm_config& cfg, std::vector<std::pair<size_t, uint32_t>>& cand,
+                                   WordAt word_at, BcTables& out) {
     const int Q = cfg.vel_set;
     const int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
-    const size_t N = (size_t)nx * ny * nz;
-    if (n != N) { err = "node map size does not match nx*ny*nz"; return VLBM_ERR_INVALID; }
-    out.cls.assign(N, NODE_BULK);
-    out.slot.assign(N, -1);
-    out.recs.clear();
-    out.bc_nodes.clear();
-    std::vector<uint8_t> need_slot(N, 0);
-    for (size_t k = 0; k < N; ++k) {
-        uint32_t m = map[k];
-        if (!((m >> VLBM_MAP_IS_USED_OFFSET) & 1u)) {
-            err = "nodes marked unused (interpolated-bounce-back duct builders) are not supported";
-            return VLBM_ERR_UNSUPPORTED;
-        }
-        int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
-        bool save = (m >> VLBM_MAP_SAVE_POST_COL_OFFSET) & 1u;
-        if (scheme == VLBM_BC_INTERP_BOUNCE_BACK || scheme == VLBM_BC_SPECIAL) {
-            err = "interpolated bounce-back and builder-specific (SPECIAL) schemes are not supported";
-            return VLBM_ERR_UNSUPPORTED;
-        }
-        if (scheme != VLBM_BC_NULL || save) need_slot[k] = 1;
-    }
     // Free-slip reads post-collision populations of tangential neighbours
     // (freeSlip.cu:26-167); make sure those neighbours keep them.
-    for (size_t k = 0; k < N; ++k) {
-        uint32_t m = map[k];
+    const size_t ncand = cand.size();
+    bool added = false;
+    for (size_t c = 0; c < ncand; ++c) {
+        const size_t k = cand[c].first;
+        const uint32_t m = cand[c].second;
         if (((m >> VLBM_MAP_SCHEME_OFFSET) & 7) != VLBM_BC_FREE_SLIP) continue;
-        int dir = (m >> VLBM_MAP_DIRECTION_OFFSET) & 31;
+        const int dir = (m >> VLBM_MAP_DIRECTION_OFFSET) & 31;
         if (dir > VLBM_BACK) continue;
         int nrm[3][3];
         dir_normals(dir, nrm);
-        int x = (int)(k % nx), y = (int)((k / nx) % ny), z = (int)(k / ((size_t)nx * ny));
+        const int x = (int)(k % nx), y = (int)((k / nx) % ny), z = (int)(k / ((size_t)nx * ny));
         for (int i = 1; i < Q; ++i) {
             if (bb_role(dir, i) != 1) continue;
             int t[3] = {lat_cx(i), lat_cy(i), lat_cz(i)};
             for (int a = 0; a < 3; ++a) if (nrm[0][a] != 0) t[a] = 0;
-            int xs = ((x - t[0]) % nx + nx) % nx, ys = ((y - t[1]) % ny + ny) % ny,
-                zs = ((z - t[2]) % nz + nz) % nz;
-            need_slot[(size_t)nx * ((size_t)ny * zs + ys) + xs] = 1;
+            const int xs = ((x - t[0]) % nx + nx) % nx, ys = ((y - t[1]) % ny + ny) % ny,
+                      zs = ((z - t[2]) % nz + nz) % nz;
+            const size_t kn = (size_t)nx * ((size_t)ny * zs + ys) + xs;
+            cand.emplace_back(kn, word_at(kn));
+            added = true;
         }
     }
-    for (size_t k = 0; k < N; ++k) {
-        if (!need_slot[k]) continue;
-        uint32_t m = map[k];
-        int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
-        int dir = (m >> VLBM_MAP_DIRECTION_OFFSET) & 31;
-        int geo = (m >> VLBM_MAP_GEOMETRY_OFFSET) & 1;
-        BcRec r;
-        std::memset(&r, 0, sizeof(r));
-        r.scheme = K_BC_NONE;
-        r.dir = (uint8_t)dir;
-        r.uw[0] = (float)cfg.ux_bc[(m >> VLBM_MAP_UX_IDX_OFFSET) & 7];
-        r.uw[1] = (float)cfg.uy_bc[(m >> VLBM_MAP_UY_IDX_OFFSET) & 7];
-        r.uw[2] = (float)cfg.uz_bc[(m >> VLBM_MAP_UZ_IDX_OFFSET) & 7];
-        r.rhow = (float)cfg.rho_bc[(m >> VLBM_MAP_RHO_IDX_OFFSET) & 7];
-        int nrm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        dir_normals(dir, nrm);
-        r.axis = nrm[0][0] != 0 ? 0 : (nrm[0][1] != 0 ? 1 : 2);
-        uint32_t mask = 0;
+    if (added) {
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    }
+    // bounce-back role masks per direction
+    uint32_t role_mask[26];
+    for (int d = 0; d < 26; ++d) {
+        role_mask[d] = 0;
         for (int i = 1; i < Q; ++i)
-            if (bb_role(dir, i) == 1) mask |= 1u << i;
-        switch (scheme) {
-        case VLBM_BC_BOUNCE_BACK:
-            // edges/corners act only when concave (boundaryConditionsHandler.cu:158-256)
-            if (dir < VLBM_NORTH_WEST || geo == VLBM_CONCAVE) { r.scheme = K_BC_BOUNCE; r.mask = mask; }
-            break;
-        case VLBM_BC_VEL_BOUNCE_BACK:
-            // faces only (boundaryConditionsHandler.cu:274-304); D3Q27 extends the D3Q19 rule
-            if (dir <= VLBM_BACK) { r.scheme = K_BC_VEL_BOUNCE; r.mask = mask; }
-            break;
-        case VLBM_BC_FREE_SLIP:
-            if (dir <= VLBM_BACK) { r.scheme = K_BC_FREE_SLIP; r.mask = mask; }
-            break;
-        case VLBM_BC_VEL_ZOUHE:
-            // D3Q19 faces only; the reference compiles an empty body for D3Q27
-            if (Q == 19 && dir <= VLBM_BACK) { r.scheme = K_BC_VEL_ZOUHE; r.mask = mask; }
-            break;
-        case VLBM_BC_PRES_ZOUHE:
-            if (Q == 19 && dir <= VLBM_BACK) { r.scheme = K_BC_PRES_ZOUHE; r.mask = mask; }
-            break;
-        default: break;
+            if (bb_role(d, i) == 1) role_mask[d] |= 1u << i;
+    }
+    out.recs.clear();
+    out.bc_nodes.clear();
+    out.recs.reserve(cand.size());
+    out.bc_nodes.reserve(cand.size());
+    uint32_t last_word = 0;
+    BcRec last{};
+    bool have_last = false;
+    for (const auto& kw : cand) {
+        const uint32_t m = kw.second;
+        if (!have_last || m != last_word) {   // the record depends on the word only
+            const int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
+            const int dir = (m >> VLBM_MAP_DIRECTION_OFFSET) & 31;
+            const int geo = (m >> VLBM_MAP_GEOMETRY_OFFSET) & 1;
+            BcRec r;
+            std::memset(&r, 0, sizeof(r));
+            r.scheme = K_BC_NONE;
+            r.dir = (uint8_t)dir;
+            r.uw[0] = (float)cfg.ux_bc[(m >> VLBM_MAP_UX_IDX_OFFSET) & 7];
+            r.uw[1] = (float)cfg.uy_bc[(m >> VLBM_MAP_UY_IDX_OFFSET) & 7];
+            r.uw[2] = (float)cfg.uz_bc[(m >> VLBM_MAP_UZ_IDX_OFFSET) & 7];
+            r.rhow = (float)cfg.rho_bc[(m >> VLBM_MAP_RHO_IDX_OFFSET) & 7];
+            int nrm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            dir_normals(dir, nrm);
+            r.axis = nrm[0][0] != 0 ? 0 : (nrm[0][1] != 0 ? 1 : 2);
+            const uint32_t mask = dir < 26 ? role_mask[dir] : 0u;
+            switch (scheme) {
+            case VLBM_BC_BOUNCE_BACK:
+                // edges/corners act only when concave (boundaryConditionsHandler.cu:158-256)
+                if (dir < VLBM_NORTH_WEST || geo == VLBM_CONCAVE) { r.scheme = K_BC_BOUNCE; r.mask = mask; }
+                break;
+            case VLBM_BC_VEL_BOUNCE_BACK:
+                // faces only (boundaryConditionsHandler.cu:274-304); D3Q27 extends the D3Q19 rule
+                if (dir <= VLBM_BACK) { r.scheme = K_BC_VEL_BOUNCE; r.mask = mask; }
+                break;
+            case VLBM_BC_FREE_SLIP:
+                if (dir <= VLBM_BACK) { r.scheme = K_BC_FREE_SLIP; r.mask = mask; }
+                break;
+            case VLBM_BC_VEL_ZOUHE:
+                // D3Q19 faces only; the reference compiles an empty body for D3Q27
+                if (Q == 19 && dir <= VLBM_BACK) { r.scheme = K_BC_VEL_ZOUHE; r.mask = mask; }
+                break;
+            case VLBM_BC_PRES_ZOUHE:
+                if (Q == 19 && dir <= VLBM_BACK) { r.scheme = K_BC_PRES_ZOUHE; r.mask = mask; }
+                break;
+            default: break;
+            }
+            last = r;
+            last_word = m;
+            have_last = true;
         }
-        out.slot[k] = (int32_t)out.recs.size();
-        out.cls[k] = NODE_BC;
-        out.recs.push_back(r);
-        out.bc_nodes.push_back((int32_t)k);
+        out.recs.push_back(last);
+        out.bc_nodes.push_back((int32_t)kw.first);
     }
     return VLBM_OK;
+}
+
+}  // namespace
+
+vlbm_status build_bc_tables(const vlbm_config& cfg, const uint32_t* map, size_t n, BcTables& out,
+                            std::string& err) {
+    const size_t N = (size_t)cfg.nx * cfg.ny * cfg.nz;
+    if (n != N) { err = "node map size does not match nx*ny*nz"; return VLBM_ERR_INVALID; }
+    std::vector<std::pair<size_t, uint32_t>> cand;
+    for (size_t k = 0; k < N; ++k) {
+        const uint32_t m = map[k];
+        if (!((m >> VLBM_MAP_IS_USED_OFFSET) & 1u)) {
+            err = "nodes marked unused (interpolated-bounce-back duct builders) are not supported";
+            return VLBM_ERR_UNSUPPORTED;
+        }
+        const int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
+        if (scheme == VLBM_BC_INTERP_BOUNCE_BACK || scheme == VLBM_BC_SPECIAL) {
+            err = "interpolated bounce-back and builder-specific (SPECIAL) schemes are not supported";
+            return VLBM_ERR_UNSUPPORTED;
+        }
+        if (needs_slot(m)) cand.emplace_back(k, m);
+    }
+    return tables_from_candidates(cfg, cand, [map](size_t k) { return map[k]; }, out);
+}
+
+vlbm_status build_bc_tables_builder(const vlbm_config& cfg, int builder, BcTables& out, std::string& err) {
+    const int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
+    uint32_t w;
+    if (!builder_word(builder, 0, 0, 0, nx, ny, nz, w)) { err = "unknown builder id"; return VLBM_ERR_NOT_FOUND; }
+    auto word_at = [&](size_t k) {
+        uint32_t m;
+        builder_word(builder, (int)(k % nx), (int)((k / nx) % ny), (int)(k / ((size_t)nx * ny)), nx, ny, nz, m);
+        return m;
+    };
+    // the builders mark domain-face nodes only: visit the six faces
+    std::vector<std::pair<size_t, uint32_t>> cand;
+    auto visit = [&](int x, int y, int z) {
+        uint32_t m;
+        builder_word(builder, x, y, z, nx, ny, nz, m);
+        if (needs_slot(m)) cand.emplace_back((size_t)nx * ((size_t)ny * z + y) + x, m);
+    };
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y) {
+            const bool face_yz = (z == 0 || z == nz - 1 || y == 0 || y == ny - 1);
+            if (face_yz) {
+                for (int x = 0; x < nx; ++x) visit(x, y, z);
+            } else {
+                visit(0, y, z);
+                if (nx > 1) visit(nx - 1, y, z);
+            }
+        }
+    return tables_from_candidates(cfg, cand, word_at, out);
 }
 
 }  // namespace vlbm
@@ -191,51 +309,12 @@ extern "C" vlbm_status vlbm_build_node_map(int builder, int nx, int ny, int nz, 
     for (int z = 0; z < nz; ++z)
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) {
-                size_t k = (size_t)nx * ((size_t)ny * z + y) + x;
-                uint32_t w = make_word(VLBM_BC_NULL, 0);
-                int d;
-                switch (builder) {
-                case VLBM_BUILDER_PERIODIC: break;
-                case VLBM_BUILDER_PLATES_Y:  // parallelPlatesBounceBack_Y.cu:57-159
-                    if (y == 0) w = make_word(VLBM_BC_BOUNCE_BACK, VLBM_SOUTH);
-                    else if (y == ny - 1) w = make_word(VLBM_BC_BOUNCE_BACK, VLBM_NORTH);
-                    break;
-                case VLBM_BUILDER_PLATES_Y_FREE_SLIP:  // parallelPlatesBounceBackFreeSlip.cu
-                    if (y == 0) w = make_word(VLBM_BC_BOUNCE_BACK, VLBM_SOUTH);
-                    else if (y == ny - 1) w = make_word(VLBM_BC_FREE_SLIP, VLBM_NORTH);
-                    break;
-                case VLBM_BUILDER_PLATES_Y_ZOUHE:  // couetteZouHe.cu
-                    if (y == 0) w = make_word(VLBM_BC_VEL_ZOUHE, VLBM_SOUTH, 0, 0, 2);
-                    else if (y == ny - 1) w = make_word(VLBM_BC_VEL_ZOUHE, VLBM_NORTH, 0, 0, 1);
-                    break;
-                case VLBM_BUILDER_LID_DRIVEN:  // lidDrivenBounceBack.cu:57-170 (z periodic)
-                case VLBM_BUILDER_SQUARE_DUCT: {  // squareDuctBounceBack.cu (z periodic)
-                    d = combine_dir(side(y, ny, true), side(x, nx, true), 0);
-                    if (d < 0) break;
-                    if (builder == VLBM_BUILDER_LID_DRIVEN && d == VLBM_NORTH)
-                        w = make_word(VLBM_BC_VEL_BOUNCE_BACK, VLBM_NORTH, 1);
-                    else
-                        w = make_word(VLBM_BC_BOUNCE_BACK, d);
-                    break;
-                }
-                case VLBM_BUILDER_DUCT_YZ:  // walls y and z, periodic x
-                    d = combine_dir(side(y, ny, true), 0, side(z, nz, true));
-                    if (d >= 0) w = make_word(VLBM_BC_BOUNCE_BACK, d);
-                    break;
-                case VLBM_BUILDER_CLOSED_BOX:  // closedBoxBounceBack.cu:56-208
-                case VLBM_BUILDER_LID_CAVITY_CLOSED:
-                    d = combine_dir(side(y, ny, true), side(x, nx, true), side(z, nz, true));
-                    if (d < 0) break;
-                    if (builder == VLBM_BUILDER_LID_CAVITY_CLOSED && d == VLBM_NORTH)
-                        w = make_word(VLBM_BC_VEL_BOUNCE_BACK, VLBM_NORTH, 1);
-                    else
-                        w = make_word(VLBM_BC_BOUNCE_BACK, d);
-                    break;
-                default:
+                uint32_t w;
+                if (!builder_word(builder, x, y, z, nx, ny, nz, w)) {
                     set_last_error("unknown builder id");
                     return VLBM_ERR_NOT_FOUND;
                 }
-                map_out[k] = w;
+                map_out[(size_t)nx * ((size_t)ny * z + y) + x] = w;
             }
     return VLBM_OK;
 }

@@ -4,26 +4,31 @@
 // 4*IBM_MAX_ITERATION host-synchronised launches, two of which sweep the whole
 // lattice (gpuUpdateMacrIBM recomputes rho,u everywhere; gpuEulerSumIBMAuxsReset
 // adds the auxiliary fields everywhere, once per iteration).  Here only the
-// Eulerian nodes inside each sphere's stencil support are touched:
+// Eulerian nodes inside each sphere's stencil support are touched, in six
+// launches per step with one forcing iteration (three more per iteration):
 //
-//   k_ibm_box        one CTA per sphere: unwrapped node extent -> Eulerian box,
-//                    node forces reset (gpuResetNodesForces ibm.cu:651-668)
-//   k_ibm_gather     one CTA per sphere: rho,u of the post-boundary populations
-//                    with the constant body force (gpuUpdateMacrIBM ibm.cu:544-648)
-//                    for the box nodes, written to dense fields; each node is
-//                    appended once to a compact list (atomicOr on its class bit)
-//   k_ibm_contacts   one CTA: old values, Hertz-Mindlin contacts with
-//                    deterministic slot updates and sums, predictor
+//   k_ibm_begin      CTAs 0..np-1: unwrapped node extent -> Eulerian box of
+//                    each sphere, node forces reset (gpuResetNodesForces
+//                    ibm.cu:651-668); CTA np: touched-node count reset, old
+//                    values, Hertz-Mindlin contacts with deterministic slot
+//                    updates and sums, predictor
+//   k_ibm_gather     several CTAs per sphere: rho,u of the post-boundary
+//                    populations with the constant body force
+//                    (gpuUpdateMacrIBM ibm.cu:544-648) for the box nodes,
+//                    written to dense fields; each node is appended once to a
+//                    compact list (atomicOr on its class bit)
 //   per multi-direct-forcing iteration:
 //     k_ibm_interp_spread  several CTAs per sphere, one warp per Lagrangian
 //                    node with its 64 stencil points split over the lanes:
 //                    Peskin 4-point interpolation (warp reduction), direct
-//                    forcing, spreading with global atomics; per-CTA
+//                    forcing, spreading with fixed-point atomics; per-CTA
 //                    force/torque partials
 //     k_ibm_update   partials added in a fixed order, particle velocity and
-//                    rotation update
-//     k_ibm_euler    over the node list: u += fAux/(2 rho), F += fAux, fAux = 0
-//   k_ibm_move / k_ibm_move_nodes   particle and Lagrangian node movement
+//                    rotation update; in the last iteration also the particle
+//                    movement and the step clock
+//     k_ibm_euler    over the node list: u += fAux/(2 rho), F += fAux,
+//                    fAux = 0; in the last iteration also the Lagrangian node
+//                    movement
 //
 // Particle state, contacts and integration are FP64; the Eulerian fields FP32.
 #include <cuda_runtime.h>
@@ -117,11 +122,10 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 }
 
 // ---------------------------------------------------------------- box --
-__global__ void __launch_bounds__(IBM_THREADS) k_ibm_box(IbmParams P, DPart* parts, const double* X, const double* Y,
-                                                          const double* Z, double* fx, double* fy, double* fz,
-                                                          double* dx, double* dy, double* dz) {
+__device__ void ibm_box(const IbmParams& P, DPart* parts, int sphere, const double* X, const double* Y,
+                        const double* Z, double* fx, double* fy, double* fz, double* dx, double* dy, double* dz) {
     __shared__ double sh[32];
-    DPart& p = parts[blockIdx.x];
+    DPart& p = parts[sphere];
     const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
     const int Li[3] = {P.nx, P.ny, P.nz};
     double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
@@ -396,11 +400,7 @@ __device__ void update_center(const IbmParams& P, DPart& p) {
     for (int a = 0; a < 3; ++a) p.w[a] = wn[a];
 }
 
-__global__ void __launch_bounds__(IBM_THREADS) k_ibm_contacts(IbmParams P, DPart* parts, double* contrib,
-                                                              const int* steps_taken) {
-    // index of the fluid step just taken (main.cu:270); read on the device so a
-    // captured IBM step can be replayed
-    P.step = *steps_taken;
+__device__ void ibm_contacts(const IbmParams& P, DPart* parts, double* contrib) {
     const int np = P.np;
     // gpuUpdateParticleOldValues ibm.cu:995-1042
     for (int i = threadIdx.x; i < np; i += blockDim.x) {
@@ -446,6 +446,25 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_contacts(IbmParams P, DPart
         }
         update_center(P, pj);  // predictor (ibm.cu:98-103)
     }
+}
+
+// One launch for the start of the IBM step: blocks 0..np-1 find the Eulerian
+// box of their sphere and reset its node forces (k_ibm_box part), block np
+// resets the touched-node count and runs the old-value copy, the contacts and
+// the predictor (they read positions only, which the boxes do not change).
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_begin(IbmParams P, DPart* parts, const double* X, const double* Y,
+                                                            const double* Z, double* fx, double* fy, double* fz,
+                                                            double* dx, double* dy, double* dz, double* contrib,
+                                                            int* count) {
+    if ((int)blockIdx.x < P.np) {
+        ibm_box(P, parts, blockIdx.x, X, Y, Z, fx, fy, fz, dx, dy, dz);
+        return;
+    }
+    // index of the fluid step just taken (main.cu:270), kept on the device so
+    // a captured IBM step can be replayed
+    P.step = count[1];
+    if (threadIdx.x == 0) count[0] = 0;
+    ibm_contacts(P, parts, contrib);
 }
 
 // -------------------------------------------------- interpolation/spread --
@@ -616,7 +635,23 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_interp_spread(IbmParams P, 
         for (int a = 0; a < 6; ++a) fpart[((size_t)sphere * split + sub) * 6 + a] = tot6[a];
 }
 
-__global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int split) {
+// gpuParticleMovement ibm.cu:899-993
+__device__ void move_particle(const IbmParams& P, DPart& p) {
+    if (!p.movable) return;
+    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
+    for (int a = 0; a < 3; ++a) {
+        const double dx = p.vel[a] * P.alpha + p.vel_old[a] * (1.0 - P.alpha);
+        if (P.wall[a]) p.pos[a] += dx;
+        else p.pos[a] = fmod(p.pos[a] + dx + L[a], L[a]);
+        p.w_avg[a] = p.w[a] * P.alpha + p.w_old[a] * (1.0 - P.alpha);
+        p.w_pos[a] += p.w_avg[a];
+    }
+}
+
+// Sphere force/torque partials added in a fixed order, velocity and rotation
+// update; after the last forcing iteration also the particle movement
+// (gpuParticleMovement ibm.cu:899-993) and the step clock.
+__global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int split, int last, int* count) {
     for (int i = threadIdx.x; i < P.np; i += blockDim.x) {
         DPart& p = parts[i];
         double t[6] = {0, 0, 0, 0, 0, 0};
@@ -624,49 +659,14 @@ __global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int
             for (int a = 0; a < 6; ++a) t[a] += fpart[((size_t)i * split + b) * 6 + a];
         for (int a = 0; a < 3; ++a) { p.f[a] += t[a]; p.M[a] += t[3 + a]; }
         update_center(P, p);
+        if (last) move_particle(P, p);
     }
-}
-
-// gpuEulerSumIBMAuxsReset restricted to the touched nodes
-__global__ void k_ibm_euler(IbmParams P, float* fields, unsigned long long* faux, float* fibm, uint8_t* cls,
-                            const int* list, const int* count) {
-    const int cnt = *count;
-    const size_t N = (size_t)P.nx * P.ny * P.nz;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
-        const int n = list[k];
-        const float rho = fields[n];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float v = from_fix(faux[a * N + n]);
-            fields[(1 + a) * N + n] += 0.5f * v / rho;
-            fibm[a * N + n] += v;
-            faux[a * N + n] = 0ull;
-        }
-        cls[n] = cls[n] | NODE_IBM_FORCE;
-    }
-}
-
-// gpuParticleMovement ibm.cu:899-993
-__global__ void k_ibm_move(IbmParams P, DPart* parts, int* steps_taken) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) *steps_taken += 1;   // read by the next step's contacts
-    const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
-    for (int i = threadIdx.x; i < P.np; i += blockDim.x) {
-        DPart& p = parts[i];
-        if (!p.movable) continue;
-        for (int a = 0; a < 3; ++a) {
-            const double dx = p.vel[a] * P.alpha + p.vel_old[a] * (1.0 - P.alpha);
-            if (P.wall[a]) p.pos[a] += dx;
-            else p.pos[a] = fmod(p.pos[a] + dx + L[a], L[a]);
-            p.w_avg[a] = p.w[a] * P.alpha + p.w_old[a] * (1.0 - P.alpha);
-            p.w_pos[a] += p.w_avg[a];
-        }
-    }
+    if (last && threadIdx.x == 0) count[1] += 1;   // read by the next step's contacts
 }
 
 // gpuParticleNodeMovement ibm.cu:1044-1197
-__global__ void k_ibm_move_nodes(IbmParams P, const DPart* parts, const int* pid, double* X, double* Y, double* Z) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.nnodes) return;
+__device__ void move_node(const IbmParams& P, const DPart* parts, const int* pid, double* X, double* Y, double* Z,
+                          int k) {
     const DPart& p = parts[pid[k]];
     if (!p.movable) return;
     const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
@@ -697,6 +697,34 @@ __global__ void k_ibm_move_nodes(IbmParams P, const DPart* parts, const int* pid
     np3[2] = p.pos[2] + 2 * ((qi * qj - q0 * qj) * v[0] + (qj * qk + q0 * qi) * v[1] + (t + qk * qk) * v[2]);
     for (int a = 0; a < 3; ++a) *Pp[a] = P.wall[a] ? np3[a] : fmod(np3[a] + L[a], L[a]);
 }
+
+// Over the touched-node list: u += fAux/(2 rho), F += fAux, fAux = 0
+// (gpuEulerSumIBMAuxsReset restricted to the touched nodes); after the last
+// forcing iteration the same launch moves the Lagrangian nodes
+// (gpuParticleNodeMovement ibm.cu:1044-1197), which k_ibm_update's particle
+// movement precedes.
+__global__ void k_ibm_euler(IbmParams P, float* fields, unsigned long long* faux, float* fibm, uint8_t* cls,
+                            const int* list, const int* count, const DPart* parts, const int* pid, double* X,
+                            double* Y, double* Z, int move_nodes) {
+    const int cnt = *count;
+    const size_t N = (size_t)P.nx * P.ny * P.nz;
+    if (move_nodes)
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P.nnodes; k += gridDim.x * blockDim.x)
+            move_node(P, parts, pid, X, Y, Z, k);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const int n = list[k];
+        const float rho = fields[n];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float v = from_fix(faux[a * N + n]);
+            fields[(1 + a) * N + n] += 0.5f * v / rho;
+            fibm[a * N + n] += v;
+            faux[a * N + n] = 0ull;
+        }
+        cls[n] = cls[n] | NODE_IBM_FORCE;
+    }
+}
+
 
 __global__ void k_ibm_fixup(const float* fields, long long N, const int* list, const int* count, float* rho, float* ux,
                             float* uy, float* uz) {
@@ -785,32 +813,33 @@ vlbm_status ibm_step(vlbm_sim* s) {
     if (!st || st->np == 0) return VLBM_OK;
     const IbmParams& P = st->prm;
     cudaStream_t cs = s->stream;
-    IBM_CUDA(cudaMemsetAsync(st->count, 0, sizeof(int), cs));
-    k_ibm_box<<<st->np, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nfx, st->nfy, st->nfz, st->ndx,
-                                              st->ndy, st->ndz);
+    k_ibm_begin<<<st->np + 1, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nfx, st->nfy, st->nfz,
+                                                     st->ndx, st->ndy, st->ndz, st->contrib, st->count);
     IBM_CUDA(cudaGetLastError());
     IBM_CUDA(gather_dispatch(s, st));
-    k_ibm_contacts<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->contrib, st->count + 1);
-    IBM_CUDA(cudaGetLastError());
-    // grid-stride over the touched-node list: enough blocks for the boxes of
-    // all spheres, at most one per 256 lattice nodes
-    const int euler_blocks = (int)std::min<long long>((s->N + 255) / 256, std::max<long long>(1, st->euler_blocks));
-    for (int it = 0; it < st->cfg.max_iterations; ++it) {
+    // grid-stride over the touched-node list (and the Lagrangian nodes in the
+    // last iteration): enough blocks for the boxes of all spheres, at most one
+    // per 256 lattice nodes
+    const int euler_blocks = (int)std::min<long long>(
+        (s->N + 255) / 256, std::max<long long>(std::max<long long>(1, st->euler_blocks), (st->nnodes + 255) / 256));
+    const int iters = std::max(1, st->cfg.max_iterations);
+    for (int it = 0; it < iters; ++it) {
+        const int last = it == iters - 1;
         k_ibm_interp_spread<<<st->np * st->split, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nS,
                                                                          st->nfx, st->nfy, st->nfz, st->ndx, st->ndy,
                                                                          st->ndz, st->fields, st->faux, st->fpart,
                                                                          st->split);
         IBM_CUDA(cudaGetLastError());
-        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->fpart, st->split);
+        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->fpart, st->split, last, st->count);
         IBM_CUDA(cudaGetLastError());
-        k_ibm_euler<<<euler_blocks, 256, 0, cs>>>(P, st->fields, st->faux, s->fibm, s->cls, st->list, st->count);
+        k_ibm_euler<<<euler_blocks, 256, 0, cs>>>(P, st->fields, st->faux, s->fibm, s->cls, st->list, st->count,
+                                                  st->parts, st->npid, st->nx, st->ny, st->nz, last);
         IBM_CUDA(cudaGetLastError());
     }
-    k_ibm_move<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->count + 1);
-    k_ibm_move_nodes<<<(st->nnodes + 255) / 256, 256, 0, cs>>>(P, st->parts, st->npid, st->nx, st->ny, st->nz);
-    IBM_CUDA(cudaGetLastError());
     return VLBM_OK;
 }
+
+int ibm_iterations(const vlbm_sim* s) { return s->ibm ? s->ibm->cfg.max_iterations : 0; }
 
 void ibm_counts(const vlbm_sim* s, int* np, int* nn) {
     *np = s->ibm ? s->ibm->np : 0;

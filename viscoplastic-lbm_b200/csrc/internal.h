@@ -67,15 +67,18 @@ struct MacroParams {
 };
 
 // Host-side analysis of a reference node map.
+// Boundary slots in increasing node order: every listed node has class
+// NODE_BC and slot index = its position; all other nodes are bulk.
 struct BcTables {
-    std::vector<uint8_t> cls;        // [N]
-    std::vector<int32_t> slot;       // [N] (-1 for bulk)
     std::vector<BcRec> recs;         // [nbc]
     std::vector<int32_t> bc_nodes;   // [nbc] node index of each slot
 };
 
 vlbm_status build_bc_tables(const vlbm_config& cfg, const uint32_t* map, size_t n, BcTables& out,
                             std::string& err);
+// The same tables for a named builder, without a node map (faces only).
+vlbm_status build_bc_tables_builder(const vlbm_config& cfg, int builder, BcTables& out, std::string& err);
+bool builder_word(int builder, int x, int y, int z, int nx, int ny, int nz, uint32_t& w);
 
 // Role of population i at a bounce-back node with direction dir:
 // 0 known, 1 replaced, 2 kept with its streamed value ("dead" population).

@@ -13,8 +13,9 @@
 //    k_batch_advance.  A sphere-free lattice that fills a wave of that kernel
 //    by itself gets its own k_step launch.  Each lattice with spheres runs its
 //    fluid and IBM launches on its own side stream (a graph branch that
-//    overlaps the others).  One step and eight steps are captured in CUDA
-//    graphs per phase (steps since the tables were built, mod 2) and replayed
+//    overlaps the others).  A membership's first segment runs with direct
+//    launches; once it has lasted a segment, one step is captured in a CUDA
+//    graph per phase (steps since the tables were built, mod 2) and replayed
 //    until the membership changes;
 //  * pump() enqueues the steps in segments of at most kSegment steps and does
 //    its host work (admission of queued requests, table rebuilds, graph
@@ -29,6 +30,7 @@
 #include <chrono>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <string>
 #include <unordered_map>
@@ -39,17 +41,17 @@
 namespace vlbm {
 
 // After every lattice of the batch took its step.
-__global__ void k_batch_advance(BatchSlot* slots, int nslots) {
+__global__ void k_batch_advance(BatchState* state, int nslots) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nslots) return;
-    slots[i].parity ^= 1;
-    slots[i].side_cur ^= 1;
-    slots[i].apply_bc = 1;
+    state[i].parity ^= 1;
+    state[i].side_cur ^= 1;
+    state[i].apply_bc = 1;
 }
 
-cudaError_t launch_batch_advance(BatchSlot* slots, int nslots, cudaStream_t s) {
+cudaError_t launch_batch_advance(BatchState* state, int nslots, cudaStream_t s) {
     if (nslots <= 0) return cudaSuccess;
-    k_batch_advance<<<(nslots + 127) / 128, 128, 0, s>>>(slots, nslots);
+    k_batch_advance<<<(nslots + 127) / 128, 128, 0, s>>>(state, nslots);
     return cudaGetLastError();
 }
 
@@ -59,7 +61,6 @@ using namespace vlbm;
 
 namespace {
 
-constexpr int kGraphSteps = 8;        // steps per replay of the long graph (even: keeps the phase)
 constexpr int kSegment = 64;          // steps enqueued between two host bookkeeping points
 constexpr int kSegmentsInFlight = 8;  // the host waits when more segments are queued
 constexpr size_t kKeptResults = 256;  // finished fields kept for vlbm_server_fetch
@@ -100,14 +101,19 @@ size_t estimate_bytes(const vlbm_request& r) {
     return b;
 }
 
-// The lattices of one kernel family, split by their AA parity when the tables
-// were built: part b holds the lattices whose parity was b, which at phase ph
-// (steps since the rebuild, mod 2) step with parity b ^ ph.
+// The lattices of one kernel family that share the batched launches, in
+// chunks of at most BATCH_MAX_SLOTS lattices of equal AA parity at the time
+// the tables were built: a chunk of part b steps with parity b ^ ph at phase
+// ph (steps since the rebuild, mod 2).
+struct Chunk {
+    int part;
+    BatchLaunch L;        // the chunk's lattice parameters (launch arguments)
+    size_t table_off;
+    int ntiles, grid;
+};
 struct Group {
     int Q, op, rheo, st;
-    size_t off[2];
-    int ntiles[2];
-    int grid[2];
+    std::vector<Chunk> chunks;
 };
 
 // Device memory cache of the server.  Buffers released by retired lattices are
@@ -212,23 +218,42 @@ struct vlbm_server {
     std::deque<std::pair<uint64_t, std::vector<float>>> results;   // finished ux fields, by tag
     size_t bytes_in_use = 0;
     double lattice_updates = 0.0;
-    double prof[5] = {0, 0, 0, 0, 0};   // admit, rebuild+capture, enqueue, wait, read-out
+    // admit, rebuild, enqueue (incl. graph captures), wait, read-out [s];
+    // batch steps, direct kernel launches, graph launches, graph captures
+    double prof[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // batch tables (rebuilt when the membership changes)
     bool dirty = true;
-    BatchSlot* d_slots = nullptr;
+    BatchState* d_state = nullptr;
     BatchBlock* d_table = nullptr;
     size_t cap_slots = 0, cap_table = 0;
     std::vector<void*> old_tables;      // outgrown table buffers, freed with the server
-    BatchSlot* h_slots = nullptr;       // pinned staging of the tables
-    BatchBlock* h_table = nullptr;
-    cudaEvent_t upload_done = nullptr;  // staging may be rewritten once this completed
+    // pinned staging of the tables: a ring, so a rebuild does not wait for the
+    // GPU to reach the previous upload (an entry is reused once its upload ran)
+    struct Staging {
+        BatchState* slots = nullptr;
+        BatchBlock* table = nullptr;
+        size_t cap_slots = 0, cap_table = 0;
+        cudaEvent_t uploaded = nullptr;
+        bool pending = false;
+    };
+    Staging staging[4];
+    int next_staging = 0;
+    std::vector<void*> old_pinned;      // outgrown staging, freed with the server
+    int stable_segments = 0;            // segments run since the last rebuild
+    bool use_graphs = false;            // the batch's GPU step is short next to its launch cost
+    long long own_launch_min_nodes = -1;  // -1: one wave of the batched kernel
+    double last_launches = 0.0;         // kernel launches of the last enqueue_steps
+    double capture_s = 0.0;             // host seconds in graph captures (part of enqueue)
     std::vector<Group> groups;
     int nslots = 0;
     int phase = 0;                 // steps since the last rebuild, mod 2
-    std::vector<int> ibm_res;      // indices into res of lattices with spheres (side streams)
-    std::vector<int> own_res;      // indices into res of large sphere-free lattices (own launches)
-    // per phase: graphs of one step and of kGraphSteps steps
-    cudaGraphExec_t graph1[2] = {nullptr, nullptr}, graphK[2] = {nullptr, nullptr};
+    std::vector<int> ibm_res;      // indices into res of lattices with spheres
+    std::vector<int> own_res;      // indices into res of large sphere-free lattices
+    std::vector<int> branch_res;   // both of the above: own launches on a side stream each
+    std::vector<int> table_res;    // the lattices of the batched launches
+    // per phase: graph of one step (captured once a membership has lasted a
+    // segment; short captures, because memberships change often)
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr};
     // side streams of the lattices with spheres (graph branches)
     std::vector<cudaStream_t> side_streams;
     std::vector<cudaEvent_t> join_events;
@@ -237,8 +262,7 @@ struct vlbm_server {
     void drop_graphs() {
         for (int p = 0; p < 2; ++p) {
             if (graph1[p]) cudaGraphExecDestroy(graph1[p]);
-            if (graphK[p]) cudaGraphExecDestroy(graphK[p]);
-            graph1[p] = graphK[p] = nullptr;
+            graph1[p] = nullptr;
         }
     }
     ~vlbm_server() {
@@ -251,12 +275,15 @@ struct vlbm_server {
         }
         for (cudaEvent_t e : segments) cudaEventDestroy(e);
         drop_graphs();
-        cudaFree(d_slots);
+        cudaFree(d_state);
         cudaFree(d_table);
         for (void* p : old_tables) cudaFree(p);
-        if (h_slots) cudaFreeHost(h_slots);
-        if (h_table) cudaFreeHost(h_table);
-        if (upload_done) cudaEventDestroy(upload_done);
+        for (Staging& g : staging) {
+            if (g.slots) cudaFreeHost(g.slots);
+            if (g.table) cudaFreeHost(g.table);
+            if (g.uploaded) cudaEventDestroy(g.uploaded);
+        }
+        for (void* p : old_pinned) cudaFreeHost(p);
         for (cudaStream_t t : side_streams) cudaStreamDestroy(t);
         for (cudaEvent_t e : join_events) cudaEventDestroy(e);
         if (fork_event) cudaEventDestroy(fork_event);
@@ -270,8 +297,10 @@ vlbm_status server_rebuild(vlbm_server* sv) {
     sv->drop_graphs();
     sv->groups.clear();
     sv->ibm_res.clear();
+    sv->table_res.clear();
+    sv->branch_res.clear();
     sv->phase = 0;
-    std::vector<BatchSlot> slots;
+    std::vector<BatchState> slots;
     std::vector<BatchBlock> table;
     auto key = [](const vlbm_sim* s) {
         const vlbm_config& c = s->cfg;
@@ -285,45 +314,86 @@ vlbm_status server_rebuild(vlbm_server* sv) {
     });
     int cur = -1;
     sv->own_res.clear();
+    // Lattices with spheres step on their own side stream (fluid and IBM
+    // launches).  A sphere-free lattice that fills a wave of the batched kernel
+    // by itself may get its own k_step launch (parameters in the constant bank,
+    // about 30 % faster per node than the batched kernel) on a side stream,
+    // largest first, while the host time of all launches of a step stays below
+    // about 60 % of the GPU time of the step; the rest share the batched
+    // launches.  Estimates: 4 us of host time per launch, populations
+    // streamed at 4.5 TB/s.
+    std::vector<char> own(sv->res.size(), 0);
+    {
+        double gpu_us = 0.0, host_us = 4.0;   // the state-advance launch
+        std::vector<std::pair<long long, int>> cand;
+        for (size_t i = 0; i < sv->res.size(); ++i) {
+            const vlbm_sim* s = sv->res[i].sim;
+            gpu_us += 2.0 * s->Q * s->store_bytes * (double)s->N / 4.5e6;
+            if (s->ibm) { host_us += 4.0 * (3.0 + 3.0 * std::max(1, ibm_iterations(s))); continue; }
+            const long long wave = sv->own_launch_min_nodes >= 0
+                                       ? sv->own_launch_min_nodes
+                                       : (long long)std::max(1, batched_blocks_per_sm(s->Q, s->cfg.storage,
+                                                                                      s->cfg.collision,
+                                                                                      s->cfg.rheology)) *
+                                             sv->sms * 256;
+            if (s->N >= wave) cand.emplace_back(s->N, (int)i);
+            else host_us += 0.5;   // its share of the batched launches
+        }
+        std::sort(cand.begin(), cand.end(), std::greater<std::pair<long long, int>>());
+        for (const auto& c : cand) {
+            if (sv->own_launch_min_nodes >= 0 || host_us + 4.0 <= 0.6 * gpu_us) {
+                own[c.second] = 1;
+                host_us += 4.0;
+            }
+        }
+    }
     for (int idx : order) {
         vlbm_sim* s = sv->res[idx].sim;
-        // Lattices with spheres step on their own side stream (fluid and IBM
-        // launches); sphere-free lattices that fill a wave of the batched
-        // kernel by themselves get their own k_step launch (parameters in the
-        // constant bank, one node per thread); the rest share the table.
         if (s->ibm) { sv->ibm_res.push_back(idx); continue; }
-        const long long wave = (long long)std::max(1, batched_blocks_per_sm(s->Q, s->cfg.storage, s->cfg.collision,
-                                                                            s->cfg.rheology)) * sv->sms * BATCH_TILE;
-        if (s->N >= wave) { sv->own_res.push_back(idx); continue; }
+        if (own[idx]) { sv->own_res.push_back(idx); continue; }
+        sv->table_res.push_back(idx);
         const int k = key(s);
         if (k != cur) {
-            Group g{s->Q, s->cfg.collision, s->cfg.rheology, s->cfg.storage, {table.size(), table.size()}, {0, 0}, {0, 0}};
-            sv->groups.push_back(g);
+            sv->groups.push_back(Group{s->Q, s->cfg.collision, s->cfg.rheology, s->cfg.storage, {}});
             cur = k;
         }
         Group& g = sv->groups.back();
         const int part = s->parity;
-        if (part == 1 && g.ntiles[1] == 0) g.off[1] = table.size();
-        BatchSlot bs;
+        if (g.chunks.empty() || g.chunks.back().part != part ||
+            (int)(slots.size() - g.chunks.back().L.state_base) >= BATCH_MAX_SLOTS) {
+            g.chunks.emplace_back();
+            Chunk& c = g.chunks.back();
+            std::memset(&c.L, 0, sizeof(c.L));
+            c.part = part;
+            c.L.state_base = (int)slots.size();
+            c.table_off = table.size();
+            c.ntiles = 0;
+            c.grid = 0;
+        }
+        Chunk& c = g.chunks.back();
+        const int local = (int)slots.size() - c.L.state_base;
+        StepParams pp = make_params(s);
+        pp.side_prev = s->side[0];     // the kernel picks the current one from the state
+        pp.side_next = s->side[1];
+        c.L.p[local] = pp;
+        BatchState bs;
         std::memset(&bs, 0, sizeof(bs));
-        bs.p = make_params(s);
-        bs.side[0] = s->side[0];
-        bs.side[1] = s->side[1];
         bs.parity = s->parity;
         bs.side_cur = s->side_cur;
         bs.apply_bc = s->apply_bc;
-        const int slot = (int)slots.size();
         slots.push_back(bs);
         const unsigned nt = (unsigned)((s->N + BATCH_TILE - 1) / BATCH_TILE);
-        for (unsigned t = 0; t < nt; ++t) table.push_back(BatchBlock{slot, t * (unsigned)BATCH_TILE});
-        g.ntiles[part] += (int)nt;
+        for (unsigned t = 0; t < nt; ++t) table.push_back(BatchBlock{local, t * (unsigned)BATCH_TILE});
+        c.ntiles += (int)nt;
     }
     for (Group& g : sv->groups) {
         const int per_sm = std::max(1, batched_blocks_per_sm(g.Q, g.st, g.op, g.rheo));
-        for (int b = 0; b < 2; ++b) g.grid[b] = std::min(g.ntiles[b], per_sm * sv->sms);
+        for (Chunk& c : g.chunks) c.grid = std::min(c.ntiles, per_sm * sv->sms);
     }
-    // one side stream and join event per lattice with spheres
-    while (sv->side_streams.size() < sv->ibm_res.size()) {
+    sv->branch_res = sv->ibm_res;
+    sv->branch_res.insert(sv->branch_res.end(), sv->own_res.begin(), sv->own_res.end());
+    // one side stream and join event per lattice with its own launches
+    while (sv->side_streams.size() < sv->branch_res.size()) {
         cudaStream_t t = nullptr;
         cudaEvent_t ev = nullptr;
         cudaError_t e = cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking);
@@ -340,59 +410,85 @@ vlbm_status server_rebuild(vlbm_server* sv) {
         if (e != cudaSuccess) { sv->fork_event = nullptr; return cuda_status(e, "server fork event"); }
     }
     sv->nslots = (int)slots.size();
-    // Grow the device tables and their pinned staging without cudaFree or
-    // cudaFreeHost (both synchronise the device): outgrown device buffers are
-    // kept until the server is destroyed, staging is replaced after the last
-    // upload from it completed.
-    if (sv->upload_done) {
-        cudaError_t e = cudaEventSynchronize(sv->upload_done);
-        if (e != cudaSuccess) return cuda_status(e, "server table upload");
-    }
+    // Grow the device tables without cudaFree (it synchronises the device):
+    // outgrown buffers are kept until the server is destroyed.  The device
+    // tables are rewritten in place: the upload is ordered after the queued
+    // steps that still read them.
     if (slots.size() > sv->cap_slots) {
         const size_t cap = std::max<size_t>(256, slots.size() * 2);
         void* d = nullptr;
-        void* h = nullptr;
-        if (cudaMalloc(&d, cap * sizeof(BatchSlot)) != cudaSuccess ||
-            cudaHostAlloc(&h, cap * sizeof(BatchSlot), cudaHostAllocDefault) != cudaSuccess) {
+        if (cudaMalloc(&d, cap * sizeof(BatchState)) != cudaSuccess) {
             cudaGetLastError();
-            if (d) cudaFree(d);
             set_last_error("server slot table allocation failed");
             return VLBM_ERR_NOMEM;
         }
-        if (sv->d_slots) sv->old_tables.push_back(sv->d_slots);
-        if (sv->h_slots) cudaFreeHost(sv->h_slots);
-        sv->d_slots = static_cast<BatchSlot*>(d);
-        sv->h_slots = static_cast<BatchSlot*>(h);
+        if (sv->d_state) sv->old_tables.push_back(sv->d_state);
+        sv->d_state = static_cast<BatchState*>(d);
         sv->cap_slots = cap;
     }
     if (table.size() > sv->cap_table) {
         const size_t cap = std::max<size_t>(1 << 16, table.size() * 2);
         void* d = nullptr;
-        void* h = nullptr;
-        if (cudaMalloc(&d, cap * sizeof(BatchBlock)) != cudaSuccess ||
-            cudaHostAlloc(&h, cap * sizeof(BatchBlock), cudaHostAllocDefault) != cudaSuccess) {
+        if (cudaMalloc(&d, cap * sizeof(BatchBlock)) != cudaSuccess) {
             cudaGetLastError();
-            if (d) cudaFree(d);
             set_last_error("server tile table allocation failed");
             return VLBM_ERR_NOMEM;
         }
         if (sv->d_table) sv->old_tables.push_back(sv->d_table);
-        if (sv->h_table) cudaFreeHost(sv->h_table);
         sv->d_table = static_cast<BatchBlock*>(d);
-        sv->h_table = static_cast<BatchBlock*>(h);
         sv->cap_table = cap;
     }
     if (!slots.empty()) {
-        std::memcpy(sv->h_slots, slots.data(), slots.size() * sizeof(BatchSlot));
-        std::memcpy(sv->h_table, table.data(), table.size() * sizeof(BatchBlock));
-        cudaError_t e = cudaMemcpyAsync(sv->d_slots, sv->h_slots, slots.size() * sizeof(BatchSlot),
-                                        cudaMemcpyHostToDevice, sv->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(sv->d_table, sv->h_table, table.size() * sizeof(BatchBlock), cudaMemcpyHostToDevice,
+        vlbm_server::Staging& g = sv->staging[sv->next_staging];
+        sv->next_staging = (sv->next_staging + 1) % 4;
+        cudaError_t e = cudaSuccess;
+        if (g.pending) e = cudaEventSynchronize(g.uploaded);   // normally long complete
+        g.pending = false;
+        if (e == cudaSuccess && slots.size() > g.cap_slots) {
+            void* h = nullptr;
+            e = cudaHostAlloc(&h, sv->cap_slots * sizeof(BatchState), cudaHostAllocDefault);
+            if (e == cudaSuccess) {
+                if (g.slots) sv->old_pinned.push_back(g.slots);
+                g.slots = static_cast<BatchState*>(h);
+                g.cap_slots = sv->cap_slots;
+            }
+        }
+        if (e == cudaSuccess && table.size() > g.cap_table) {
+            void* h = nullptr;
+            e = cudaHostAlloc(&h, sv->cap_table * sizeof(BatchBlock), cudaHostAllocDefault);
+            if (e == cudaSuccess) {
+                if (g.table) sv->old_pinned.push_back(g.table);
+                g.table = static_cast<BatchBlock*>(h);
+                g.cap_table = sv->cap_table;
+            }
+        }
+        if (e == cudaSuccess && !g.uploaded) e = cudaEventCreateWithFlags(&g.uploaded, cudaEventDisableTiming);
+        if (e == cudaSuccess) {
+            std::memcpy(g.slots, slots.data(), slots.size() * sizeof(BatchState));
+            std::memcpy(g.table, table.data(), table.size() * sizeof(BatchBlock));
+            e = cudaMemcpyAsync(sv->d_state, g.slots, slots.size() * sizeof(BatchState), cudaMemcpyHostToDevice,
                                 sv->stream);
-        if (e == cudaSuccess && !sv->upload_done) e = cudaEventCreateWithFlags(&sv->upload_done, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventRecord(sv->upload_done, sv->stream);
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(sv->d_table, g.table, table.size() * sizeof(BatchBlock), cudaMemcpyHostToDevice,
+                                sv->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(g.uploaded, sv->stream);
         if (e != cudaSuccess) return cuda_status(e, "server table upload");
+        g.pending = true;
+    }
+    sv->stable_segments = 0;
+    {   // graphs pay off where host launch time is comparable to the GPU step:
+        // estimate both (about 4 us of host time per launch; the populations
+        // streamed at about 4 TB/s, which the large lattices reach)
+        double launches = 1.0 + (double)sv->own_res.size();
+        for (const Group& g : sv->groups) launches += (double)g.chunks.size();
+        double bytes = 0.0;
+        for (const Resident& r : sv->res) {
+            bytes += 2.0 * r.sim->Q * r.sim->store_bytes * (double)r.sim->N;
+            if (r.sim->ibm) launches += 3.0 + 3.0 * std::max(1, ibm_iterations(r.sim));
+        }
+        const double host_us = 4.0 * launches, gpu_us = bytes / 4.0e6;
+        sv->use_graphs = gpu_us < 3.0 * host_us;
     }
     sv->dirty = false;
     return VLBM_OK;
@@ -415,49 +511,50 @@ void advance_host(vlbm_sim* s) {
 // other and the batched work.  Advances the host mirrors and the phase.
 vlbm_status enqueue_steps(vlbm_server* sv, int n) {
     cudaError_t e = cudaSuccess;
-    if (!sv->ibm_res.empty()) {
+    if (!sv->branch_res.empty()) {
         e = cudaEventRecord(sv->fork_event, sv->stream);
         if (e != cudaSuccess) return cuda_status(e, "fork event");
     }
+    double launches = 0.0;
     for (int i = 0; i < n; ++i) {
         for (const Group& g : sv->groups)
-            for (int b = 0; b < 2; ++b) {
-                const bool odd = (b ^ sv->phase) != 0;
-                e = launch_batched(g.Q, g.st, sv->d_slots, sv->d_table + g.off[b], g.ntiles[b], g.grid[b], odd, g.op,
+            for (const Chunk& c : g.chunks) {
+                const bool odd = (c.part ^ sv->phase) != 0;
+                e = launch_batched(g.Q, g.st, c.L, sv->d_state, sv->d_table + c.table_off, c.ntiles, c.grid, odd, g.op,
                                    g.rheo, sv->stream);
                 if (e != cudaSuccess) return cuda_status(e, "batched step");
+                launches += 1.0;
             }
-        e = launch_batch_advance(sv->d_slots, sv->nslots, sv->stream);
-        if (e != cudaSuccess) return cuda_status(e, "batch advance");
-        sv->phase ^= 1;
-        for (int idx : sv->own_res) {
-            vlbm_status st = fluid_step(sv->res[idx].sim);   // advances the mirror
-            if (st != VLBM_OK) return st;
+        if (sv->nslots > 0) {
+            e = launch_batch_advance(sv->d_state, sv->nslots, sv->stream);
+            if (e != cudaSuccess) return cuda_status(e, "batch advance");
+            launches += 1.0;
         }
+        sv->phase ^= 1;
     }
-    for (size_t r = 0; r < sv->res.size(); ++r) {
-        vlbm_sim* s = sv->res[r].sim;
-        if (s->ibm) continue;
-        if (std::find(sv->own_res.begin(), sv->own_res.end(), (int)r) != sv->own_res.end()) continue;
-        for (int i = 0; i < n; ++i) advance_host(s);
-    }
-    for (size_t j = 0; j < sv->ibm_res.size(); ++j) {
-        vlbm_sim* s = sv->res[sv->ibm_res[j]].sim;
+    for (int idx : sv->table_res)
+        for (int i = 0; i < n; ++i) advance_host(sv->res[idx].sim);
+    // lattices with their own launches: one side stream each, forked from the
+    // server stream before the first step and joined after the last
+    for (size_t j = 0; j < sv->branch_res.size(); ++j) {
+        vlbm_sim* s = sv->res[sv->branch_res[j]].sim;
         cudaStream_t side = sv->side_streams[j];
         e = cudaStreamWaitEvent(side, sv->fork_event, 0);
         if (e != cudaSuccess) return cuda_status(e, "fork wait");
         s->stream = side;
         vlbm_status st = VLBM_OK;
         for (int i = 0; i < n && st == VLBM_OK; ++i) {
-            st = fluid_step(s);
-            if (st == VLBM_OK) st = ibm_step(s);
+            st = fluid_step(s);   // advances the mirror
+            if (st == VLBM_OK && s->ibm) st = ibm_step(s);
         }
+        launches += (double)n * (1.0 + (s->ibm ? 2.0 + 3.0 * std::max(1, ibm_iterations(s)) : 0.0));
         s->stream = sv->stream;
         if (st != VLBM_OK) return st;
         e = cudaEventRecord(sv->join_events[j], side);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(sv->stream, sv->join_events[j], 0);
         if (e != cudaSuccess) return cuda_status(e, "join");
     }
+    sv->last_launches = launches;
     return VLBM_OK;
 }
 
@@ -466,6 +563,7 @@ struct HostState { int parity, side_cur, apply_bc; long long step; };
 // Capture `steps` steps starting at the current phase; host mirrors and
 // phase are left as they were (the replay advances them).
 vlbm_status capture(vlbm_server* sv, int steps, cudaGraphExec_t* out) {
+    const double t_start = now_s();
     std::vector<HostState> saved;
     for (const Resident& r : sv->res) saved.push_back({r.sim->parity, r.sim->side_cur, r.sim->apply_bc, r.sim->step});
     const int phase = sv->phase;
@@ -474,6 +572,7 @@ vlbm_status capture(vlbm_server* sv, int steps, cudaGraphExec_t* out) {
     if (e != cudaSuccess) return cuda_status(e, "begin capture");
     vlbm_status st = enqueue_steps(sv, steps);
     e = cudaStreamEndCapture(sv->stream, &g);
+    sv->prof[8] += 1.0;
     for (size_t i = 0; i < sv->res.size(); ++i) {
         vlbm_sim* s = sv->res[i].sim;
         s->parity = saved[i].parity; s->side_cur = saved[i].side_cur;
@@ -483,6 +582,7 @@ vlbm_status capture(vlbm_server* sv, int steps, cudaGraphExec_t* out) {
     if (st != VLBM_OK) { if (g) cudaGraphDestroy(g); return st; }
     if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
     if (g) cudaGraphDestroy(g);
+    sv->capture_s += now_s() - t_start;
     return cuda_status(e, "server step graph");
 }
 
@@ -493,6 +593,7 @@ vlbm_status replay(vlbm_server* sv, cudaGraphExec_t* slot, int steps) {
     }
     cudaError_t e = cudaGraphLaunch(*slot, sv->stream);
     if (e != cudaSuccess) return cuda_status(e, "cudaGraphLaunch");
+    sv->prof[7] += 1.0;
     for (Resident& r : sv->res)
         for (int i = 0; i < steps; ++i) advance_host(r.sim);
     sv->phase ^= steps & 1;
@@ -507,21 +608,25 @@ vlbm_status server_steps(vlbm_server* sv, uint64_t k) {
         // Lattices with their own launches take the boundary flag from the
         // host mirror: their first step (no boundary rule yet) runs outside
         // the graphs, whose steps all apply the rule.
-        bool direct = false;
-        for (int idx : sv->ibm_res) direct |= sv->res[idx].sim->apply_bc == 0;
-        for (int idx : sv->own_res) direct |= sv->res[idx].sim->apply_bc == 0;
-        if (direct) {
+        bool first = false;
+        for (int idx : sv->branch_res) first |= sv->res[idx].sim->apply_bc == 0;
+        if (first) {
             st = enqueue_steps(sv, 1);
+            sv->prof[6] += sv->last_launches;
             left -= 1;
-        } else if (left >= (uint64_t)kGraphSteps) {
-            st = replay(sv, &sv->graphK[sv->phase], kGraphSteps);
-            left -= kGraphSteps;
+        } else if (!sv->use_graphs || sv->stable_segments == 0) {
+            // direct launches: for a fresh membership (capturing pays off only
+            // if it lasts) and for batches whose GPU step hides the launches
+            st = enqueue_steps(sv, (int)left);
+            sv->prof[6] += sv->last_launches;
+            left = 0;
         } else {
             st = replay(sv, &sv->graph1[sv->phase], 1);
             left -= 1;
         }
     }
     for (const Resident& r : sv->res) sv->lattice_updates += (double)r.sim->N * (double)(k - left);
+    sv->prof[5] += (double)(k - left);
     return st;
 }
 
@@ -549,11 +654,7 @@ vlbm_status server_admit(vlbm_server* sv) {
         cfg.layout = VLBM_LAYOUT_NATURAL;   // the batched kernel streams one node per thread
         vlbm_sim* s = nullptr;
         vlbm_status st = sim_create(&cfg, &sv->cache, &s);
-        if (st == VLBM_OK) {
-            std::vector<uint32_t> map((size_t)cfg.nx * cfg.ny * cfg.nz);
-            st = vlbm_build_node_map(p.req.builder, cfg.nx, cfg.ny, cfg.nz, map.data(), map.size());
-            if (st == VLBM_OK) st = vlbm_set_node_map(s, map.data(), map.size());
-        }
+        if (st == VLBM_OK) st = vlbm_set_builder(s, p.req.builder);
         if (st == VLBM_OK && !p.spheres.empty())
             st = vlbm_add_spheres(s, &p.req.ibm, p.spheres.data(), (int32_t)p.spheres.size());
         if (st == VLBM_OK) st = vlbm_set_stream(s, sv->stream);
@@ -756,6 +857,7 @@ vlbm_status vlbm_server_pump(vlbm_server* sv, uint32_t steps, vlbm_completion* o
         t0 = now_s();
         sv->prof[2] += t0 - t1;
         if ((st = end_segment(sv)) != VLBM_OK) break;
+        sv->stable_segments += 1;
         t1 = now_s();
         sv->prof[3] += t1 - t0;
         // host work while the GPU runs the queued segments
@@ -807,7 +909,15 @@ vlbm_status vlbm_server_fetch(vlbm_server* sv, uint64_t tag, float* ux, size_t n
 
 vlbm_status vlbm_server_profile(vlbm_server* sv, double* seconds, int32_t n) {
     if (!sv || (n > 0 && !seconds)) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
-    for (int32_t i = 0; i < n && i < 5; ++i) seconds[i] = sv->prof[i];
+    sv->prof[9] = sv->capture_s;
+    for (int32_t i = 0; i < n && i < 10; ++i) seconds[i] = sv->prof[i];
+    return VLBM_OK;
+}
+
+vlbm_status vlbm_server_set_own_launch_min(vlbm_server* sv, int64_t nodes) {
+    if (!sv) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    sv->own_launch_min_nodes = nodes < 0 ? -1 : nodes;
+    sv->dirty = true;
     return VLBM_OK;
 }
 

@@ -42,6 +42,7 @@ struct vlbm_sim {
     uint8_t* cls = nullptr;          // [N] node class
     int32_t* bc_slot = nullptr;      // [N]
     vlbm::BcRec* bc = nullptr;       // [nbc]
+    int32_t* bc_node = nullptr;      // [nbc] node index of each boundary slot
     float* side[2] = {nullptr, nullptr};  // [Q][nbc] post-collision at boundary nodes
     int nbc = 0;
     int pairH = 0;                   // z-paired layout (NZ/2) or 0
@@ -60,8 +61,6 @@ struct vlbm_sim {
     bool geometry = false;
     int block = 256;                 // launch variant (threads per block)
     int variant = 0;
-    std::vector<uint32_t> host_map;  // last node map (for outputs / servers)
-    vlbm::BcTables tables;
 
     vlbm::IbmState* ibm = nullptr;   // owned; released by ibm_destroy
     vlbm::DeviceAllocator* allocator = nullptr;   // not owned; nullptr: cudaMalloc/cudaFree
@@ -96,5 +95,6 @@ vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy
 void ibm_destroy(IbmState* st, DeviceAllocator* allocator);
 void ibm_reset(vlbm_sim* s);
 void ibm_counts(const vlbm_sim* s, int* np, int* nn);
+int ibm_iterations(const vlbm_sim* s);
 
 }  // namespace vlbm

@@ -230,8 +230,8 @@ __device__ __forceinline__ void zouhe_pres19(float (&f)[19], int dir, float rw) 
 
 // ----------------------------------------------------- boundary at gather --
 template <int Q>
-__device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int slot, int x, int y, int z,
-                                      const Nbr& nb, unsigned n) {
+__device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, const float* __restrict__ side_prev,
+                                      int slot, int x, int y, int z, const Nbr& nb, unsigned n) {
     const BcRec r = p.bc[slot];
     const size_t nbc = (size_t)p.nbc;
     switch (r.scheme) {
@@ -239,7 +239,7 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int
         // bounceBack.cu:26-498: unknown <- own post-collision opposite
 #pragma unroll
         for (int i = 1; i < Q; ++i)
-            if ((r.mask >> i) & 1u) f[i] = p.side_prev[(size_t)lat_opp(i) * nbc + slot];
+            if ((r.mask >> i) & 1u) f[i] = side_prev[(size_t)lat_opp(i) * nbc + slot];
         break;
     case K_BC_VEL_BOUNCE: {
         // D3Q19_VelBounceBack.cu:31-43: rho_w over all streamed populations
@@ -269,7 +269,7 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int
                 const int tx = a == 0 ? 0 : lat_cx(i), ty = a == 1 ? 0 : lat_cy(i), tz = a == 2 ? 0 : lat_cz(i);
                 const unsigned src = n + nb.off(-tx, -ty, -tz);
                 const int sslot = p.bc_slot[src];
-                f[i] = p.side_prev[(size_t)j * nbc + sslot];
+                f[i] = side_prev[(size_t)j * nbc + sslot];
             }
         break;
     case K_BC_VEL_ZOUHE:
@@ -281,6 +281,11 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int
     default: break;
     }
     (void)x; (void)y; (void)z;
+}
+template <int Q>
+__device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int slot, int x, int y, int z,
+                                      const Nbr& nb, unsigned n) {
+    apply_bc<Q>(f, p, p.side_prev, slot, x, y, z, nb, n);
 }
 
 // Storage index of node (x, y, z) in the z-paired layout: nodes z and z+H
@@ -295,8 +300,8 @@ __device__ __forceinline__ int wrap1(int v, int n) { return v < 0 ? v + n : (v >
 // Gather f_i(x, t) of node n (after boundary rules).  Returns the side-store
 // slot of a boundary node, -1 for bulk nodes.
 template <int Q, int ST, bool ODD, bool PAIRED = false>
-__device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr& nb, int x, int y, int z,
-                                      float (&f)[Q], uint8_t& cls) {
+__device__ __forceinline__ int gather(const StepParams& p, const float* side_prev, int use_bc, unsigned n,
+                                      const Nbr& nb, int x, int y, int z, float (&f)[Q], uint8_t& cls) {
     using S = Store<ST>;
     using T = typename S::T;
     const size_t N = (size_t)p.N;
@@ -316,7 +321,7 @@ __device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr
         int slot = -1;
         if (cls & NODE_BC) {
             slot = p.bc_slot[n];
-            if (p.apply_bc) apply_bc<Q>(f, p, slot, x, y, z, nb, n);
+            if (use_bc) apply_bc<Q>(f, p, side_prev, slot, x, y, z, nb, n);
         }
         return slot;
     }
@@ -337,9 +342,14 @@ __device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr
     int slot = -1;
     if (cls & NODE_BC) {
         slot = p.bc_slot[n];
-        if (p.apply_bc) apply_bc<Q>(f, p, slot, x, y, z, nb, n);
+        if (use_bc) apply_bc<Q>(f, p, side_prev, slot, x, y, z, nb, n);
     }
     return slot;
+}
+template <int Q, int ST, bool ODD, bool PAIRED = false>
+__device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr& nb, int x, int y, int z,
+                                      float (&f)[Q], uint8_t& cls) {
+    return gather<Q, ST, ODD, PAIRED>(p, p.side_prev, p.apply_bc, n, nb, x, y, z, f, cls);
 }
 
 // Moments of a node: rho, u (with half force, lbm.cu:79-111), non-equilibrium
@@ -491,8 +501,8 @@ __device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega
 // (lbm.cu:45-58), moments, relaxation (lbm.cu:192-222), collision, and the
 // post-collision copy of boundary nodes (lbm.cu:463-470).
 template <int Q, int OP, int RHEO>
-__device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned n, uint8_t cls, int slot,
-                                                  float (&f)[Q]) {
+__device__ __forceinline__ void relax_and_collide(const StepParams& p, float* side_next, unsigned n, uint8_t cls,
+                                                  int slot, float (&f)[Q]) {
     float fx = p.fx, fy = p.fy, fz = p.fz;
     if (cls & NODE_IBM_FORCE) {
         const size_t N = (size_t)p.N;
@@ -515,8 +525,13 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned 
     if (slot >= 0) {
         const size_t nbc = (size_t)p.nbc;
 #pragma unroll
-        for (int i = 0; i < Q; ++i) p.side_next[(size_t)i * nbc + slot] = f[i];
+        for (int i = 0; i < Q; ++i) side_next[(size_t)i * nbc + slot] = f[i];
     }
+}
+template <int Q, int OP, int RHEO>
+__device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned n, uint8_t cls, int slot,
+                                                  float (&f)[Q]) {
+    relax_and_collide<Q, OP, RHEO>(p, p.side_next, n, cls, slot, f);
 }
 
 // ------------------------------------------------------------ kernels --
@@ -524,7 +539,8 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned 
 // at 4 resident 256-thread blocks per SM (64 registers) keeps enough loads in
 // flight to saturate HBM.
 template <int Q, int OP, int RHEO, int ST, bool ODD>
-__device__ __forceinline__ void step_node(const StepParams& p, unsigned n) {
+__device__ __forceinline__ void step_node(const StepParams& p, const float* side_prev, float* side_next, int use_bc,
+                                          unsigned n) {
     using S = Store<ST>;
     using T = typename S::T;
     const int x = (int)(n % (unsigned)p.nx);
@@ -536,8 +552,8 @@ __device__ __forceinline__ void step_node(const StepParams& p, unsigned n) {
 
     float f[Q];
     uint8_t cls;
-    const int slot = gather<Q, ST, ODD>(p, n, nb, x, y, z, f, cls);
-    relax_and_collide<Q, OP, RHEO>(p, n, cls, slot, f);
+    const int slot = gather<Q, ST, ODD>(p, side_prev, use_bc, n, nb, x, y, z, f, cls);
+    relax_and_collide<Q, OP, RHEO>(p, side_next, n, cls, slot, f);
     nb.launder();
     T* plane = static_cast<T*>(p.pop);
     const size_t N = (size_t)p.N;
@@ -557,53 +573,80 @@ template <int Q, int OP, int RHEO, int ST, bool ODD>
 __global__ void __launch_bounds__(256) k_step(const StepParams p) {
     const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= (unsigned)p.N) return;
-    step_node<Q, OP, RHEO, ST, ODD>(p, n);
+    step_node<Q, OP, RHEO, ST, ODD>(p, p.side_prev, p.side_next, p.apply_bc, n);
 }
 
 // ------------------------------------------------------- batched step --
 // Many lattices of one (velocity set, operator, rheology, storage) group
 // advance in one launch.  The launch walks a table of tiles (lattice slot,
 // first node; BATCH_TILE consecutive nodes each) with a grid-stride loop, so a
-// grid of a few blocks per SM is persistent over all lattices.  Lattices whose
+// grid of a few blocks per SM is persistent over all lattices.  The lattices'
+// parameters are the launch's own arguments (constant bank, no shared-memory
+// copy and no barrier per tile).  Lattices whose
 // AA parity differs go to different tables (the parity is a template argument,
 // as in k_step); the side-store buffer index and the boundary flag of every
 // lattice live in its slot in device memory and are advanced by
 // k_batch_advance after the group launches, so a captured step can be
 // replayed any number of times.
 constexpr int BATCH_TILE = 256;
+constexpr int BATCH_MAX_SLOTS = 64;   // lattices per launch (their parameters are the launch's arguments)
 
-struct BatchSlot {
-    StepParams p;
-    float* side[2];
-    int parity, side_cur, apply_bc, pad;
+// Per-lattice state that changes every step (advanced by k_batch_advance).
+struct BatchState {
+    int side_cur, apply_bc, parity, pad;
 };
 struct BatchBlock {
-    int slot;           // lattice of this tile
+    int slot;           // lattice of this tile: index into the launch's parameters
     unsigned first;     // first node of this tile
 };
+// Arguments of one batched launch: the step parameters of up to
+// BATCH_MAX_SLOTS lattices (side_prev / side_next hold side[0] / side[1]) in
+// the kernel's constant parameter space, read with uniform indices.
+struct BatchLaunch {
+    StepParams p[BATCH_MAX_SLOTS];
+    int state_base;     // index of p[0]'s entry in the state array
+};
+
+// Resident blocks per SM the batched kernel is compiled for: D3Q19 fits five
+// 256-thread blocks (51 registers), D3Q27 four (64 registers).
+template <int Q> constexpr int batch_min_blocks() { return Q == 19 ? 5 : 4; }
 
 template <int Q, int OP, int RHEO, int ST, bool ODD>
-__global__ void __launch_bounds__(256) k_step_batched(const BatchSlot* __restrict__ slots,
-                                                      const BatchBlock* __restrict__ table, int ntiles) {
+__global__ void __launch_bounds__(256, batch_min_blocks<Q>()) k_step_batched(const __grid_constant__ BatchLaunch L,
+                                                                            const BatchState* __restrict__ state,
+                                                                            const BatchBlock* __restrict__ table,
+                                                                            int ntiles) {
     __shared__ StepParams sp;
+    __shared__ float* sides[2];
+    __shared__ int use_bc;
     constexpr int WORDS = (int)(sizeof(StepParams) / 4);
     static_assert(sizeof(StepParams) % 4 == 0, "StepParams is copied as 32-bit words");
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const BatchBlock e = table[t];
-        const BatchSlot* s = slots + e.slot;
-        __syncthreads();   // the previous tile is done with sp
-        if (threadIdx.x < WORDS)
-            reinterpret_cast<unsigned*>(&sp)[threadIdx.x] = reinterpret_cast<const unsigned*>(&s->p)[threadIdx.x];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const int cur = s->side_cur;
-            sp.side_prev = s->side[cur];
-            sp.side_next = s->side[cur ^ 1];
-            sp.apply_bc = s->apply_bc;
+    int t = blockIdx.x;
+    if (t >= ntiles) return;
+    BatchBlock e = table[t];
+    int cur = -1;   // lattice whose parameters are in sp (block-uniform)
+    for (; t < ntiles; t += gridDim.x) {
+        // the next tile's entry is fetched while this one computes
+        const int tn = t + gridDim.x;
+        const BatchBlock en = tn < ntiles ? table[tn] : e;
+        if (e.slot != cur) {   // uniform: every thread holds the same entry
+            __syncthreads();   // the previous lattice's tiles are done with sp
+            if (threadIdx.x < WORDS)
+                reinterpret_cast<unsigned*>(&sp)[threadIdx.x] =
+                    reinterpret_cast<const unsigned*>(&L.p[e.slot])[threadIdx.x];
+            if (threadIdx.x == WORDS) {
+                const BatchState st = state[L.state_base + e.slot];
+                const StepParams& q = L.p[e.slot];
+                sides[0] = st.side_cur ? const_cast<float*>(q.side_next) : const_cast<float*>(q.side_prev);
+                sides[1] = st.side_cur ? const_cast<float*>(q.side_prev) : q.side_next;
+                use_bc = st.apply_bc;
+            }
+            __syncthreads();
+            cur = e.slot;
         }
-        __syncthreads();
         const unsigned n = e.first + threadIdx.x;
-        if (n < (unsigned)sp.N) step_node<Q, OP, RHEO, ST, ODD>(sp, n);
+        if (n < (unsigned)sp.N) step_node<Q, OP, RHEO, ST, ODD>(sp, sides[0], sides[1], use_bc, n);
+        e = en;
     }
 }
 

@@ -171,6 +171,7 @@ _SIGS = {
     "vlbm_create": [C.POINTER(Config), C.POINTER(_P)],
     "vlbm_destroy": [_P],
     "vlbm_set_node_map": [_P, _U32P, C.c_size_t],
+    "vlbm_set_builder": [_P, C.c_int32],
     "vlbm_build_node_map": [C.c_int, C.c_int, C.c_int, C.c_int, _U32P, C.c_size_t],
     "vlbm_init_equilibrium": [_P, C.c_double, C.c_double, C.c_double, C.c_double],
     "vlbm_step": [_P, C.c_uint32],
@@ -195,6 +196,7 @@ _SIGS = {
                           C.POINTER(C.c_int64), C.POINTER(C.c_double)],
     "vlbm_server_fetch": [_P, C.c_uint64, _F32P, C.c_size_t],
     "vlbm_server_profile": [_P, _F64P, C.c_int32],
+    "vlbm_server_set_own_launch_min": [_P, C.c_int64],
     "vlbm_server_destroy": [_P],
     "vlbm_autotune": [_P, C.POINTER(C.c_int32)],
     "vlbm_set_variant": [_P, C.c_int32],
@@ -249,10 +251,11 @@ class Simulation:
         _check(_lib.vlbm_create(C.byref(cfg), C.byref(h)), "vlbm_create")
         self._h = h
         self.n = cfg.nx * cfg.ny * cfg.nz
-        if node_map is None and builder is not None:
-            node_map = build_node_map(builder, cfg.nx, cfg.ny, cfg.nz)
         if node_map is None:
-            node_map = build_node_map(BUILDER_PERIODIC, cfg.nx, cfg.ny, cfg.nz)
+            # named builder: tables straight from the builder's rules on the faces
+            _check(_lib.vlbm_set_builder(self._h, BUILDER_PERIODIC if builder is None else builder),
+                   "vlbm_set_builder")
+            return
         node_map = np.ascontiguousarray(node_map, dtype=np.uint32).ravel()
         _check(_lib.vlbm_set_node_map(self._h, node_map.ctypes.data_as(_U32P), node_map.size),
                "vlbm_set_node_map")
@@ -391,10 +394,15 @@ class Server:
         return {"resident": r.value, "queued": q.value, "bytes": b.value, "lattice_updates": lu.value}
 
     def profile(self):
-        """Host seconds spent in admission, rebuild+capture, enqueue, GPU waits, read-outs."""
-        out = (C.c_double * 5)()
-        _check(_lib.vlbm_server_profile(self._h, out, 5), "vlbm_server_profile")
-        return dict(zip(("admit", "rebuild", "enqueue", "wait", "readout"), list(out)))
+        """Host seconds per phase of the serving loop and launch counters."""
+        out = (C.c_double * 10)()
+        _check(_lib.vlbm_server_profile(self._h, out, 10), "vlbm_server_profile")
+        return dict(zip(("admit_s", "rebuild_s", "enqueue_s", "wait_s", "readout_s", "batch_steps",
+                         "direct_launches", "graph_launches", "graph_captures", "capture_s"), list(out)))
+
+    def set_own_launch_min(self, nodes):
+        """Lattices of at least `nodes` nodes get their own launch (-1: default rule)."""
+        _check(_lib.vlbm_server_set_own_launch_min(self._h, nodes), "vlbm_server_set_own_launch_min")
 
     def fetch(self, tag, n):
         out = np.empty(n, dtype=np.float32)
