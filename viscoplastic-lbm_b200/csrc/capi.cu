@@ -64,6 +64,7 @@ StepParams make_params(vlbm_sim* s) {
     p.nbc = s->nbc;
     p.pairH = s->pairH;
     p.apply_bc = s->apply_bc;
+    p.ctr = s->step_ctr;
     p.omega_newt = (float)(1.0 / c.tau);                 // var.h:105 OMEGA
     p.fx = (float)c.fx; p.fy = (float)c.fy; p.fz = (float)c.fz;
     p.omega_p = (float)(1.0 / (3.0 * c.eta_p + 0.5));    // nnf.h:128 OMEGA_P
@@ -109,14 +110,20 @@ static vlbm_status alloc_dev(vlbm_sim* s, void** p, size_t bytes) {
     return VLBM_OK;
 }
 
-// Side store of the boundary nodes at rest equilibrium: side[b][i][slot] = w_i rho0.
-__global__ void k_fill_side(float* s0, float* s1, int nbc, int Q, float rho0) {
+// Side store of the boundary nodes at rest equilibrium.  It holds
+// post-collision deviations g_i = f_i - w_i rho0, zero at rest.
+__global__ void k_fill_side(float* s0, float* s1, int nbc, int Q) {
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= (long long)Q * nbc) return;
-    const int i = (int)(k / nbc);
-    const float v = (float)(Q == 19 ? Lattice<19>::w(i) : Lattice<27>::w(i)) * rho0;
-    s0[k] = v;
-    s1[k] = v;
+    s0[k] = 0.f;
+    s1[k] = 0.f;
+}
+
+__global__ void k_set_step_ctr(unsigned* ctr, int parity, unsigned step) { ctr[parity & 1] = step; }
+
+cudaError_t sync_step_ctr(vlbm_sim* s, cudaStream_t stream) {
+    k_set_step_ctr<<<1, 1, 0, stream>>>(s->step_ctr, s->parity, (unsigned)s->step);
+    return cudaGetLastError();
 }
 
 // Class bytes and slot indices of the boundary nodes (all others stay bulk).
@@ -131,8 +138,7 @@ __global__ void k_scatter_bc(const int32_t* bc_node, int nbc, uint8_t* cls, int3
 static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
     if (s->nbc == 0) return VLBM_OK;
     const long long tot = (long long)s->Q * s->nbc;
-    k_fill_side<<<(unsigned)((tot + 255) / 256), 256, 0, s->stream>>>(s->side[0], s->side[1], s->nbc, s->Q,
-                                                                        (float)s->cfg.rho0);
+    k_fill_side<<<(unsigned)((tot + 255) / 256), 256, 0, s->stream>>>(s->side[0], s->side[1], s->nbc, s->Q);
     VLBM_CUDA(cudaGetLastError());
     VLBM_CUDA(cudaStreamSynchronize(s->stream));
     return VLBM_OK;
@@ -201,7 +207,7 @@ using namespace vlbm;
 vlbm_sim::~vlbm_sim() {
     if (ibm) { ibm_destroy(ibm, allocator); ibm = nullptr; }
     for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)bc_node, (void*)side[0], (void*)side[1],
-                    (void*)omega, (void*)fibm, (void*)err, (void*)scratch, (void*)red_scratch})
+                    (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch})
         free_with(allocator, p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -294,6 +300,8 @@ vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator,
     s->bc_slot = static_cast<int32_t*>(p);
     if ((st = alloc_dev(s, &p, sizeof(unsigned int))) != VLBM_OK) { delete s; return st; }
     s->err = static_cast<unsigned int*>(p);
+    if ((st = alloc_dev(s, &p, 2 * sizeof(unsigned int))) != VLBM_OK) { delete s; return st; }
+    s->step_ctr = static_cast<unsigned int*>(p);
     if (cfg->rheology == VLBM_POWERLAW) {
         if ((st = alloc_dev(s, &p, N * sizeof(float))) != VLBM_OK) { delete s; return st; }
         s->omega = static_cast<float*>(p);
@@ -344,6 +352,7 @@ vlbm_status vlbm_init_equilibrium(vlbm_sim* s, double rho, double ux, double uy,
     s->parity = 0;
     s->apply_bc = 0;     // the initial state carries no boundary rule (main.cu:204-213)
     s->step = 0;
+    VLBM_CUDA(sync_step_ctr(s, s->stream));
     if (s->fibm) VLBM_CUDA(cudaMemsetAsync(s->fibm, 0, (size_t)3 * s->N * sizeof(float), s->stream));
     if (s->nbc > 0) { vlbm_status st = fill_side_equilibrium(s); if (st != VLBM_OK) return st; }
     if (s->ibm) ibm_reset(s);
@@ -438,6 +447,7 @@ vlbm_status vlbm_set_populations(vlbm_sim* s, const float* pops, size_t n) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     s->parity = 0;
     s->apply_bc = 0;   // given populations already carry their boundary values
+    VLBM_CUDA(sync_step_ctr(s, s->stream));
     return cuda_status(e, "vlbm_set_populations");
 }
 
@@ -521,6 +531,7 @@ vlbm_status vlbm_autotune(vlbm_sim* s, int32_t* chosen) {
     if (bo) VLBM_CUDA(cudaMemcpy(s->omega, bo, (size_t)s->N * sizeof(float), cudaMemcpyDeviceToDevice));
     cudaFree(bp); cudaFree(bs0); cudaFree(bs1); cudaFree(bo);
     s->parity = parity; s->side_cur = side_cur; s->apply_bc = apply; s->step = step;
+    sync_step_ctr(s, s->stream);
     vlbm_set_variant(s, bestv);
     if (chosen) *chosen = bestv;
     VLBM_CUDA(cudaGetLastError());

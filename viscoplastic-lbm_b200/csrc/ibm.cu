@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmPa
         float f[Q];
         uint8_t cls;
         gather<Q, ST, ODD, PAIRED>(sp, n, nb, x, y, z, f, cls);
-        const Mom m = moments<Q, false>(f, P.fx, P.fy, P.fz);
+        const Mom m = moments<Q, false>(f, P.fx, P.fy, P.fz, sp.rho0);
         fields[n] = m.rho;
         fields[N + n] = m.ux;
         fields[2 * N + n] = m.uy;

@@ -58,6 +58,7 @@ struct StepParams {
     float omega_p, yield;       // Bingham
     float n_index, k_cons, gamma0;  // Power-Law
     float scale, inv_scale, rho0;   // deviation storage
+    unsigned* ctr;                  // [2] step counter by AA parity (seeds the stochastic rounding)
 };
 
 struct MacroParams {

@@ -47,6 +47,7 @@ __global__ void k_batch_advance(BatchState* state, int nslots) {
     state[i].parity ^= 1;
     state[i].side_cur ^= 1;
     state[i].apply_bc = 1;
+    state[i].step += 1;
 }
 
 cudaError_t launch_batch_advance(BatchState* state, int nslots, cudaStream_t s) {
@@ -381,6 +382,7 @@ vlbm_status server_rebuild(vlbm_server* sv) {
         bs.parity = s->parity;
         bs.side_cur = s->side_cur;
         bs.apply_bc = s->apply_bc;
+        bs.step = (unsigned)s->step;
         slots.push_back(bs);
         const unsigned nt = (unsigned)((s->N + BATCH_TILE - 1) / BATCH_TILE);
         for (unsigned t = 0; t < nt; ++t) table.push_back(BatchBlock{local, t * (unsigned)BATCH_TILE});
@@ -392,6 +394,13 @@ vlbm_status server_rebuild(vlbm_server* sv) {
     }
     sv->branch_res = sv->ibm_res;
     sv->branch_res.insert(sv->branch_res.end(), sv->own_res.begin(), sv->own_res.end());
+    // lattices with their own launches count their steps on the device (the
+    // stochastic-rounding seed); one that stepped in the batched launch so far
+    // resumes from its host count
+    for (int idx : sv->branch_res) {
+        cudaError_t e = sync_step_ctr(sv->res[idx].sim, sv->stream);
+        if (e != cudaSuccess) return cuda_status(e, "step counter");
+    }
     // one side stream and join event per lattice with its own launches
     while (sv->side_streams.size() < sv->branch_res.size()) {
         cudaStream_t t = nullptr;

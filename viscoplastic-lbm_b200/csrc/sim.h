@@ -49,6 +49,7 @@ struct vlbm_sim {
     float* omega = nullptr;          // [N] Power-Law state
     float* fibm = nullptr;           // [3][N] IBM force (allocated with spheres)
     unsigned int* err = nullptr;     // device error word
+    unsigned int* step_ctr = nullptr;  // [2] device step count by AA parity
     float* scratch = nullptr;        // [5][N] macroscopic output scratch (lazy)
     double* red_scratch = nullptr;   // FP64 reduction partials + result (lazy)
     size_t device_bytes = 0;
@@ -70,6 +71,8 @@ struct vlbm_sim {
 namespace vlbm {
 
 StepParams make_params(vlbm_sim* s);
+// Write the host step count into the device counter slot of the current parity.
+cudaError_t sync_step_ctr(vlbm_sim* s, cudaStream_t stream);
 // Device memory of a simulation, through its allocator (if any).
 cudaError_t sim_malloc(vlbm_sim* s, void** p, size_t bytes);
 void sim_free(vlbm_sim* s, void* p);

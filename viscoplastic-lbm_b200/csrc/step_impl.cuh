@@ -33,27 +33,74 @@
 namespace vlbm {
 
 // ------------------------------------------------------------- storage --
+// Half-precision stores round stochastically: a deviation is rounded up in
+// magnitude with probability equal to the dropped fraction, so the stored
+// value is exact on average.  With round-to-nearest, a slow body-force-driven
+// flow stalls: the per-step change of a population (about 3 w c.F, ~1e-6 for
+// F = 5e-6) is below half an FP16 ulp of its deviation (~1e-2 x 2^-11) and is
+// rounded away every step.  The random bits come from a per-thread linear
+// congruential stream seeded by a hash of (node, step), so a run is
+// reproducible and independent of the launch it runs in.
+struct Rng {
+    unsigned x;
+    __device__ __forceinline__ Rng(unsigned n, unsigned seed) {
+        unsigned h = n * 0x9E3779B1u + seed * 0x85EBCA77u + 0x165667B1u;
+        h ^= h >> 16;
+        h *= 0x7FEB352Du;
+        h ^= h >> 15;
+        h *= 0x846CA68Bu;
+        h ^= h >> 16;
+        x = h;
+    }
+    __device__ __forceinline__ unsigned next() { x = x * 1664525u + 1013904223u; return x; }
+};
+
+// float -> half, rounding toward zero after adding 13 random bits below the
+// kept mantissa (stochastic rounding of normal values).
+__device__ __forceinline__ __half half_sr(float v, unsigned r) {
+    return __float2half_rz(__uint_as_float(__float_as_uint(v) + (r >> 19)));
+}
+// float -> bfloat16, the same with 16 random bits.
+__device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, unsigned r) {
+    return __ushort_as_bfloat16((unsigned short)((__float_as_uint(v) + (r >> 16)) >> 16));
+}
+
+// The kernels work on deviations g_i = f_i - w_i rho0 from the rest
+// equilibrium: moments are sums of small numbers and the collision produces the
+// post-collision deviation directly.  Summing full populations instead (values
+// w_i + small, whose trailing bits are those of w_i on every node) makes the
+// FP32 rounding of rho systematic: with half-precision storage that created
+// ~1e-7 of mass per node and step.  FP32 storage keeps the populations
+// themselves (the reference's state); half storage keeps g_i * scale.
 template <int ST> struct Store;
 template <> struct Store<VLBM_STORE_F32> {
     using T = float;
-    static __device__ __forceinline__ float ld(const T* p, float, const StepParams&) { return *p; }
-    static __device__ __forceinline__ void st(T* p, float v, float, const StepParams&) { *p = v; }
+    static __device__ __forceinline__ float ld(const T* p, float w, const StepParams& s) { return *p - w * s.rho0; }
+    static __device__ __forceinline__ void st(T* p, float g, float w, const StepParams& s, Rng&) { *p = g + w * s.rho0; }
+    // a full population (initial state, user state)
+    static __device__ __forceinline__ void st_abs(T* p, float v, float, const StepParams&) { *p = v; }
 };
 template <> struct Store<VLBM_STORE_F16> {
     using T = __half;
-    static __device__ __forceinline__ float ld(const T* p, float w, const StepParams& s) {
-        return fmaf(__half2float(*p), s.inv_scale, w * s.rho0);
+    static __device__ __forceinline__ float ld(const T* p, float, const StepParams& s) {
+        return __half2float(*p) * s.inv_scale;
     }
-    static __device__ __forceinline__ void st(T* p, float v, float w, const StepParams& s) {
+    static __device__ __forceinline__ void st(T* p, float g, float, const StepParams& s, Rng& r) {
+        *p = half_sr(g * s.scale, r.next());
+    }
+    static __device__ __forceinline__ void st_abs(T* p, float v, float w, const StepParams& s) {
         *p = __float2half_rn((v - w * s.rho0) * s.scale);
     }
 };
 template <> struct Store<VLBM_STORE_BF16> {
     using T = __nv_bfloat16;
-    static __device__ __forceinline__ float ld(const T* p, float w, const StepParams& s) {
-        return fmaf(__bfloat162float(*p), s.inv_scale, w * s.rho0);
+    static __device__ __forceinline__ float ld(const T* p, float, const StepParams& s) {
+        return __bfloat162float(*p) * s.inv_scale;
     }
-    static __device__ __forceinline__ void st(T* p, float v, float w, const StepParams& s) {
+    static __device__ __forceinline__ void st(T* p, float g, float, const StepParams& s, Rng& r) {
+        *p = bf16_sr(g * s.scale, r.next());
+    }
+    static __device__ __forceinline__ void st_abs(T* p, float v, float w, const StepParams& s) {
         *p = __float2bfloat16_rn((v - w * s.rho0) * s.scale);
     }
 };
@@ -245,10 +292,12 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, con
         // D3Q19_VelBounceBack.cu:31-43: rho_w over all streamed populations
         // (including the wrapped unknowns), unknown <- streamed opposite
         // - 6 rho_w w_i (c_opp . u_w).  The opposite of an unknown at a face is
-        // always a known population, so the update can run in place.
+        // always a known population, so the update can run in place.  On
+        // deviations: rho_w = rho0 + sum g, and w_opp = w_i cancels.
         float rw = 0.f;
 #pragma unroll
         for (int i = 0; i < Q; ++i) rw += f[i];
+        rw += p.rho0;
 #pragma unroll
         for (int i = 1; i < Q; ++i)
             if ((r.mask >> i) & 1u) {
@@ -273,10 +322,15 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, con
             }
         break;
     case K_BC_VEL_ZOUHE:
-        if constexpr (Q == 19) zouhe_vel19(f, r.dir, r.uw[0], r.uw[1], r.uw[2]);
-        break;
     case K_BC_PRES_ZOUHE:
-        if constexpr (Q == 19) zouhe_pres19(f, r.dir, r.rhow);
+        if constexpr (Q == 19) {   // the reference's formulas act on full populations
+#pragma unroll
+            for (int i = 0; i < Q; ++i) f[i] += Lattice<Q>::w(i) * p.rho0;
+            if (r.scheme == K_BC_VEL_ZOUHE) zouhe_vel19(f, r.dir, r.uw[0], r.uw[1], r.uw[2]);
+            else zouhe_pres19(f, r.dir, r.rhow);
+#pragma unroll
+            for (int i = 0; i < Q; ++i) f[i] -= Lattice<Q>::w(i) * p.rho0;
+        }
         break;
     default: break;
     }
@@ -356,14 +410,18 @@ __device__ __forceinline__ int gather(const StepParams& p, unsigned n, const Nbr
 // second moments (lbm.cu:149-190) and the stress magnitude used by the
 // rheology models (lbm.cu:192-208).
 struct Mom {
-    float rho, ux, uy, uz;
+    float rho, drho, ux, uy, uz;
     float pxx, pyy, pzz, pxy, pxz, pyz;
 };
 
+// Moments of the deviations g_i = f_i - w_i rho0: rho = rho0 + sum g,
+// rho u = sum c g + F/2, and the non-equilibrium second moments
+// Pi_ab = sum c_a c_b f - rho (u_a u_b + delta_ab / 3)
+//       = sum c_a c_b g - rho u_a u_b - delta_ab (rho - rho0) / 3.
 template <int Q, bool NEED_PI>
-__device__ __forceinline__ Mom moments(const float (&f)[Q], float fx, float fy, float fz) {
-    // Sums over opposite pairs: e = f_i + f_opp feeds the even moments (rho,
-    // second moments), o = f_i - f_opp the odd ones (momentum).
+__device__ __forceinline__ Mom moments(const float (&f)[Q], float fx, float fy, float fz, float rho0) {
+    // Sums over opposite pairs: e = g_i + g_opp feeds the even moments (rho,
+    // second moments), o = g_i - g_opp the odd ones (momentum).
     Mom m;
     float rho = f[0], jx = 0.f, jy = 0.f, jz = 0.f;
     float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
@@ -384,16 +442,23 @@ __device__ __forceinline__ Mom moments(const float (&f)[Q], float fx, float fy, 
             if (cy && cz) syz += cy * cz * e;
         }
     }
-    const float inv = __fdividef(1.f, rho);  // hardware reciprocal (<= 2 ulp)
+    // correctly rounded reciprocal: u = j/rho enters every equilibrium, and a
+    // biased approximate reciprocal (the hardware MUFU result is within 2 ulp
+    // but not unbiased) acts like a spurious force proportional to the
+    // momentum, which shifts a slow channel flow by ~1e-3 over 1e4 steps
+    const float drho = rho;
+    rho += rho0;
+    const float inv = __frcp_rn(rho);
     m.rho = rho;
+    m.drho = drho;
     m.ux = (jx + 0.5f * fx) * inv;
     m.uy = (jy + 0.5f * fy) * inv;
     m.uz = (jz + 0.5f * fz) * inv;
     if (NEED_PI) {
-        const float cs2 = 1.f / 3.f;
-        m.pxx = sxx - rho * (m.ux * m.ux + cs2);
-        m.pyy = syy - rho * (m.uy * m.uy + cs2);
-        m.pzz = szz - rho * (m.uz * m.uz + cs2);
+        const float dr3 = drho * (1.f / 3.f);
+        m.pxx = sxx - rho * m.ux * m.ux - dr3;
+        m.pyy = syy - rho * m.uy * m.uy - dr3;
+        m.pzz = szz - rho * m.uz * m.uz - dr3;
         m.pxy = sxy - rho * m.ux * m.uy;
         m.pxz = sxz - rho * m.ux * m.uz;
         m.pyz = syz - rho * m.uy * m.uz;
@@ -447,7 +512,8 @@ __device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega
     if (OP == VLBM_OP_REGULARIZED) {
         const float A = 4.5f * (1.f - omega);
         const float tr = (m.pxx + m.pyy + m.pzz) * (1.f / 3.f);
-        const float K0 = m.rho * (1.f - 1.5f * uu) - 3.f * B * uF - A * tr;
+        // the rest part w_i rho0 is not formed: K0 is the deviation of rho(1 - 1.5 u^2)
+        const float K0 = m.drho - 1.5f * m.rho * uu - 3.f * B * uF - A * tr;
         const float alpha = 3.f * B - A * (1.f / 3.f);
         const float r3 = 3.f * m.rho, r45 = 4.5f * m.rho, b9 = 9.f * B;
         f[0] = Lattice<Q>::w(0) * K0;
@@ -478,7 +544,8 @@ __device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega
         }
     } else {
         const float om1 = 1.f - omega;
-        const float base = omega * m.rho * (1.f - 1.5f * uu) - 3.f * B * uF;
+        // on deviations: (1 - omega) w rho0 + omega w rho0 cancels against w rho0
+        const float base = omega * (m.drho - 1.5f * m.rho * uu) - 3.f * B * uF;
         const float r45 = 4.5f * omega * m.rho, r3 = 3.f * omega * m.rho, b9 = 9.f * B, b3 = 3.f * B;
         f[0] = om1 * f[0] + Lattice<Q>::w(0) * base;
 #pragma unroll
@@ -511,7 +578,7 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, float* si
         p.cls[n] = cls & (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
     }
     constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
-    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz);
+    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz, p.rho0);
     if (!(m.rho > 0.f && m.rho < 1e30f)) atomicOr(p.err, 1u);
     float omega = p.omega_newt;
     if (RHEO != VLBM_NEWTONIAN) {
@@ -540,7 +607,7 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned 
 // flight to saturate HBM.
 template <int Q, int OP, int RHEO, int ST, bool ODD>
 __device__ __forceinline__ void step_node(const StepParams& p, const float* side_prev, float* side_next, int use_bc,
-                                          unsigned n) {
+                                          unsigned seed, unsigned n) {
     using S = Store<ST>;
     using T = typename S::T;
     const int x = (int)(n % (unsigned)p.nx);
@@ -555,25 +622,37 @@ __device__ __forceinline__ void step_node(const StepParams& p, const float* side
     const int slot = gather<Q, ST, ODD>(p, side_prev, use_bc, n, nb, x, y, z, f, cls);
     relax_and_collide<Q, OP, RHEO>(p, side_next, n, cls, slot, f);
     nb.launder();
+    Rng rng(n, seed);
     T* plane = static_cast<T*>(p.pop);
     const size_t N = (size_t)p.N;
 #pragma unroll
     for (int j = 0; j < Q; ++j, plane += N) {
         if (!ODD) {  // plane j receives the post-collision value of opp(j) at this node
             const int i = lat_opp(j);
-            S::st(plane + n, f[i], Lattice<Q>::w(i), p);
+            S::st(plane + n, f[i], Lattice<Q>::w(i), p, rng);
         } else {     // plane j receives population j streamed to the downstream node
             const unsigned dst = n + nb.off(lat_cx(j), lat_cy(j), lat_cz(j));
-            S::st(plane + dst, f[j], Lattice<Q>::w(j), p);
+            S::st(plane + dst, f[j], Lattice<Q>::w(j), p, rng);
         }
     }
 }
 
+// The step count that seeds the stochastic rounding lives on the device, one
+// slot per AA parity: a step reads its parity's slot and block 0 writes the
+// incremented count to the other parity's slot, which no thread of this step
+// reads, so a replayed graph of steps keeps counting.
+__device__ __forceinline__ unsigned step_seed(const StepParams& p, bool odd) {
+    const unsigned s = p.ctr[odd ? 1 : 0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr[odd ? 0 : 1] = s + 1;
+    return s;
+}
+
 template <int Q, int OP, int RHEO, int ST, bool ODD>
 __global__ void __launch_bounds__(256) k_step(const StepParams p) {
+    const unsigned seed = step_seed(p, ODD);
     const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= (unsigned)p.N) return;
-    step_node<Q, OP, RHEO, ST, ODD>(p, p.side_prev, p.side_next, p.apply_bc, n);
+    step_node<Q, OP, RHEO, ST, ODD>(p, p.side_prev, p.side_next, p.apply_bc, seed, n);
 }
 
 // ------------------------------------------------------- batched step --
@@ -593,7 +672,8 @@ constexpr int BATCH_MAX_SLOTS = 64;   // lattices per launch (their parameters a
 
 // Per-lattice state that changes every step (advanced by k_batch_advance).
 struct BatchState {
-    int side_cur, apply_bc, parity, pad;
+    int side_cur, apply_bc, parity;
+    unsigned step;      // steps taken (the stochastic-rounding seed)
 };
 struct BatchBlock {
     int slot;           // lattice of this tile: index into the launch's parameters
@@ -619,6 +699,7 @@ __global__ void __launch_bounds__(256, batch_min_blocks<Q>()) k_step_batched(con
     __shared__ StepParams sp;
     __shared__ float* sides[2];
     __shared__ int use_bc;
+    __shared__ unsigned seed;
     constexpr int WORDS = (int)(sizeof(StepParams) / 4);
     static_assert(sizeof(StepParams) % 4 == 0, "StepParams is copied as 32-bit words");
     int t = blockIdx.x;
@@ -640,12 +721,13 @@ __global__ void __launch_bounds__(256, batch_min_blocks<Q>()) k_step_batched(con
                 sides[0] = st.side_cur ? const_cast<float*>(q.side_next) : const_cast<float*>(q.side_prev);
                 sides[1] = st.side_cur ? const_cast<float*>(q.side_prev) : q.side_next;
                 use_bc = st.apply_bc;
+                seed = (unsigned)st.step;
             }
             __syncthreads();
             cur = e.slot;
         }
         const unsigned n = e.first + threadIdx.x;
-        if (n < (unsigned)sp.N) step_node<Q, OP, RHEO, ST, ODD>(sp, sides[0], sides[1], use_bc, n);
+        if (n < (unsigned)sp.N) step_node<Q, OP, RHEO, ST, ODD>(sp, sides[0], sides[1], use_bc, seed, n);
         e = en;
     }
 }
@@ -671,7 +753,7 @@ __global__ void __launch_bounds__(256) k_macro(const MacroParams mp) {
         fx += mp.fibm_const[n]; fy += mp.fibm_const[N + n]; fz += mp.fibm_const[2 * N + n];
     }
     constexpr bool NEED_PI = RHEO != VLBM_NEWTONIAN;
-    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz);
+    const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz, p.rho0);
     if (mp.rho) mp.rho[n] = m.rho;
     if (mp.ux) mp.ux[n] = m.ux;
     if (mp.uy) mp.uy[n] = m.uy;
@@ -703,7 +785,7 @@ __global__ void __launch_bounds__(256) k_get_pops(const StepParams p, float* out
     uint8_t cls;
     gather<Q, ST, ODD, PAIRED>(p, n, nb, x, y, z, f, cls);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) out[(size_t)i * (size_t)p.N + n] = f[i];
+    for (int i = 0; i < Q; ++i) out[(size_t)i * (size_t)p.N + n] = f[i] + Lattice<Q>::w(i) * p.rho0;
 }
 
 // Natural-layout store of given populations (equilibrium init or user state).
@@ -732,7 +814,7 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
             const float cu = lat_cx(i) * ux + lat_cy(i) * uy + lat_cz(i) * uz;
             v = Lattice<Q>::w(i) * rho * (1.f - 1.5f * uu + 3.f * cu * (1.f + 1.5f * cu));
         }
-        S::st(A + (size_t)i * N + sidx, v, Lattice<Q>::w(i), p);
+        S::st_abs(A + (size_t)i * N + sidx, v, Lattice<Q>::w(i), p);
     }
     if (p.omega) p.omega[n] = __int_as_float(0x7f800000);  // eta = +inf <=> omega = 0 (lbmInitialization.cu:111)
 }
@@ -742,32 +824,33 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
 template <int ST> struct Pair;
 template <> struct Pair<VLBM_STORE_F32> {
     using V = float2;
-    static __device__ __forceinline__ float get(const V& v, int lane, float, const StepParams&) {
-        return lane ? v.y : v.x;
+    static __device__ __forceinline__ float get(const V& v, int lane, float w, const StepParams& s) {
+        return (lane ? v.y : v.x) - w * s.rho0;
     }
-    static __device__ __forceinline__ void set(V& v, int lane, float f, float, const StepParams&) {
+    static __device__ __forceinline__ void set(V& v, int lane, float g, float w, const StepParams& s, Rng&) {
+        const float f = g + w * s.rho0;
         if (lane) v.y = f; else v.x = f;
     }
     static __device__ __forceinline__ V swap(const V& v) { return make_float2(v.y, v.x); }
 };
 template <> struct Pair<VLBM_STORE_F16> {
     using V = __half2;
-    static __device__ __forceinline__ float get(const V& v, int lane, float w, const StepParams& s) {
-        return fmaf(lane ? __high2float(v) : __low2float(v), s.inv_scale, w * s.rho0);
+    static __device__ __forceinline__ float get(const V& v, int lane, float, const StepParams& s) {
+        return (lane ? __high2float(v) : __low2float(v)) * s.inv_scale;
     }
-    static __device__ __forceinline__ void set(V& v, int lane, float f, float w, const StepParams& s) {
-        const __half h = __float2half_rn((f - w * s.rho0) * s.scale);
+    static __device__ __forceinline__ void set(V& v, int lane, float g, float, const StepParams& s, Rng& r) {
+        const __half h = half_sr(g * s.scale, r.next());
         v = lane ? __halves2half2(__low2half(v), h) : __halves2half2(h, __high2half(v));
     }
     static __device__ __forceinline__ V swap(const V& v) { return __lowhigh2highlow(v); }
 };
 template <> struct Pair<VLBM_STORE_BF16> {
     using V = __nv_bfloat162;
-    static __device__ __forceinline__ float get(const V& v, int lane, float w, const StepParams& s) {
-        return fmaf(lane ? __high2float(v) : __low2float(v), s.inv_scale, w * s.rho0);
+    static __device__ __forceinline__ float get(const V& v, int lane, float, const StepParams& s) {
+        return (lane ? __high2float(v) : __low2float(v)) * s.inv_scale;
     }
-    static __device__ __forceinline__ void set(V& v, int lane, float f, float w, const StepParams& s) {
-        const __nv_bfloat16 h = __float2bfloat16_rn((f - w * s.rho0) * s.scale);
+    static __device__ __forceinline__ void set(V& v, int lane, float g, float, const StepParams& s, Rng& r) {
+        const __nv_bfloat16 h = bf16_sr(g * s.scale, r.next());
         v = lane ? __halves2bfloat162(__low2bfloat16(v), h) : __halves2bfloat162(h, __high2bfloat16(v));
     }
     static __device__ __forceinline__ V swap(const V& v) { return __lowhigh2highlow(v); }
@@ -780,6 +863,7 @@ template <int Q, int OP, int RHEO, int ST, bool ODD>
 __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
     using PV = Pair<ST>;
     using V = typename PV::V;
+    const unsigned seed = step_seed(p, ODD);
     const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned M = (unsigned)(p.N >> 1);
     if (m >= M) return;
@@ -824,8 +908,13 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             }
         }
         relax_and_collide<Q, OP, RHEO>(p, n, cls, slot, f);
+        // random draws in destination-plane order, as the one-node kernel makes them
+        Rng rng(n, seed);
 #pragma unroll
-        for (int i = 0; i < Q; ++i) PV::set(in[i], lane, f[i], Lattice<Q>::w(i), p);
+        for (int j = 0; j < Q; ++j) {
+            const int i = ODD ? j : lat_opp(j);
+            PV::set(in[i], lane, f[i], Lattice<Q>::w(i), p, rng);
+        }
     }
     pn.launder();
     V* out = reinterpret_cast<V*>(p.pop);
