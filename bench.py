@@ -134,6 +134,36 @@ def cpu_baseline(vlbm, seconds_budget=15.0):
             "sample": f"{NX}x{NY}x{nz} slab of the workload, {steps} steps, FP64 oracle, {dt:.1f} s"}
 
 
+def storage_accuracy(vlbm, steps=6000, nxz=8):
+    """Velocity relative L2 of each population storage against the FP64 oracle.
+
+    The benchmark channel (walls in y, periodic x and z, NY = 128, the same
+    Bingham parameters) is invariant along x and z, so an nxz x 128 x nxz slab
+    carries its profile; the oracle runs it on the host.
+    """
+    import numpy as np
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    oracle.set_threads(os.cpu_count() or 1)
+    cfg = make_cfg(vlbm)
+    cfg.nx, cfg.nz = nxz, nxz
+    node_map = vlbm.build_node_map(vlbm.BUILDER_PLATES_Y, nxz, NY, nxz)
+    o = oracle.Oracle(cfg, node_map)
+    o.step(steps)
+    ref = o.macroscopics()["ux"]
+    out = {"steps": steps, "lattice": f"{nxz}x{NY}x{nxz}", "reference": "FP64 oracle"}
+    for name, st in (("f32", vlbm.STORE_F32), ("f16", vlbm.STORE_F16), ("bf16", vlbm.STORE_BF16)):
+        c = make_cfg(vlbm, st)
+        c.nx, c.nz = nxz, nxz
+        sim = vlbm.Simulation(c, node_map=node_map)
+        sim.step(steps)
+        sim.sync()
+        ux = sim.macroscopics()["ux"].astype(np.float64)
+        sim.close()
+        out[name + "_rel_l2_ux"] = float(np.linalg.norm(ux - ref) / np.linalg.norm(ref))
+    return out
+
+
 def serving_requests(vlbm, n, step_scale, seed=2024):
     """A seeded sample of the Bingham-duct serving stream.
 
@@ -385,6 +415,9 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(vlbm)
+    accuracy = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        accuracy = storage_accuracy(vlbm)
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_leg(vlbm, args.serving_requests, args.serving_step_scale, args.serving_rate)
@@ -408,6 +441,7 @@ def main():
             "gpu_launches": args.steps,
             "kernel_variant": variant,
             "clocks": clk,
+            "storage_accuracy": accuracy,
             "serving": serving,
         }
         print(json.dumps(line), flush=True)
