@@ -119,9 +119,10 @@ typedef struct vlbm_config {
 
 /* Population storage order.  NATURAL: planes [Q][z][y][x].  ZPAIR: nodes z and
  * z+NZ/2 of the same (x, y) are adjacent, so every stencil access of the fused
- * step is one aligned two-node vector (requires even NZ).  AUTO picks ZPAIR for
- * D3Q19 with FP16/BF16 storage and even NZ, NATURAL otherwise.  The layout is
- * internal: every entry point takes and returns the [z][y][x] order. */
+ * step is one aligned two-node vector (requires even NZ) and the arithmetic
+ * runs on packed FP32x2.  AUTO picks ZPAIR for even NZ with FP16/BF16 storage
+ * or D3Q27, NATURAL otherwise (D3Q19 FP32).  The layout is internal: every
+ * entry point takes and returns the [z][y][x] order. */
 enum { VLBM_LAYOUT_AUTO = 0, VLBM_LAYOUT_NATURAL = 1, VLBM_LAYOUT_ZPAIR = 2 };
 
 /* Fill `cfg` with the reference defaults (var.h / nnf.h values, D3Q19, FP32,

@@ -278,10 +278,13 @@ vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator,
     {   // population layout
         const bool even_z = cfg->nz % 2 == 0;
         int lay = cfg->layout;
-        // two-node threads pay off where the per-node state is small: D3Q19 with
-        // 2-byte storage (the D3Q27 pair kernel needs over 110 registers)
+        // two-node threads with packed FP32x2 arithmetic pay off where the step
+        // is bound by instruction issue: 2-byte storage, and D3Q27 (measured on
+        // B200: D3Q27 256^3 FP32 30.1 vs 28.3k MLUPS, FP16 37.7 vs 31.8k; D3Q19
+        // FP32 is at the HBM roofline either way and keeps the natural layout)
         if (lay == VLBM_LAYOUT_AUTO)
-            lay = (cfg->storage != VLBM_STORE_F32 && cfg->vel_set == 19 && even_z) ? VLBM_LAYOUT_ZPAIR : VLBM_LAYOUT_NATURAL;
+            lay = ((cfg->storage != VLBM_STORE_F32 || cfg->vel_set == 27) && even_z) ? VLBM_LAYOUT_ZPAIR
+                                                                                      : VLBM_LAYOUT_NATURAL;
         if (lay == VLBM_LAYOUT_ZPAIR && !even_z) { delete s; set_last_error("the z-paired layout needs an even nz"); return VLBM_ERR_INVALID; }
         s->pairH = lay == VLBM_LAYOUT_ZPAIR ? cfg->nz / 2 : 0;
     }

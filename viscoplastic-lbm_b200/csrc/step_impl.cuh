@@ -29,6 +29,7 @@
 #include <cuda_bf16.h>
 #include "internal.h"
 #include "lattice.cuh"
+#include "pair_math.cuh"
 
 namespace vlbm {
 
@@ -832,6 +833,13 @@ template <> struct Pair<VLBM_STORE_F32> {
         if (lane) v.y = f; else v.x = f;
     }
     static __device__ __forceinline__ V swap(const V& v) { return make_float2(v.y, v.x); }
+    // both lanes as deviations / packed from deviations
+    static __device__ __forceinline__ float2 get2(const V& v, float w, const StepParams& s) {
+        return sub2(v, f2(w * s.rho0));
+    }
+    static __device__ __forceinline__ V pack2(float2 g, float w, const StepParams& s, Rng&, Rng&) {
+        return add2(g, f2(w * s.rho0));
+    }
 };
 template <> struct Pair<VLBM_STORE_F16> {
     using V = __half2;
@@ -843,6 +851,18 @@ template <> struct Pair<VLBM_STORE_F16> {
         v = lane ? __halves2half2(__low2half(v), h) : __halves2half2(h, __high2half(v));
     }
     static __device__ __forceinline__ V swap(const V& v) { return __lowhigh2highlow(v); }
+    static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams& s) {
+        return mul2(__half22float2(v), f2(s.inv_scale));
+    }
+    // both lanes rounded stochastically and packed with one conversion
+    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng& r1) {
+        const float2 v = mul2(g, f2(s.scale));
+        const float lo = __uint_as_float(__float_as_uint(v.x) + (r0.next() >> 19));
+        const float hi = __uint_as_float(__float_as_uint(v.y) + (r1.next() >> 19));
+        unsigned out;
+        asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(hi), "f"(lo));
+        return *reinterpret_cast<__half2*>(&out);
+    }
 };
 template <> struct Pair<VLBM_STORE_BF16> {
     using V = __nv_bfloat162;
@@ -854,6 +874,16 @@ template <> struct Pair<VLBM_STORE_BF16> {
         v = lane ? __halves2bfloat162(__low2bfloat16(v), h) : __halves2bfloat162(h, __high2bfloat16(v));
     }
     static __device__ __forceinline__ V swap(const V& v) { return __lowhigh2highlow(v); }
+    static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams& s) {
+        return mul2(__bfloat1622float2(v), f2(s.inv_scale));
+    }
+    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng& r1) {
+        const float2 v = mul2(g, f2(s.scale));
+        const unsigned lo = (__float_as_uint(v.x) + (r0.next() >> 16)) >> 16;
+        const unsigned hi = (__float_as_uint(v.y) + (r1.next() >> 16)) & 0xFFFF0000u;
+        const unsigned out = hi | lo;
+        return *reinterpret_cast<const __nv_bfloat162*>(&out);
+    }
 };
 
 // One thread advances the node pair (x, y, zp) / (x, y, zp+H).  Every access is
@@ -890,31 +920,80 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             in[i] = sw ? PV::swap(v) : v;
         }
     }
+    // both nodes as float2 deviations: lane 0 is (x, y, zp), lane 1 (x, y, zp + H)
+    float2 g[Q];
 #pragma unroll
-    for (int lane = 0; lane < 2; ++lane) {
-        const int z = zp + lane * H;
-        const unsigned n = (unsigned)(((size_t)z * p.ny + y) * p.nx + x);
-        float f[Q];
+    for (int i = 0; i < Q; ++i) g[i] = PV::get2(in[i], Lattice<Q>::w(i), p);
+    const unsigned n0 = (unsigned)(((size_t)zp * p.ny + y) * p.nx + x);
+    const unsigned n1 = (unsigned)(((size_t)(zp + H) * p.ny + y) * p.nx + x);
+    const uint8_t c0 = p.cls[n0], c1 = p.cls[n1];
+    int slot0 = -1, slot1 = -1;
+    if ((c0 | c1) & NODE_BC) {   // boundary rules per lane, on scalars
 #pragma unroll
-        for (int i = 0; i < Q; ++i) f[i] = PV::get(in[i], lane, Lattice<Q>::w(i), p);
-        const uint8_t cls = p.cls[n];
-        int slot = -1;
-        if (cls & NODE_BC) {
-            slot = p.bc_slot[n];
+        for (int lane = 0; lane < 2; ++lane) {
+            const uint8_t cl = lane ? c1 : c0;
+            if (!(cl & NODE_BC)) continue;
+            const unsigned nl = lane ? n1 : n0;
+            const int zl = zp + lane * H;
+            const int sl = p.bc_slot[nl];
+            if (lane) slot1 = sl; else slot0 = sl;
             if (p.apply_bc) {
+                float f[Q];
+#pragma unroll
+                for (int i = 0; i < Q; ++i) f[i] = lane_of(g[i], lane);
                 Nbr nb;
-                nb.init(x, y, z, p.nx, p.ny, p.nz);
-                apply_bc<Q>(f, p, slot, x, y, z, nb, n);
+                nb.init(x, y, zl, p.nx, p.ny, p.nz);
+                apply_bc<Q>(f, p, sl, x, y, zl, nb, nl);
+#pragma unroll
+                for (int i = 0; i < Q; ++i) set_lane(g[i], lane, f[i]);
             }
         }
-        relax_and_collide<Q, OP, RHEO>(p, n, cls, slot, f);
-        // random draws in destination-plane order, as the one-node kernel makes them
-        Rng rng(n, seed);
+    }
+    float2 fx2 = f2(p.fx), fy2 = f2(p.fy), fz2 = f2(p.fz);
+    if ((c0 | c1) & NODE_IBM_FORCE) {   // IBM force read and reset (lbm.cu:45-58)
+        const size_t N = (size_t)p.N;
 #pragma unroll
-        for (int j = 0; j < Q; ++j) {
-            const int i = ODD ? j : lat_opp(j);
-            PV::set(in[i], lane, f[i], Lattice<Q>::w(i), p, rng);
+        for (int lane = 0; lane < 2; ++lane) {
+            const uint8_t cl = lane ? c1 : c0;
+            if (!(cl & NODE_IBM_FORCE)) continue;
+            const unsigned nl = lane ? n1 : n0;
+            set_lane(fx2, lane, p.fx + p.fibm[nl]);
+            set_lane(fy2, lane, p.fy + p.fibm[N + nl]);
+            set_lane(fz2, lane, p.fz + p.fibm[2 * N + nl]);
+            p.fibm[nl] = 0.f; p.fibm[N + nl] = 0.f; p.fibm[2 * N + nl] = 0.f;
+            p.cls[nl] = cl & (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
         }
+    }
+    constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
+    const Mom2 mm = moments2<Q, NEED_PI>(g, fx2, fy2, fz2, p.rho0);
+    if (!(mm.rho.x > 0.f && mm.rho.x < 1e30f) || !(mm.rho.y > 0.f && mm.rho.y < 1e30f)) atomicOr(p.err, 1u);
+    float2 omega = f2(p.omega_newt);
+    if (RHEO != VLBM_NEWTONIAN) {
+        const float2 aux = stress_aux2(mm, fx2, fy2, fz2);
+#pragma unroll
+        for (int lane = 0; lane < 2; ++lane) {
+            const unsigned nl = lane ? n1 : n0;
+            const float old = (RHEO == VLBM_POWERLAW) ? p.omega[nl] : 0.f;
+            float eta = 0.f;
+            set_lane(omega, lane, relax<RHEO>(p, old, lane_of(aux, lane), eta));
+            if (RHEO == VLBM_POWERLAW) p.omega[nl] = eta;   // state update, lbm.cu:215-219
+        }
+    }
+    collide2<Q, OP>(g, mm, omega, fx2, fy2, fz2);
+    if (slot0 >= 0 || slot1 >= 0) {   // post-collision values of boundary nodes (lbm.cu:463-470)
+        const size_t nbc = (size_t)p.nbc;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            if (slot0 >= 0) p.side_next[(size_t)i * nbc + slot0] = g[i].x;
+            if (slot1 >= 0) p.side_next[(size_t)i * nbc + slot1] = g[i].y;
+        }
+    }
+    // random draws per node in destination-plane order, as the one-node kernel makes them
+    Rng r0(n0, seed), r1(n1, seed);
+#pragma unroll
+    for (int j = 0; j < Q; ++j) {
+        const int i = ODD ? j : lat_opp(j);
+        in[i] = PV::pack2(g[i], Lattice<Q>::w(i), p, r0, r1);
     }
     pn.launder();
     V* out = reinterpret_cast<V*>(p.pop);
