@@ -854,11 +854,13 @@ template <> struct Pair<VLBM_STORE_F16> {
     static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams& s) {
         return mul2(__half22float2(v), f2(s.inv_scale));
     }
-    // both lanes rounded stochastically and packed with one conversion
-    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng& r1) {
+    // both lanes rounded stochastically (13 random bits each, two slices of one
+    // draw) and packed with one conversion
+    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
         const float2 v = mul2(g, f2(s.scale));
-        const float lo = __uint_as_float(__float_as_uint(v.x) + (r0.next() >> 19));
-        const float hi = __uint_as_float(__float_as_uint(v.y) + (r1.next() >> 19));
+        const unsigned r = r0.next();
+        const float lo = __uint_as_float(__float_as_uint(v.x) + (r >> 19));
+        const float hi = __uint_as_float(__float_as_uint(v.y) + ((r >> 6) & 0x1FFFu));
         unsigned out;
         asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(hi), "f"(lo));
         return *reinterpret_cast<__half2*>(&out);
@@ -877,10 +879,11 @@ template <> struct Pair<VLBM_STORE_BF16> {
     static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams& s) {
         return mul2(__bfloat1622float2(v), f2(s.inv_scale));
     }
-    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng& r1) {
+    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
         const float2 v = mul2(g, f2(s.scale));
-        const unsigned lo = (__float_as_uint(v.x) + (r0.next() >> 16)) >> 16;
-        const unsigned hi = (__float_as_uint(v.y) + (r1.next() >> 16)) & 0xFFFF0000u;
+        const unsigned r = r0.next();
+        const unsigned lo = (__float_as_uint(v.x) + (r >> 16)) >> 16;
+        const unsigned hi = (__float_as_uint(v.y) + (r & 0xFFFFu)) & 0xFFFF0000u;
         const unsigned out = hi | lo;
         return *reinterpret_cast<const __nv_bfloat162*>(&out);
     }
@@ -988,8 +991,10 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             if (slot1 >= 0) p.side_next[(size_t)i * nbc + slot1] = g[i].y;
         }
     }
-    // random draws per node in destination-plane order, as the one-node kernel makes them
-    Rng r0(n0, seed), r1(n1, seed);
+    // one random stream per node pair, drawn in destination-plane order; each
+    // draw gives both lanes their bits (the one-node kernel has a stream per
+    // node, so the two layouts round differently but equally well)
+    Rng r0(n0, seed), r1(n0, seed);
 #pragma unroll
     for (int j = 0; j < Q; ++j) {
         const int i = ODD ? j : lat_opp(j);
