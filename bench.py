@@ -55,11 +55,23 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """dram read+write bytes per launch of the fused kernel from the committed ncu summary."""
-    path = os.path.join(REPO, "profiles", "fused_step_d3q19_bingham_256x128x64.md")
+TRAFFIC_PROFILES = {
+    # (storage, resolved layout) -> ncu summary of that kernel on this workload
+    ("f32", "natural"): "fused_step_d3q19_bingham_256x128x64.md",
+    ("f16", "zpair"): "fused_step2_d3q19_bingham_f16_256x128x64.md",
+}
+
+
+def committed_traffic(storage, layout):
+    """dram read+write bytes per launch of the fused kernel from the committed ncu summary
+    of the same storage and layout (None when no capture of that kernel is committed)."""
+    if layout == "auto":   # the library's AUTO rule for D3Q19 with an even nz
+        layout = "natural" if storage == "f32" else "zpair"
+    name = TRAFFIC_PROFILES.get((storage, layout))
+    if name is None:
+        return None
     try:
-        for line in open(path):
+        for line in open(os.path.join(REPO, "profiles", name)):
             if line.startswith("traffic_bytes_per_launch:"):
                 return float(line.split(":", 1)[1].strip())
     except OSError:
@@ -384,7 +396,7 @@ def main():
     bytes_per_node = info.bytes_per_node_step
     achieved_gbs = bytes_per_node * N / (ms / 1e3 / args.steps) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = committed_traffic()
+    traffic = committed_traffic(args.storage, args.layout)
 
     # end to end through the public API with host buffers: upload the state from
     # pinned host memory, advance, read the macroscopics back
