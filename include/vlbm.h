@@ -277,6 +277,57 @@ vlbm_status vlbm_get_lagrangian_nodes(vlbm_sim* sim, double* pos, double* force,
 vlbm_status vlbm_write_macr_bin(vlbm_sim* sim, const char* path_files, const char* id_sim,
                                 uint32_t step_label, int32_t export_forces);
 
+/* --------------------------------------------------------- checkpoint --- */
+/* Complete state of a simulation as one image (replaces operateSimCheckpoint /
+ * saveSimCheckpoint / loadSimCheckpoint, simCheckpoint.cu:216-318, which write
+ * and read step, pop, popAux, rho, u, omega, f and the IBM arrays as raw files):
+ * populations as stored, boundary side stores, Power-Law omega, IBM force field
+ * and node classes, device step counters, particle and Lagrangian-node state,
+ * with a header that names the lattice, storage, layout and geometry and a
+ * trailing hash.  A run resumed from an image continues bit for bit like the
+ * run that wrote it.  Both calls synchronise the simulation's stream.
+ *
+ * vlbm_checkpoint_save: writes the image into `buf` (`n` bytes) and its size
+ * into `*needed` (may be NULL); `buf` NULL only reports the size; a buffer
+ * smaller than the image returns VLBM_ERR_INVALID with nothing written.
+ * vlbm_checkpoint_load: the simulation must have been created with the same
+ * nx, ny, nz, velocity set, storage (and scale) and layout, have the same
+ * geometry and, with spheres, the same particle and node counts (the reference
+ * creates its particles before loading them too); otherwise VLBM_ERR_INVALID
+ * and the simulation is unchanged.  A corrupt or truncated image:
+ * VLBM_ERR_INVALID; another format version: VLBM_ERR_UNSUPPORTED. */
+vlbm_status vlbm_checkpoint_save(vlbm_sim* sim, void* buf, size_t n, size_t* needed);
+vlbm_status vlbm_checkpoint_load(vlbm_sim* sim, const void* buf, size_t n);
+/* The same image as the file PATH/ID/checkpoint/0_state.bin (the reference's
+ * <gpu>_<name>.bin naming under PATH/ID/checkpoint; folders created as needed,
+ * written to a temporary name and renamed).  Missing file: VLBM_ERR_NOT_FOUND. */
+vlbm_status vlbm_save_checkpoint(vlbm_sim* sim, const char* path_files, const char* id_sim);
+vlbm_status vlbm_load_checkpoint(vlbm_sim* sim, const char* path_files, const char* id_sim);
+
+/* ----------------------------------------------------- data treatment --- */
+/* Report-step data treatment on the device (treatData.cpp:25-89 and stopSim
+ * treatData.cpp:451-460, which copy rho and u to the host and loop in FP32):
+ *   residual = sum |u - u_prev| / sum |u| (1 when sum |u| = 0), u_prev = the
+ *              velocity at the previous call (zero before the first call and
+ *              after vlbm_init_equilibrium / vlbm_set_populations), the
+ *              reference's macrCPUOld (main.cu:430-434);
+ *   avg_rho  = sum rho / N;
+ *   avg_uz_plane_xz[y] = sum over x, z of uz / (NX * NZ), when not NULL (`ny`
+ *              must then be NY); the mean of this call, where the reference's
+ *              avgUzPlanXZ keeps adding every report's mean (never cleared);
+ *   stop     = residual < resid_max || avg_rho < 0 (RESID_MAX, var.h:119: 1e-5).
+ * Sums are FP64 on the device in a fixed order (bit-reproducible); 3 + NY
+ * doubles are copied to the host.  Synchronises the simulation's stream. */
+typedef struct vlbm_treat {
+    int64_t step;
+    double residual;
+    double avg_rho;
+    int32_t stop;
+    int32_t reserved;
+} vlbm_treat;
+vlbm_status vlbm_treat_data(vlbm_sim* sim, double resid_max, vlbm_treat* out, double* avg_uz_plane_xz,
+                            int32_t ny);
+
 /* ------------------------------------------------------------ serving --- */
 typedef struct vlbm_server vlbm_server;
 typedef struct vlbm_request {

@@ -213,6 +213,24 @@ def sphere_mesh(diameter, mesh_scale=1.0):
     return xyz.reshape(3, n), S
 
 
+def treat_data(rho, ux, uy, uz, prev=None, resid_max=1e-5):
+    """Report-step data treatment of treatData.cpp:25-89 and stopSim
+    treatData.cpp:451-460, in FP64: residual = sum |u - u_old| / sum |u|
+    (1 when sum |u| = 0; u_old zero when `prev` is None), avgRho = mean rho,
+    avgUzPlanXZ[y] = mean over x, z of uz for the [z][y][x] fields given (the
+    mean of this report alone: the reference's array is never cleared between
+    reports, macrProc.h:39-40), stop = residual < RESID_MAX or avgRho < 0."""
+    u = np.stack([np.asarray(a, dtype=np.float64) for a in (ux, uy, uz)])
+    old = np.zeros_like(u) if prev is None else np.stack([np.asarray(a, dtype=np.float64) for a in prev])
+    num = np.sqrt(((u - old) ** 2).sum(axis=0)).sum()
+    den = np.sqrt((u ** 2).sum(axis=0)).sum()
+    residual = num / den if den != 0 else 1.0
+    avg_rho = float(np.asarray(rho, dtype=np.float64).mean())
+    avg_uz = u[2].mean(axis=(0, 2))
+    return {"residual": float(residual), "avg_rho": avg_rho, "avg_uz_plane_xz": avg_uz,
+            "stop": bool(residual < resid_max or avg_rho < 0)}
+
+
 # --------------------------------------------------------------------------
 # Literal restatement of the reference builders (node-map words).
 # Bit layout src/CUDA/structs/nodeTypeMap.h:15-133.

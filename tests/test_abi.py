@@ -45,3 +45,13 @@ def test_invalid_config_is_rejected_without_gpu(vlbm):
     st = vlbm.lib().vlbm_create(ctypes.byref(c), ctypes.byref(h))
     assert st == vlbm.ERR_INVALID
     assert b"tau" in vlbm.lib().vlbm_last_error()
+
+
+def test_checkpoint_calls_reject_null_arguments_without_gpu(vlbm):
+    import ctypes
+    L = vlbm.lib()
+    need = ctypes.c_size_t()
+    assert L.vlbm_checkpoint_save(None, None, 0, ctypes.byref(need)) == vlbm.ERR_INVALID
+    assert L.vlbm_checkpoint_load(None, None, 0) == vlbm.ERR_INVALID
+    assert L.vlbm_save_checkpoint(None, None, None) == vlbm.ERR_INVALID
+    assert L.vlbm_load_checkpoint(None, b"/nonexistent", b"x") == vlbm.ERR_INVALID

@@ -54,3 +54,22 @@ def test_bingham_plug_profile(vlbm, oracle):
     core = ux[ny // 2 - 2: ny // 2 + 2]
     assert np.ptp(core) / core.mean() < 2e-2
     assert rel < 0.1, rel
+
+
+def test_treat_data_restatement_on_hand_values(oracle):
+    """treatData.cpp:25-89 on a 2x2x1 lattice worked by hand."""
+    rho = np.array([[[1.0, 1.2], [0.9, 0.9]]])              # [z][y][x]
+    ux = np.array([[[3.0, 0.0], [0.0, 0.0]]])
+    uy = np.array([[[4.0, 0.0], [0.0, 1.0]]])
+    uz = np.array([[[0.0, 2.0], [0.5, 0.5]]])
+    r = oracle.treat_data(rho, ux, uy, uz)
+    assert r["residual"] == 1.0                               # u_old = 0
+    assert abs(r["avg_rho"] - 1.0) < 1e-15
+    np.testing.assert_allclose(r["avg_uz_plane_xz"], [1.0, 0.5])
+    prev = (np.zeros_like(ux), np.zeros_like(uy), uz)         # only uz known before
+    r2 = oracle.treat_data(rho, ux, uy, uz, prev=prev)
+    # |du| = 5, 0, 0, 1 ; |u| = 5, 2, 0.5, sqrt(1.25)
+    assert abs(r2["residual"] - 6.0 / (7.5 + np.sqrt(1.25))) < 1e-15
+    z = np.zeros_like(ux)
+    assert oracle.treat_data(rho, z, z, z)["residual"] == 1.0  # sum |u| = 0
+    assert oracle.treat_data(-rho, ux, uy, uz, resid_max=0.0)["stop"]   # negative mean density

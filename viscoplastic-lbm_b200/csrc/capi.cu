@@ -191,7 +191,7 @@ vlbm_status sim_macroscopics_device(vlbm_sim* s, float* rho, float* ux, float* u
     return VLBM_OK;
 }
 
-static vlbm_status ensure_scratch(vlbm_sim* s) {
+vlbm_status ensure_scratch(vlbm_sim* s) {
     if (s->scratch) return VLBM_OK;
     void* p = nullptr;
     vlbm_status st = alloc_dev(s, &p, (size_t)5 * s->N * sizeof(float));
@@ -207,7 +207,8 @@ using namespace vlbm;
 vlbm_sim::~vlbm_sim() {
     if (ibm) { ibm_destroy(ibm, allocator); ibm = nullptr; }
     for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)bc_node, (void*)side[0], (void*)side[1],
-                    (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch})
+                    (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch,
+                    (void*)treat_prev, (void*)treat_red})
         free_with(allocator, p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -355,6 +356,7 @@ vlbm_status vlbm_init_equilibrium(vlbm_sim* s, double rho, double ux, double uy,
     s->parity = 0;
     s->apply_bc = 0;     // the initial state carries no boundary rule (main.cu:204-213)
     s->step = 0;
+    s->treat_prev_valid = false;
     VLBM_CUDA(sync_step_ctr(s, s->stream));
     if (s->fibm) VLBM_CUDA(cudaMemsetAsync(s->fibm, 0, (size_t)3 * s->N * sizeof(float), s->stream));
     if (s->nbc > 0) { vlbm_status st = fill_side_equilibrium(s); if (st != VLBM_OK) return st; }
@@ -450,6 +452,7 @@ vlbm_status vlbm_set_populations(vlbm_sim* s, const float* pops, size_t n) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     s->parity = 0;
     s->apply_bc = 0;   // given populations already carry their boundary values
+    s->treat_prev_valid = false;
     VLBM_CUDA(sync_step_ctr(s, s->stream));
     return cuda_status(e, "vlbm_set_populations");
 }

@@ -841,6 +841,27 @@ vlbm_status ibm_step(vlbm_sim* s) {
 
 int ibm_iterations(const vlbm_sim* s) { return s->ibm ? s->ibm->cfg.max_iterations : 0; }
 
+uint32_t ibm_record_bytes() { return (uint32_t)sizeof(DPart); }
+
+// The IBM state that carries from one step to the next: particle records
+// (positions, velocities, rotation, forces of the previous step, contact
+// history), Lagrangian nodes, the macroscopics of the touched nodes with their
+// list, and the step clock.  Per-step scratch (spread accumulators, pair and
+// per-CTA partials) is zero or rewritten before it is read, so it is not saved.
+void ibm_state_regions(vlbm_sim* s, std::vector<StateRegion>& out) {
+    IbmState* st = s->ibm;
+    if (!st || st->np == 0) return;
+    const size_t nn = (size_t)st->nnodes, N = (size_t)s->N;
+    out.push_back({100, st->parts, (size_t)st->np * sizeof(DPart)});
+    uint32_t id = 101;
+    for (double* p : {st->nx, st->ny, st->nz, st->nS, st->nfx, st->nfy, st->nfz, st->ndx, st->ndy, st->ndz})
+        out.push_back({id++, p, nn * sizeof(double)});
+    out.push_back({111, st->npid, nn * sizeof(int)});
+    out.push_back({112, st->fields, 4 * N * sizeof(float)});
+    out.push_back({113, st->list, N * sizeof(int)});
+    out.push_back({114, st->count, 2 * sizeof(int)});
+}
+
 void ibm_counts(const vlbm_sim* s, int* np, int* nn) {
     *np = s->ibm ? s->ibm->np : 0;
     *nn = s->ibm ? s->ibm->nnodes : 0;

@@ -52,6 +52,9 @@ struct vlbm_sim {
     unsigned int* step_ctr = nullptr;  // [2] device step count by AA parity
     float* scratch = nullptr;        // [5][N] macroscopic output scratch (lazy)
     double* red_scratch = nullptr;   // FP64 reduction partials + result (lazy)
+    float* treat_prev = nullptr;     // [3][N] velocity of the previous data report (lazy)
+    double* treat_red = nullptr;     // data-report partial sums + results (lazy)
+    bool treat_prev_valid = false;   // false: the previous velocity is zero
     size_t device_bytes = 0;
 
     // host state
@@ -87,12 +90,23 @@ vlbm_status cuda_status(cudaError_t e, const char* what);
 vlbm_status fluid_step(vlbm_sim* s);   // one fused step (no IBM)
 vlbm_status sim_macroscopics_device(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz, float* omega);
 vlbm_status sim_validate_config(const vlbm_config& c, std::string& why);
+// Allocate the [5][N] macroscopic scratch (rho, ux, uy, uz, omega) if needed.
+vlbm_status ensure_scratch(vlbm_sim* s);
 
 // FP64 mass/momentum reduction (reduce.cu)
 int reduce_blocks(long long N);
 cudaError_t launch_moments_sum(vlbm_sim* s, double* partials, double* out);
 
+// A device range that a checkpoint saves and restores (checkpoint.cu).
+struct StateRegion {
+    uint32_t id;
+    void* dev;
+    size_t bytes;
+};
+
 // IBM hooks (ibm.cu)
+void ibm_state_regions(vlbm_sim* s, std::vector<StateRegion>& out);
+uint32_t ibm_record_bytes();   // bytes of one device particle record
 vlbm_status ibm_step(vlbm_sim* s);
 vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz);
 void ibm_destroy(IbmState* st, DeviceAllocator* allocator);

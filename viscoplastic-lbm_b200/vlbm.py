@@ -144,6 +144,11 @@ class Info(C.Structure):
     ]
 
 
+class Treat(C.Structure):
+    _fields_ = [("step", C.c_int64), ("residual", C.c_double), ("avg_rho", C.c_double),
+                ("stop", C.c_int32), ("reserved", C.c_int32)]
+
+
 class Request(C.Structure):
     _fields_ = [
         ("cfg", Config), ("builder", C.c_int32), ("steps", C.c_uint32),
@@ -189,6 +194,11 @@ _SIGS = {
     "vlbm_get_particles": [_P, C.POINTER(ParticleState), C.c_int32],
     "vlbm_get_lagrangian_nodes": [_P, _F64P, _F64P, C.c_size_t],
     "vlbm_write_macr_bin": [_P, C.c_char_p, C.c_char_p, C.c_uint32, C.c_int32],
+    "vlbm_checkpoint_save": [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)],
+    "vlbm_checkpoint_load": [_P, _P, C.c_size_t],
+    "vlbm_save_checkpoint": [_P, C.c_char_p, C.c_char_p],
+    "vlbm_load_checkpoint": [_P, C.c_char_p, C.c_char_p],
+    "vlbm_treat_data": [_P, C.c_double, C.POINTER(Treat), _F64P, C.c_int32],
     "vlbm_server_create": [C.c_int, C.c_size_t, C.c_int32, C.POINTER(_P)],
     "vlbm_server_submit": [_P, C.POINTER(Request)],
     "vlbm_server_pump": [_P, C.c_uint32, C.POINTER(Completion), C.c_int32, C.POINTER(C.c_int32)],
@@ -347,6 +357,35 @@ class Simulation:
     def write_macr_bin(self, path_files, id_sim, step_label, export_forces=False):
         _check(_lib.vlbm_write_macr_bin(self._h, path_files.encode(), id_sim.encode(),
                                         step_label, int(export_forces)), "vlbm_write_macr_bin")
+
+    def checkpoint(self):
+        """The complete state as a uint8 image (vlbm_checkpoint_save)."""
+        need = C.c_size_t()
+        _check(_lib.vlbm_checkpoint_save(self._h, None, 0, C.byref(need)), "vlbm_checkpoint_save")
+        buf = np.empty(need.value, dtype=np.uint8)
+        _check(_lib.vlbm_checkpoint_save(self._h, buf.ctypes.data_as(_P), buf.size, C.byref(need)),
+               "vlbm_checkpoint_save")
+        return buf
+
+    def restore(self, image):
+        """Continue from an image written by checkpoint() (vlbm_checkpoint_load)."""
+        a = np.ascontiguousarray(image, dtype=np.uint8)
+        _check(_lib.vlbm_checkpoint_load(self._h, a.ctypes.data_as(_P), a.size), "vlbm_checkpoint_load")
+
+    def save_checkpoint(self, path_files, id_sim):
+        _check(_lib.vlbm_save_checkpoint(self._h, path_files.encode(), id_sim.encode()), "vlbm_save_checkpoint")
+
+    def load_checkpoint(self, path_files, id_sim):
+        _check(_lib.vlbm_load_checkpoint(self._h, path_files.encode(), id_sim.encode()), "vlbm_load_checkpoint")
+
+    def treat_data(self, resid_max=1e-5):
+        """Report-step residual, mean density, per-plane mean uz and stop flag (vlbm_treat_data)."""
+        t = Treat()
+        prof = np.empty(self.cfg.ny, dtype=np.float64)
+        _check(_lib.vlbm_treat_data(self._h, resid_max, C.byref(t), prof.ctypes.data_as(_F64P), prof.size),
+               "vlbm_treat_data")
+        return {"step": t.step, "residual": t.residual, "avg_rho": t.avg_rho, "stop": bool(t.stop),
+                "avg_uz_plane_xz": prof}
 
     def autotune(self):
         v = C.c_int32()
