@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define VLBM_ABI_VERSION 1
+#define VLBM_ABI_VERSION 2
 
 typedef int vlbm_status;
 enum {
@@ -63,6 +63,12 @@ enum { VLBM_STORE_F32 = 0, VLBM_STORE_F16 = 1, VLBM_STORE_BF16 = 2 };
 #define VLBM_MAP_SCHEME_OFFSET 18
 #define VLBM_MAP_IS_USED_OFFSET 21
 #define VLBM_MAP_SAVE_POST_COL_OFFSET 22
+/* Interpolated bounce-back: unknown in-plane directions, bit d for the D2Q9
+ * direction d of (1,0), (0,1), (-1,0), (0,-1), (1,1), (-1,1), (-1,-1), (1,-1)
+ * (SPC_INTERP_BB_OFFSET, nodeTypeMap.h:98-107); the wall is the inner cylinder
+ * when the direction field is VLBM_SOUTH, the outer one when VLBM_NORTH
+ * (setIsInsideNodeInterpoBB, nodeTypeMap.h:306-319). */
+#define VLBM_MAP_INTERP_BB_OFFSET 23
 
 /* BC schemes (nodeTypeMap.h:35-56) */
 enum {
@@ -93,7 +99,11 @@ enum {
     VLBM_BUILDER_DUCT_YZ = 5,           /* square duct walls y,z, periodic x (serving ducts) */
     VLBM_BUILDER_LID_CAVITY_CLOSED = 6, /* all six faces, moving lid at y=NY-1          */
     VLBM_BUILDER_PLATES_Y_FREE_SLIP = 7,/* bounce-back y=0, free-slip y=NY-1            */
-    VLBM_BUILDER_PLATES_Y_ZOUHE = 8     /* velocity Zou-He at y=0 and y=NY-1 (Couette)  */
+    VLBM_BUILDER_PLATES_Y_ZOUHE = 8,    /* velocity Zou-He at y=0 and y=NY-1 (Couette)  */
+    VLBM_BUILDER_CIRCULAR_DUCT = 9,     /* circularDuctInterpBounceBack.cu: cylinder along z,
+                                           interpolated bounce-back, nodes outside unused */
+    VLBM_BUILDER_ANNULAR_DUCT = 10      /* annularDuctInterpBounceBack.cu: outer and inner
+                                           cylinders along z (INTERNAL_DUCT_BC)           */
 };
 
 typedef struct vlbm_config {
@@ -115,6 +125,16 @@ typedef struct vlbm_config {
     double storage_scale;        /* F16/BF16 deviation scale; 0 = library default   */
     int32_t layout;              /* VLBM_LAYOUT_*: population storage order          */
     int32_t reserved[7];
+    /* Cylindrical ducts (var.h:142-162), axis along z through the lattice centre
+     * (DUCT_CENTER_X/Y).  Radii <= 0 take the var.h values: outer NY/2 - 1.5,
+     * inner outer/4.  Wall motion of the interpolated bounce-back
+     * (interpolatedBounceBack.cu:26-58): axial velocity and angular velocity of
+     * each cylinder; the outer rotation is scaled by z/NZ as in the reference.
+     * vlbm_set_builder uses these radii; vlbm_build_node_map (no configuration)
+     * the var.h values. */
+    double duct_outer_radius, duct_inner_radius;
+    double duct_outer_velocity, duct_outer_rotation;
+    double duct_inner_velocity, duct_inner_rotation;
 } vlbm_config;
 
 /* Population storage order.  NATURAL: planes [Q][z][y][x].  ZPAIR: nodes z and

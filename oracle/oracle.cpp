@@ -430,6 +430,83 @@ void bc_pres_zouhe(OSim& s, std::vector<double>& popS, size_t n, int dir, double
     for (int i = 0; i < 19; ++i) popS[(size_t)i * s.N + n] = g[i];
 }
 
+// Interpolated bounce-back on a cylinder along z, interpolatedBounceBack.cu:6-372
+// (BC_RHEOMETER false, var.h:162).  Node coordinates relative to the axis
+// (x - (NX-1)/2, y - (NY-1)/2); wall velocity from the rotation and axial
+// velocity of the outer (direction NORTH) or inner (SOUTH) cylinder, the outer
+// rotation scaled by z/NZ_TOTAL (:29-58).
+double wall_dist_a0(double x1, double y1, double x2, double y2, double R) {       // :374-389
+    double y = y2, x = std::sqrt(R * R - y * y);
+    if (x2 < 0) x = -x;
+    return std::sqrt((x - x1) * (x - x1) + (y - y1) * (y - y1));
+}
+double wall_dist_ainf(double x1, double y1, double x2, double y2, double R) {     // :392-407
+    double x = x2, y = std::sqrt(R * R - x * x);
+    if (y2 < 0) y = -y;
+    return std::sqrt((x - x1) * (x - x1) + (y - y1) * (y - y1));
+}
+double wall_dist_ap1(double x1, double y1, double x2, double y2, double R) {      // :410-430
+    double b = y1 - x1, dr = std::sqrt(2 * R * R - b * b), x = (-b + dr) * 0.5;
+    if ((x1 > x2 && (x > x1 || x < x2)) || (x1 < x2 && (x < x1 || x > x2))) x = (-b - dr) * 0.5;
+    double y = x + b;
+    return std::sqrt((x - x1) * (x - x1) + (y - y1) * (y - y1)) / std::sqrt(2.0);
+}
+double wall_dist_am1(double x1, double y1, double x2, double y2, double R) {
+    double b = y1 + x1, dr = std::sqrt(2 * R * R - b * b), x = (b + dr) * 0.5;
+    if ((x1 > x2 && (x > x1 || x < x2)) || (x1 < x2 && (x < x1 || x > x2))) x = (b - dr) * 0.5;
+    double y = -x + b;
+    return std::sqrt((x - x1) * (x - x1) + (y - y1) * (y - y1)) / std::sqrt(2.0);
+}
+
+void bc_interp_bounce_back(OSim& s, std::vector<double>& popS, const std::vector<double>& popC, size_t n,
+                           int x, int y, int z, uint32_t m) {
+    const vlbm_config& c = s.cfg;
+    const double R = c.duct_outer_radius > 0 ? c.duct_outer_radius : c.ny / 2.0 - 1.5;
+    const double r = c.duct_inner_radius > 0 ? c.duct_inner_radius : R / 4.0;
+    const bool inside = map_dir(m) == VLBM_SOUTH;
+    const unsigned bits = (m >> VLBM_MAP_INTERP_BB_OFFSET) & 0xFFu;
+    const double xNode = x - (s.nx - 1) / 2.0, yNode = y - (s.ny - 1) / 2.0;
+    const double rr = std::sqrt(xNode * xNode + yNode * yNode);
+    const double cs = xNode / rr, sn = yNode / rr;
+    double ux, uy, uz, radius;
+    if (inside) {
+        radius = r;
+        ux = -c.duct_inner_rotation * r * sn;
+        uy = c.duct_inner_rotation * r * cs;
+        uz = c.duct_inner_velocity;
+    } else {
+        radius = R;
+        const double w_o = c.duct_outer_rotation * ((double)z / (double)s.nz);
+        ux = -w_o * R * sn;
+        uy = w_o * R * cs;
+        uz = c.duct_outer_velocity;
+    }
+    static const int dirs[8][2] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}, {1, 1}, {-1, 1}, {-1, -1}, {1, -1}};
+    for (int d = 0; d < 8; ++d) {
+        if (!((bits >> d) & 1u)) continue;
+        const double x2 = xNode - dirs[d][0], y2 = yNode - dirs[d][1];
+        double q;
+        if (d == 0 || d == 2) q = wall_dist_a0(xNode, yNode, x2, y2, radius);
+        else if (d == 1 || d == 3) q = wall_dist_ainf(xNode, yNode, x2, y2, radius);
+        else if (d == 4 || d == 6) q = wall_dist_ap1(xNode, yNode, x2, y2, radius);
+        else q = wall_dist_am1(xNode, yNode, x2, y2, radius);
+        for (int i = 1; i < s.Q; ++i) {
+            if (CX[i] != dirs[d][0] || CY[i] != dirs[d][1]) continue;
+            const int o = opposite(s.Q, i);
+            const double df = weight(s.Q, i) * (CX[i] * ux + CY[i] * uy + CZ[i] * uz);
+            const double fBound = popC[(size_t)o * s.N + n];
+            double v;
+            if (q > 0.5) {   // gpuInterpolatedBounceBackHigherQ (interpolatedBounceBack.h)
+                v = (0.5 / q) * fBound + ((q - 0.5) / q) * popC[(size_t)i * s.N + n] + 3.0 * df / q;
+            } else {         // gpuInterpolatedBounceBackLowerQ: the opposite at the node x + c_i
+                const size_t na = idx(s, wrapi(x + CX[i], s.nx), wrapi(y + CY[i], s.ny), wrapi(z + CZ[i], s.nz));
+                v = 2 * q * fBound + (1 - 2 * q) * popC[(size_t)o * s.N + na] + 2 * 3.0 * df;
+            }
+            popS[(size_t)i * s.N + n] = v;
+        }
+    }
+}
+
 // gpuBoundaryConditions dispatch, boundaryConditionsHandler.cu:25-79.
 void apply_bc(OSim& s, std::vector<double>& popS, const std::vector<double>& popC, size_t n) {
     uint32_t m = s.map[n];
@@ -446,6 +523,7 @@ void apply_bc(OSim& s, std::vector<double>& popS, const std::vector<double>& pop
         bc_vel_zouhe(s, popS, n, dir, s.cfg.ux_bc[map_ux(m)], s.cfg.uy_bc[map_uy(m)], s.cfg.uz_bc[map_uz(m)]);
         break;
     case VLBM_BC_PRES_ZOUHE: bc_pres_zouhe(s, popS, n, dir, s.cfg.rho_bc[map_rho(m)]); break;
+    case VLBM_BC_INTERP_BOUNCE_BACK: bc_interp_bounce_back(s, popS, popC, n, x, y, z, m); break;
     default: break;
     }
 }
@@ -477,7 +555,7 @@ oracle_sim* oracle_create(const vlbm_config* cfg, const uint32_t* map) {
     // setupBoundaryConditionsInfo (boundaryConditionsInfo.h:76-116): list of
     // nodes whose scheme is not BC_NULL.
     for (size_t n = 0; n < s->N; ++n)
-        if (map_scheme(s->map[n]) != VLBM_BC_NULL) s->bcNodes.push_back(n);
+        if (map_scheme(s->map[n]) != VLBM_BC_NULL && map_used(s->map[n])) s->bcNodes.push_back(n);
     return reinterpret_cast<oracle_sim*>(s);
 }
 
@@ -534,6 +612,14 @@ void oracle_macro(oracle_sim* h, double* rho, double* ux, double* uy, double* uz
 #pragma omp parallel for schedule(static)
     for (long long nn = 0; nn < (long long)s.N; ++nn) {
         size_t n = (size_t)nn;
+        if (!map_used(s.map[n])) {   // never updated: the initial values (lbmInitialization.cu:100-111)
+            if (rho) rho[n] = s.cfg.rho0;
+            if (ux) ux[n] = 0.0;
+            if (uy) uy[n] = 0.0;
+            if (uz) uz[n] = 0.0;
+            if (omega) omega[n] = 0.0;
+            continue;
+        }
         double f[27];
         for (int i = 0; i < s.Q; ++i) f[i] = s.pop[(size_t)i * s.N + n];
         double fx = s.cfg.fx + s.fibm[0][n], fy = s.cfg.fy + s.fibm[1][n], fz = s.cfg.fz + s.fibm[2][n];

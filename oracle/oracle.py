@@ -245,17 +245,18 @@ def _w(scheme, d, ux=0, uz=0):
     return USED | (scheme << SCHEME_OFF) | (d << DIR_OFF) | (ux << UX_OFF) | (uz << UZ_OFF)
 
 
-def reference_builder_map(name, nx, ny, nz):
-    """Node map as the named reference builder writes it ([nz][ny][nx] uint32)."""
+def reference_builder_map(name, nx, ny, nz, outer_radius=None, inner_radius=None):
+    """Node map as the named reference builder writes it ([nz][ny][nx] uint32).
+    The duct builders take OUTER_RADIUS / INNER_RADIUS (default: var.h)."""
     out = np.full((nz, ny, nx), USED, dtype=np.uint32)
     for z in range(nz):
         for y in range(ny):
             for x in range(nx):
-                out[z, y, x] = _builder_word(name, x, y, z, nx, ny, nz)
+                out[z, y, x] = _builder_word(name, x, y, z, nx, ny, nz, outer_radius, inner_radius)
     return out.ravel()
 
 
-def _builder_word(name, x, y, z, NX, NY, NZ):
+def _builder_word(name, x, y, z, NX, NY, NZ, outer_radius=None, inner_radius=None):
     w = USED
     if name == "periodic":
         return w
@@ -322,8 +323,68 @@ def _builder_word(name, x, y, z, NX, NY, NZ):
             if cond:
                 return _w(BB, d)
         return w
+    if name in ("circular_duct", "annular_duct"):
+        return _duct_word(name == "annular_duct", x, y, NX, NY, outer_radius, inner_radius)
     raise KeyError(name)
 
 
+INTERP, IS_SAVE = 6, 1 << 22
+_DIRS8 = [(1, 0), (0, 1), (-1, 0), (0, -1), (1, 1), (-1, 1), (-1, -1), (1, -1)]
+
+
+def _dist2f(x1, y1, x2, y2):
+    """distPoints2D (globalFunctions.h:159-162) with dfloat = float."""
+    f = np.float32
+    dx, dy = f(x1) - f(x2), f(y1) - f(y2)
+    return np.sqrt(f(dx * dx) + f(dy * dy), dtype=np.float32)
+
+
+def _duct_word(annular, x, y, NX, NY, outer_radius=None, inner_radius=None):
+    """circularDuctInterpBounceBack.cu:35-123 / annularDuctInterpBounceBack.cu:35-140
+    (OUTER_RADIUS = NY/2 - 1.5, INNER_RADIUS = OUTER_RADIUS/4, DUCT_CENTER_X/Y,
+    var.h:142-162), in float as the builders compute it."""
+    f = np.float32
+    Rd = outer_radius if outer_radius else NY / 2.0 - 1.5
+    R = f(Rd)
+    r = f(inner_radius if inner_radius else Rd / 4.0)
+    xc, yc = f((NX - 1) / 2.0 + 0.5), f((NY - 1) / 2.0 + 0.5)
+    xn, yn = f(x) + f(0.5), f(y) + f(0.5)
+    dist = _dist2f(xn, yn, xc, yc)
+    s2 = np.sqrt(f(2.0), dtype=np.float32)
+    w = USED | ((F_ << DIR_OFF) if annular else 0)
+    interp = lambda inside: (w & ~((7 << SCHEME_OFF) | (31 << DIR_OFF))) | (INTERP << SCHEME_OFF) | \
+        ((S_ if inside else N_) << DIR_OFF)
+    if not annular:
+        if dist > R:
+            return w & ~USED
+        if dist > f(R - s2):
+            w = interp(False)
+        elif dist > f(R - f(2 * s2)):
+            w |= IS_SAVE
+        else:
+            return w
+    else:
+        if dist > R or dist < r:
+            w &= ~USED
+        elif dist > f(R - s2):
+            w = interp(False)
+        elif dist > f(R - f(2 * s2)):
+            w |= IS_SAVE
+        elif dist < f(r + s2):
+            w = interp(True)
+        elif dist < f(r + f(2 * s2)):
+            w |= IS_SAVE
+    for i, (dx, dy) in enumerate(_DIRS8):
+        xa, ya = f(xn - f(dx)), f(yn - f(dy))
+        unknown = True
+        if xa < NX and xa > 0 and ya < NY and ya > 0:
+            da = _dist2f(xa, ya, xc, yc)
+            unknown = bool(da > R or (annular and da < r))
+        if unknown:
+            w |= (1 << i) << 23
+    return w
+
+
 BUILDER_NAMES = {0: "periodic", 1: "plates_y", 2: "lid_driven", 3: "closed_box", 4: "square_duct",
-                 5: "duct_yz", 6: "lid_cavity_closed", 7: "plates_y_free_slip", 8: "plates_y_zouhe"}
+                 5: "duct_yz", 6: "lid_cavity_closed", 7: "plates_y_free_slip", 8: "plates_y_zouhe",
+                 9: "circular_duct", 10: "annular_duct"}

@@ -35,7 +35,7 @@ def test_config_defaults_match_reference_var_h(vlbm):
     assert c.vel_set == 19 and abs(c.tau - 0.6) < 1e-15 and c.rho0 == 1.0
     assert list(c.ux_bc)[:2] == [0.0, 0.1]            # var.h:114
     assert abs(c.eta_p - 0.3) < 1e-15 and abs(c.yield_stress - 1e-4) < 1e-18  # nnf.h:125-126
-    assert vlbm.lib().vlbm_abi_version() == 1
+    assert vlbm.lib().vlbm_abi_version() == 2
 
 
 def test_invalid_config_is_rejected_without_gpu(vlbm):

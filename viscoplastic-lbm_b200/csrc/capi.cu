@@ -54,6 +54,7 @@ StepParams make_params(vlbm_sim* s) {
     p.cls = s->cls;
     p.bc_slot = s->bc_slot;
     p.bc = s->bc;
+    p.bc_q = s->bc_q;
     p.side_prev = s->side[s->side_cur];
     p.side_next = s->side[s->side_cur ^ 1];
     p.omega = s->omega;
@@ -135,6 +136,13 @@ __global__ void k_scatter_bc(const int32_t* bc_node, int nbc, uint8_t* cls, int3
     bc_slot[n] = s;
 }
 
+// Nodes outside the fluid (map bit IS_USED clear, lbm.cu:23-24).
+__global__ void k_mark_unused(const int32_t* nodes, long long count, uint8_t* cls) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    cls[nodes[k]] = NODE_UNUSED;
+}
+
 static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
     if (s->nbc == 0) return VLBM_OK;
     const long long tot = (long long)s->Q * s->nbc;
@@ -149,11 +157,27 @@ static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
 static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
     VLBM_CUDA(cudaStreamSynchronize(s->stream));
     sim_free(s, s->bc); sim_free(s, s->side[0]); sim_free(s, s->side[1]); sim_free(s, s->bc_node);
-    s->bc = nullptr; s->side[0] = s->side[1] = nullptr; s->bc_node = nullptr;
+    sim_free(s, s->bc_q);
+    s->bc = nullptr; s->side[0] = s->side[1] = nullptr; s->bc_node = nullptr; s->bc_q = nullptr;
     s->nbc = (int)t.recs.size();
     const size_t N = (size_t)s->N;
     VLBM_CUDA(cudaMemsetAsync(s->cls, 0, (N + 3) & ~(size_t)3, s->stream));
     VLBM_CUDA(cudaMemsetAsync(s->bc_slot, 0xff, N * sizeof(int32_t), s->stream));
+    if (!t.unused_nodes.empty()) {
+        const long long cnt = (long long)t.unused_nodes.size();
+        void* d = nullptr;
+        VLBM_CUDA(cudaMallocAsync(&d, (size_t)cnt * sizeof(int32_t), s->stream));
+        cudaError_t e = cudaMemcpyAsync(d, t.unused_nodes.data(), (size_t)cnt * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) {
+            k_mark_unused<<<(unsigned)((cnt + 255) / 256), 256, 0, s->stream>>>(static_cast<const int32_t*>(d), cnt,
+                                                                               s->cls);
+            e = cudaGetLastError();
+        }
+        cudaFreeAsync(d, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);   // before the host list goes away
+        VLBM_CUDA(e);
+    }
     if (s->nbc > 0) {
         void* p;
         vlbm_status st;
@@ -169,6 +193,12 @@ static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
                                   s->stream));
         VLBM_CUDA(cudaMemcpyAsync(s->bc_node, t.bc_nodes.data(), t.bc_nodes.size() * sizeof(int32_t),
                                   cudaMemcpyHostToDevice, s->stream));
+        if (!t.q8.empty()) {
+            if ((st = alloc_dev(s, &p, t.q8.size() * sizeof(float))) != VLBM_OK) return st;
+            s->bc_q = static_cast<float*>(p);
+            VLBM_CUDA(cudaMemcpyAsync(s->bc_q, t.q8.data(), t.q8.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                      s->stream));
+        }
         k_scatter_bc<<<(s->nbc + 255) / 256, 256, 0, s->stream>>>(s->bc_node, s->nbc, s->cls, s->bc_slot);
         VLBM_CUDA(cudaGetLastError());
         if ((st = fill_side_equilibrium(s)) != VLBM_OK) return st;   // synchronises the stream
@@ -207,7 +237,7 @@ using namespace vlbm;
 vlbm_sim::~vlbm_sim() {
     if (ibm) { ibm_destroy(ibm, allocator); ibm = nullptr; }
     for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)bc_node, (void*)side[0], (void*)side[1],
-                    (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch,
+                    (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch, (void*)bc_q,
                     (void*)treat_prev, (void*)treat_red})
         free_with(allocator, p);
     if (own_stream && stream) cudaStreamDestroy(stream);

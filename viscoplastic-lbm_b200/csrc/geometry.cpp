@@ -8,6 +8,7 @@
 // of each boundary slot; the class bytes and slot indices are scattered on the
 // device.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -73,6 +74,70 @@ int dir_normals(int dir, int nrm[3][3]) {
     return k;
 }
 
+// Cylinder of the duct builders (var.h:142-162): radii (<= 0: the var.h
+// values OUTER_RADIUS = NY/2 - 1.5, INNER_RADIUS = OUTER_RADIUS/4) and the
+// centre DUCT_CENTER_X/Y in the builders' node coordinates x + 0.5, as the
+// builders hold them (dfloat = float).
+struct Duct {
+    float R, r, cx, cy;
+};
+Duct duct_of(int nx, int ny, double outer, double inner) {
+    Duct d;
+    const double R = outer > 0 ? outer : ny / 2.0 - 1.5;
+    d.R = (float)R;
+    d.r = (float)(inner > 0 ? inner : R / 4.0);
+    d.cx = (float)((nx - 1) / 2.0 + 0.5);
+    d.cy = (float)((ny - 1) / 2.0 + 0.5);
+    return d;
+}
+
+// distPoints2D (globalFunctions.h:159-162) in float.
+float dist2f(float x1, float y1, float x2, float y2) {
+    const float dx = x1 - x2, dy = y1 - y2;
+    const float s = dx * dx + dy * dy;
+    return std::sqrt(s);
+}
+
+// Word of node (x, y) of circularDuctInterpBounceBack.cu:35-123 (annular:
+// annularDuctInterpBounceBack.cu:35-140); the cross-section is the same in
+// every z plane.
+uint32_t duct_word(bool annular, int x, int y, int nx, int ny, const Duct& d) {
+    // used, no post-collision save, BC_NULL, CONCAVE, value indices 0; the
+    // annular builder also sets the direction FRONT on every node
+    uint32_t w = make_word(VLBM_BC_NULL, annular ? VLBM_FRONT : 0);
+    const float xNode = (float)x + 0.5f, yNode = (float)y + 0.5f;
+    const float dist = dist2f(xNode, yNode, d.cx, d.cy);
+    const float s2 = std::sqrt(2.0f);
+    auto set_interp = [&](bool inside) {
+        w &= ~((7u << VLBM_MAP_SCHEME_OFFSET) | (31u << VLBM_MAP_DIRECTION_OFFSET));
+        w |= (uint32_t)VLBM_BC_INTERP_BOUNCE_BACK << VLBM_MAP_SCHEME_OFFSET;
+        w |= (uint32_t)(inside ? VLBM_SOUTH : VLBM_NORTH) << VLBM_MAP_DIRECTION_OFFSET;
+    };
+    const uint32_t save = 1u << VLBM_MAP_SAVE_POST_COL_OFFSET;
+    if (!annular) {
+        if (dist > d.R) return w & ~(1u << VLBM_MAP_IS_USED_OFFSET);
+        if (dist > d.R - s2) set_interp(false);
+        else if (dist > d.R - 2 * s2) w |= save;
+        else return w;
+    } else {
+        if (dist > d.R || dist < d.r) w &= ~(1u << VLBM_MAP_IS_USED_OFFSET);
+        else if (dist > d.R - s2) set_interp(false);
+        else if (dist > d.R - 2 * s2) w |= save;
+        else if (dist < d.r + s2) set_interp(true);
+        else if (dist < d.r + 2 * s2) w |= save;
+    }
+    for (int i = 0; i < 8; ++i) {   // unknown: the node the population comes from is outside
+        const float xa = xNode - (float)kInterpDirs[i][0], ya = yNode - (float)kInterpDirs[i][1];
+        bool unknown = true;
+        if (xa < (float)nx && xa > 0.f && ya < (float)ny && ya > 0.f) {
+            const float da = dist2f(xa, ya, d.cx, d.cy);
+            unknown = da > d.R || (annular && da < d.r);
+        }
+        if (unknown) w |= (1u << i) << VLBM_MAP_INTERP_BB_OFFSET;
+    }
+    return w;
+}
+
 }  // namespace
 
 // Half-way bounce-back roles (bounceBack.cu:26-498, derived): a population
@@ -93,7 +158,8 @@ int bb_role(int dir, int i) {
 
 // Word of node (x, y, z) for a named builder; false for an unknown builder id.
 // Only nodes on the domain faces get a non-bulk word.
-bool builder_word(int builder, int x, int y, int z, int nx, int ny, int nz, uint32_t& w) {
+bool builder_word(int builder, int x, int y, int z, int nx, int ny, int nz, uint32_t& w, double outer_radius,
+                  double inner_radius) {
     w = make_word(VLBM_BC_NULL, 0);
     int d;
     switch (builder) {
@@ -133,6 +199,11 @@ bool builder_word(int builder, int x, int y, int z, int nx, int ny, int nz, uint
         else
             w = make_word(VLBM_BC_BOUNCE_BACK, d);
         break;
+    case VLBM_BUILDER_CIRCULAR_DUCT:
+    case VLBM_BUILDER_ANNULAR_DUCT:
+        w = duct_word(builder == VLBM_BUILDER_ANNULAR_DUCT, x, y, nx, ny,
+                      duct_of(nx, ny, outer_radius, inner_radius));
+        break;
     default:
         return false;
     }
@@ -141,10 +212,86 @@ bool builder_word(int builder, int x, int y, int z, int nx, int ny, int nz, uint
 
 namespace {
 
+// A node gets a boundary slot when its word names a scheme.  SAVE_POST_COL
+// alone asks the reference to keep post-collision populations for a
+// neighbour's rule; here those arrive with the streamed populations (the
+// interpolated bounce-back reads them at gather time), so no slot is needed.
 bool needs_slot(uint32_t m) {
-    const int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
-    const bool save = (m >> VLBM_MAP_SAVE_POST_COL_OFFSET) & 1u;
-    return scheme != VLBM_BC_NULL || save;
+    if (!((m >> VLBM_MAP_IS_USED_OFFSET) & 1u)) return false;
+    return ((m >> VLBM_MAP_SCHEME_OFFSET) & 7) != VLBM_BC_NULL;
+}
+
+// Normalised wall distance along a link (interpolatedBounceBack.cu:374-431,
+// gpuDistNormalizedFromNodePopulationToWall_*), in double.  (x1, y1): the
+// node, (x2, y2): the node the population comes from, R: the cylinder radius;
+// coordinates relative to the duct axis.
+double wall_a0(double x1, double y1, double x2, double y2, double R) {   // horizontal link
+    const double y = y2;
+    double x = std::sqrt(R * R - y * y);
+    if (x2 < 0) x = -x;
+    return std::sqrt((x - x1) * (x - x1) + (y - y1) * (y - y1));
+}
+double wall_ainf(double x1, double y1, double x2, double y2, double R) {   // vertical link
+    const double x = x2;
+    double y = std::sqrt(R * R - x * x);
+    if (y2 < 0) y = -y;
+    return std::sqrt((x - x1) * (x - x1) + (y - y1) * (y - y1));
+}
+double wall_diag(double x1, double y1, double x2, double y2, double R, bool slope_up) {   // _ap1 / _am1
+    const double b = slope_up ? y1 - x1 : y1 + x1;
+    const double dr = std::sqrt(2 * R * R - b * b);
+    double x = slope_up ? (-b + dr) * 0.5 : (b + dr) * 0.5;
+    if ((x1 > x2 && (x > x1 || x < x2)) || (x1 < x2 && (x < x1 || x > x2)))
+        x = slope_up ? (-b - dr) * 0.5 : (b - dr) * 0.5;
+    const double y = slope_up ? x + b : -x + b;
+    return std::sqrt((x - x1) * (x - x1) + (y - y1) * (y - y1)) / std::sqrt(2.0);
+}
+
+// Record of an interpolated bounce-back node (interpolatedBounceBack.cu:6-372):
+// unknown populations from the in-plane direction bits; per direction the
+// coefficients (A, B, K) of f_i = A f*_o + B (f*_i or f_o) + K w_i (c_i . u_w),
+// (1/(2q), (q-1/2)/q, 3/q) with f*_i where q > 1/2
+// (gpuInterpolatedBounceBackHigherQ), (2q, 1-2q, 6) with the streamed f_o
+// otherwise (LowerQ), interpolatedBounceBack.h; and the wall velocity at the
+// node: rotation about the axis plus axial velocity (the outer rotation grows
+// with z/NZ as in the reference).
+void interp_record(const vlbm_config& cfg, int x, int y, int z, uint32_t m, BcRec& r, float* coef /* [8][3] */) {
+    const int Q = cfg.vel_set;
+    const double R = cfg.duct_outer_radius > 0 ? cfg.duct_outer_radius : cfg.ny / 2.0 - 1.5;
+    const double ri = cfg.duct_inner_radius > 0 ? cfg.duct_inner_radius : R / 4.0;
+    const int dir = (m >> VLBM_MAP_DIRECTION_OFFSET) & 31;
+    const bool inside = dir == VLBM_SOUTH;
+    const unsigned bits = (m >> VLBM_MAP_INTERP_BB_OFFSET) & 0xFFu;
+    const double xn = x - (cfg.nx - 1) / 2.0, yn = y - (cfg.ny - 1) / 2.0;
+    const double rad = inside ? ri : R;
+    std::memset(&r, 0, sizeof(r));
+    r.scheme = K_BC_INTERP;
+    r.dir = (uint8_t)dir;
+    for (int i = 1; i < Q; ++i) {
+        const int d = interp_dir_of(lat_cx(i), lat_cy(i));
+        if (d >= 0 && ((bits >> d) & 1u)) r.mask |= 1u << i;
+    }
+    for (int d = 0; d < 8; ++d) {
+        double A = 0.0, B = 0.0, K = 0.0;
+        if ((bits >> d) & 1u) {
+            const double x2 = xn - kInterpDirs[d][0], y2 = yn - kInterpDirs[d][1];
+            double q;
+            if (d == 0 || d == 2) q = wall_a0(xn, yn, x2, y2, rad);
+            else if (d == 1 || d == 3) q = wall_ainf(xn, yn, x2, y2, rad);
+            else q = wall_diag(xn, yn, x2, y2, rad, d == 4 || d == 6);
+            if (q > 0.5) { A = 0.5 / q; B = (q - 0.5) / q; K = 3.0 / q; r.pad |= (uint8_t)(1u << d); }
+            else { A = 2 * q; B = 1 - 2 * q; K = 6.0; }
+        }
+        coef[3 * d] = (float)A;
+        coef[3 * d + 1] = (float)B;
+        coef[3 * d + 2] = (float)K;
+    }
+    const double rr = std::sqrt(xn * xn + yn * yn);
+    const double c = rr > 0 ? xn / rr : 0.0, s = rr > 0 ? yn / rr : 0.0;
+    const double w = inside ? cfg.duct_inner_rotation : cfg.duct_outer_rotation * ((double)z / (double)cfg.nz);
+    r.uw[0] = (float)(-w * rad * s);
+    r.uw[1] = (float)(w * rad * c);
+    r.uw[2] = (float)(inside ? cfg.duct_inner_velocity : cfg.duct_outer_velocity);
 }
 
 // Boundary records from the candidate nodes (node index, map word) of the
@@ -197,8 +344,19 @@ vlbm_status tables_from_candidates(const vlbm_config& cfg, std::vector<std::pair
     uint32_t last_word = 0;
     BcRec last{};
     bool have_last = false;
+    out.q8.clear();
     for (const auto& kw : cand) {
         const uint32_t m = kw.second;
+        if (((m >> VLBM_MAP_SCHEME_OFFSET) & 7) == VLBM_BC_INTERP_BOUNCE_BACK) {   // per-node record
+            const size_t k = kw.first;
+            if (out.q8.empty()) out.q8.assign(24 * cand.size(), 0.f);
+            BcRec r;
+            interp_record(cfg, (int)(k % nx), (int)((k / nx) % ny), (int)(k / ((size_t)nx * ny)), m, r,
+                          out.q8.data() + 24 * out.recs.size());
+            out.recs.push_back(r);
+            out.bc_nodes.push_back((int32_t)k);
+            continue;
+        }
         if (!have_last || m != last_word) {   // the record depends on the word only
             const int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
             const int dir = (m >> VLBM_MAP_DIRECTION_OFFSET) & 31;
@@ -253,15 +411,16 @@ vlbm_status build_bc_tables(const vlbm_config& cfg, const uint32_t* map, size_t 
     const size_t N = (size_t)cfg.nx * cfg.ny * cfg.nz;
     if (n != N) { err = "node map size does not match nx*ny*nz"; return VLBM_ERR_INVALID; }
     std::vector<std::pair<size_t, uint32_t>> cand;
+    out.unused_nodes.clear();
     for (size_t k = 0; k < N; ++k) {
         const uint32_t m = map[k];
-        if (!((m >> VLBM_MAP_IS_USED_OFFSET) & 1u)) {
-            err = "nodes marked unused (interpolated-bounce-back duct builders) are not supported";
-            return VLBM_ERR_UNSUPPORTED;
+        if (!((m >> VLBM_MAP_IS_USED_OFFSET) & 1u)) {   // lbm.cu:23-24
+            out.unused_nodes.push_back((int32_t)k);
+            continue;
         }
         const int scheme = (m >> VLBM_MAP_SCHEME_OFFSET) & 7;
-        if (scheme == VLBM_BC_INTERP_BOUNCE_BACK || scheme == VLBM_BC_SPECIAL) {
-            err = "interpolated bounce-back and builder-specific (SPECIAL) schemes are not supported";
+        if (scheme == VLBM_BC_SPECIAL) {
+            err = "builder-specific (SPECIAL) schemes are not supported";
             return VLBM_ERR_UNSUPPORTED;
         }
         if (needs_slot(m)) cand.emplace_back(k, m);
@@ -275,11 +434,30 @@ vlbm_status build_bc_tables_builder(const vlbm_config& cfg, int builder, BcTable
     if (!builder_word(builder, 0, 0, 0, nx, ny, nz, w)) { err = "unknown builder id"; return VLBM_ERR_NOT_FOUND; }
     auto word_at = [&](size_t k) {
         uint32_t m;
-        builder_word(builder, (int)(k % nx), (int)((k / nx) % ny), (int)(k / ((size_t)nx * ny)), nx, ny, nz, m);
+        builder_word(builder, (int)(k % nx), (int)((k / nx) % ny), (int)(k / ((size_t)nx * ny)), nx, ny, nz, m,
+                     cfg.duct_outer_radius, cfg.duct_inner_radius);
         return m;
     };
-    // the builders mark domain-face nodes only: visit the six faces
     std::vector<std::pair<size_t, uint32_t>> cand;
+    out.unused_nodes.clear();
+    if (builder == VLBM_BUILDER_CIRCULAR_DUCT || builder == VLBM_BUILDER_ANNULAR_DUCT) {
+        // the cross-section is the same in every plane: classify one, repeat it along z
+        std::vector<std::pair<int, uint32_t>> plane_cand;
+        std::vector<int> plane_unused;
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const uint32_t m = word_at((size_t)nx * y + x);
+                if (!((m >> VLBM_MAP_IS_USED_OFFSET) & 1u)) plane_unused.push_back(nx * y + x);
+                else if (needs_slot(m)) plane_cand.emplace_back(nx * y + x, m);
+            }
+        const size_t plane = (size_t)nx * ny;
+        for (int z = 0; z < nz; ++z) {
+            for (const auto& pc : plane_cand) cand.emplace_back(plane * z + pc.first, pc.second);
+            for (int u : plane_unused) out.unused_nodes.push_back((int32_t)(plane * z + u));
+        }
+        return tables_from_candidates(cfg, cand, word_at, out);
+    }
+    // the other builders mark domain-face nodes only: visit the six faces
     auto visit = [&](int x, int y, int z) {
         uint32_t m;
         builder_word(builder, x, y, z, nx, ny, nz, m);

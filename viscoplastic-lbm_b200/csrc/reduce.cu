@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_moment_partials(const StepPa
         float f[Q];
         uint8_t cls;
         gather<Q, ST, ODD, PAIRED>(p, n, nb, x, y, z, f, cls);
+        if (cls & NODE_UNUSED) continue;   // outside the fluid
         // the gather gives deviations g_i = f_i - w_i rho0
         double rho = (double)p.rho0, jx = 0.5 * p.fx, jy = 0.5 * p.fy, jz = 0.5 * p.fz;
 #pragma unroll

@@ -43,6 +43,7 @@ struct vlbm_sim {
     int32_t* bc_slot = nullptr;      // [N]
     vlbm::BcRec* bc = nullptr;       // [nbc]
     int32_t* bc_node = nullptr;      // [nbc] node index of each boundary slot
+    float* bc_q = nullptr;           // [nbc][8][3] interpolated bounce-back coefficients (or null)
     float* side[2] = {nullptr, nullptr};  // [Q][nbc] post-collision at boundary nodes
     int nbc = 0;
     int pairH = 0;                   // z-paired layout (NZ/2) or 0

@@ -333,6 +333,32 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, con
             for (int i = 0; i < Q; ++i) f[i] -= Lattice<Q>::w(i) * p.rho0;
         }
         break;
+    case K_BC_INTERP: {
+        // interpolatedBounceBack.cu:6-372.  For an unknown population i whose
+        // link crosses the wall at normalised distance q from the node:
+        //   q > 1/2:  f_i = f*_o / (2q) + (q - 1/2)/q f*_i + 3 w_i (c_i . u_w) / q
+        //   q <= 1/2: f_i = 2q f*_o + (1 - 2q) f_o + 6 w_i (c_i . u_w)
+        // with o the opposite, f* this node's post-collision values (side
+        // store) and f_o the streamed opposite, i.e. the post-collision value
+        // of the node one link inward (the reference reads it from its
+        // post-collision array at x + c_i).  The host stores per in-plane
+        // direction d the coefficients (A, B, K), and in r.pad the directions
+        // with q > 1/2, so the rule is two FMAs without a division.  The rules
+        // are affine with weights summing to one and w_o = w_i, so they hold for
+        // deviations as written.
+        const float* cf = p.bc_q + (size_t)slot * 24;
+#pragma unroll
+        for (int i = 1; i < Q; ++i) {
+            const int d = interp_dir_of(lat_cx(i), lat_cy(i));
+            if (d < 0 || !((r.mask >> i) & 1u)) continue;
+            const int o = lat_opp(i);
+            const float so = side_prev[(size_t)o * nbc + slot];
+            const float other = ((r.pad >> d) & 1u) ? side_prev[(size_t)i * nbc + slot] : f[o];
+            const float cu = lat_cx(i) * r.uw[0] + lat_cy(i) * r.uw[1] + lat_cz(i) * r.uw[2];
+            f[i] = cf[3 * d] * so + cf[3 * d + 1] * other + cf[3 * d + 2] * (Lattice<Q>::w(i) * cu);
+        }
+        break;
+    }
     default: break;
     }
     (void)x; (void)y; (void)z;
@@ -580,7 +606,7 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, float* si
     }
     constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
     const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz, p.rho0);
-    if (!(m.rho > 0.f && m.rho < 1e30f)) atomicOr(p.err, 1u);
+    if (!(m.rho > 0.f && m.rho < 1e30f) && !(cls & NODE_UNUSED)) atomicOr(p.err, 1u);
     float omega = p.omega_newt;
     if (RHEO != VLBM_NEWTONIAN) {
         const float aux = stress_aux(m, fx, fy, fz);
@@ -590,6 +616,10 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, float* si
         if (RHEO == VLBM_POWERLAW) p.omega[n] = eta;  // state update, lbm.cu:215-219
     }
     collide<Q, OP>(f, m, omega, fx, fy, fz);
+    if (cls & NODE_UNUSED) {   // lbm.cu:23-24: not updated; rest equilibrium stays in its slots
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = 0.f;
+    }
     if (slot >= 0) {
         const size_t nbc = (size_t)p.nbc;
 #pragma unroll
@@ -752,6 +782,14 @@ __global__ void __launch_bounds__(256) k_macro(const MacroParams mp) {
     if (mp.fibm_const) {
         const size_t N = (size_t)p.N;
         fx += mp.fibm_const[n]; fy += mp.fibm_const[N + n]; fz += mp.fibm_const[2 * N + n];
+    }
+    if (cls & NODE_UNUSED) {   // never updated: the initial macroscopics (lbmInitialization.cu:100-111)
+        if (mp.rho) mp.rho[n] = p.rho0;
+        if (mp.ux) mp.ux[n] = 0.f;
+        if (mp.uy) mp.uy[n] = 0.f;
+        if (mp.uz) mp.uz[n] = 0.f;
+        if (mp.omega_out) mp.omega_out[n] = 0.f;
+        return;
     }
     constexpr bool NEED_PI = RHEO != VLBM_NEWTONIAN;
     const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz, p.rho0);
@@ -969,7 +1007,9 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
     }
     constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
     const Mom2 mm = moments2<Q, NEED_PI>(g, fx2, fy2, fz2, p.rho0);
-    if (!(mm.rho.x > 0.f && mm.rho.x < 1e30f) || !(mm.rho.y > 0.f && mm.rho.y < 1e30f)) atomicOr(p.err, 1u);
+    if ((!(mm.rho.x > 0.f && mm.rho.x < 1e30f) && !(c0 & NODE_UNUSED)) ||
+        (!(mm.rho.y > 0.f && mm.rho.y < 1e30f) && !(c1 & NODE_UNUSED)))
+        atomicOr(p.err, 1u);
     float2 omega = f2(p.omega_newt);
     if (RHEO != VLBM_NEWTONIAN) {
         const float2 aux = stress_aux2(mm, fx2, fy2, fz2);
@@ -983,6 +1023,14 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
         }
     }
     collide2<Q, OP>(g, mm, omega, fx2, fy2, fz2);
+    if ((c0 | c1) & NODE_UNUSED) {   // lbm.cu:23-24: not updated; rest equilibrium stays in the slots
+        const bool u0 = c0 & NODE_UNUSED, u1 = c1 & NODE_UNUSED;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            if (u0) g[i].x = 0.f;
+            if (u1) g[i].y = 0.f;
+        }
+    }
     if (slot0 >= 0 || slot1 >= 0) {   // post-collision values of boundary nodes (lbm.cu:463-470)
         const size_t nbc = (size_t)p.nbc;
 #pragma unroll

@@ -31,14 +31,15 @@ STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
 LAYOUT_AUTO, LAYOUT_NATURAL, LAYOUT_ZPAIR = 0, 1, 2
 (BUILDER_PERIODIC, BUILDER_PLATES_Y, BUILDER_LID_DRIVEN, BUILDER_CLOSED_BOX,
  BUILDER_SQUARE_DUCT, BUILDER_DUCT_YZ, BUILDER_LID_CAVITY_CLOSED,
- BUILDER_PLATES_Y_FREE_SLIP, BUILDER_PLATES_Y_ZOUHE) = range(9)
+ BUILDER_PLATES_Y_FREE_SLIP, BUILDER_PLATES_Y_ZOUHE, BUILDER_CIRCULAR_DUCT,
+ BUILDER_ANNULAR_DUCT) = range(11)
 BC_NULL, BC_VEL_ZOUHE, BC_VEL_BOUNCE_BACK, BC_PRES_ZOUHE, BC_FREE_SLIP, \
     BC_BOUNCE_BACK, BC_INTERP_BOUNCE_BACK, BC_SPECIAL = range(8)
 DIRECTIONS = ["N", "S", "W", "E", "F", "B", "NW", "NE", "NF", "NB", "SW", "SE", "SF", "SB",
               "WF", "WB", "EF", "EB", "NWF", "NWB", "NEF", "NEB", "SWF", "SWB", "SEF", "SEB"]
 MAP_RHO_IDX_OFFSET, MAP_UZ_IDX_OFFSET, MAP_UY_IDX_OFFSET, MAP_UX_IDX_OFFSET = 0, 3, 6, 9
 MAP_GEOMETRY_OFFSET, MAP_DIRECTION_OFFSET, MAP_SCHEME_OFFSET = 12, 13, 18
-MAP_IS_USED_OFFSET, MAP_SAVE_POST_COL_OFFSET = 21, 22
+MAP_IS_USED_OFFSET, MAP_SAVE_POST_COL_OFFSET, MAP_INTERP_BB_OFFSET = 21, 22, 23
 
 
 class VlbmError(RuntimeError):
@@ -64,6 +65,9 @@ class Config(C.Structure):
         ("storage_scale", C.c_double),
         ("layout", C.c_int32),
         ("reserved", C.c_int32 * 7),
+        ("duct_outer_radius", C.c_double), ("duct_inner_radius", C.c_double),
+        ("duct_outer_velocity", C.c_double), ("duct_outer_rotation", C.c_double),
+        ("duct_inner_velocity", C.c_double), ("duct_inner_rotation", C.c_double),
     ]
 
     @classmethod
