@@ -176,6 +176,44 @@ def storage_accuracy(vlbm, steps=6000, nxz=8):
     return out
 
 
+def cube_leg(vlbm, torch, device, steps=200, warmup=10, n=256):
+    """Regularized Bingham channel at n^3 for D3Q19 and D3Q27 with FP32 and FP16
+    storage (AUTO layout, autotuned launch): MLUPS, algorithmic GB/s and the
+    fraction of the measured copy bandwidth, timed with CUDA events over
+    `steps` steps (the population arrays, 0.6-1.8 GB, exceed the 126 MB L2)."""
+    peak, _ = measured_peak()
+    out = {"lattice": f"{n}x{n}x{n}", "steps": steps,
+           "case": "regularized Bingham, tau_p 0.8, yield 1e-5, gx 5e-6, walls y, periodic x,z"}
+    for q in (19, 27):
+        for name, st in (("f32", vlbm.STORE_F32), ("f16", vlbm.STORE_F16)):
+            cfg = vlbm.Config.default(nx=n, ny=n, nz=n, vel_set=q, collision=vlbm.OP_REGULARIZED,
+                                      rheology=vlbm.BINGHAM, eta_p=0.1, yield_stress=1e-5, fx=5e-6, storage=st)
+            cfg.device = device
+            sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+            stream = torch.cuda.Stream()
+            sim.set_stream(stream.cuda_stream)
+            sim.autotune()
+            sim.init_equilibrium(1.0, 0, 0, 0)
+            sim.step(warmup)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.step(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sim.sync()
+            ms = e0.elapsed_time(e1)
+            nodes = n ** 3
+            bpn = sim.info().bytes_per_node_step
+            mlups = nodes * steps / (ms / 1e3) / 1e6
+            gbs = bpn * mlups * 1e6 / 1e9
+            out[f"d3q{q}_{name}"] = {"mlups": mlups, "achieved_gbs": gbs, "frac": gbs / peak,
+                                     "bytes_per_node": bpn, "variant": sim.info().last_kernel_variant}
+            sim.close()
+        out[f"d3q{q}_f16_over_f32"] = out[f"d3q{q}_f16"]["mlups"] / out[f"d3q{q}_f32"]["mlups"]
+    return out
+
+
 def serving_requests(vlbm, n, step_scale, seed=2024):
     """A seeded sample of the Bingham-duct serving stream.
 
@@ -334,6 +372,7 @@ def main():
     ap.add_argument("--layout", default="auto", choices=["auto", "natural", "zpair"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 D3Q19/D3Q27 FP32/FP16 leg")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-step-scale", type=float, default=0.25)
     ap.add_argument("--serving-rate", type=float, default=200.0)
@@ -430,6 +469,9 @@ def main():
     accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         accuracy = storage_accuracy(vlbm)
+    cube = None
+    if rank == 0 and world == 1 and not args.no_cube:
+        cube = cube_leg(vlbm, torch, local)
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_leg(vlbm, args.serving_requests, args.serving_step_scale, args.serving_rate)
@@ -454,6 +496,7 @@ def main():
             "kernel_variant": variant,
             "clocks": clk,
             "storage_accuracy": accuracy,
+            "lattice_256": cube,
             "serving": serving,
         }
         print(json.dumps(line), flush=True)
