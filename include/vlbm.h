@@ -122,7 +122,7 @@ typedef struct vlbm_config {
     double k_consistency;        /* nnf.h:117 K_CONSISTENCY                         */
     double gamma0;               /* nnf.h:118 GAMMA_0 (truncation)                  */
     double ux_bc[8], uy_bc[8], uz_bc[8], rho_bc[8]; /* var.h:114-117 UX_BC..RHO_BC */
-    double storage_scale;        /* F16/BF16 deviation scale; 0 = library default   */
+    double storage_scale;        /* F16/BF16 deviation scale; 0 = library default (F16: a power of two 1..2^24) */
     int32_t layout;              /* VLBM_LAYOUT_*: population storage order          */
     int32_t reserved[7];
     /* Cylindrical ducts (var.h:142-162), axis along z through the lattice centre

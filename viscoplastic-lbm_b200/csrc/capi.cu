@@ -43,6 +43,11 @@ vlbm_status sim_validate_config(const vlbm_config& c, std::string& why) {
     if (c.rheology == VLBM_BINGHAM && !(c.eta_p > 0.0 && c.yield_stress >= 0.0)) { why = "Bingham needs eta_p > 0, yield_stress >= 0"; return VLBM_ERR_INVALID; }
     if (c.rheology == VLBM_POWERLAW && !(c.n_index > 0.0 && c.k_consistency > 0.0)) { why = "Power-Law needs n_index > 0, k_consistency > 0"; return VLBM_ERR_INVALID; }
     if (!(c.rho0 > 0.0)) { why = "rho0 must be > 0"; return VLBM_ERR_INVALID; }
+    if (c.storage == VLBM_STORE_F16 && c.storage_scale > 0) {   // 2^k, 0 <= k <= 24
+        int e = 0;
+        const double m = std::frexp(c.storage_scale, &e);
+        if (m != 0.5 || e < 1 || e > 25) { why = "FP16 storage_scale must be a power of two from 1 to 2^24"; return VLBM_ERR_INVALID; }
+    }
     return VLBM_OK;
 }
 

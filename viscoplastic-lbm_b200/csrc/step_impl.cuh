@@ -893,12 +893,17 @@ template <> struct Pair<VLBM_STORE_F16> {
         return mul2(__half22float2(v), f2(s.inv_scale));
     }
     // both lanes rounded stochastically (13 random bits each, two slices of one
-    // draw) and packed with one conversion
+    // draw) and packed with one conversion.  The FP16 scale is 2^k with
+    // 0 <= k <= 24 (checked at creation), so g * scale is k added to the
+    // exponent field: one integer add carries both the scaling and the random
+    // bits.  Identical to multiplying first for every finite g: a normal g
+    // stays normal, and zero or subnormal g becomes a float far below the
+    // smallest half, which the conversion rounds to a signed zero as before.
     static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
-        const float2 v = mul2(g, f2(s.scale));
+        const unsigned k23 = __float_as_uint(s.scale) - 0x3F800000u;   // k << 23
         const unsigned r = r0.next();
-        const float lo = __uint_as_float(__float_as_uint(v.x) + (r >> 19));
-        const float hi = __uint_as_float(__float_as_uint(v.y) + ((r >> 6) & 0x1FFFu));
+        const float lo = __uint_as_float(__float_as_uint(g.x) + k23 + (r >> 19));
+        const float hi = __uint_as_float(__float_as_uint(g.y) + k23 + ((r >> 6) & 0x1FFFu));
         unsigned out;
         asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(hi), "f"(lo));
         return *reinterpret_cast<__half2*>(&out);
@@ -955,10 +960,17 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             in[j] = plane[m];
         } else {
             const int i = lat_opp(j);
+            in[i] = plane[m + pn.off(-lat_cx(i), -lat_cy(i), -lat_cz(i))];
+        }
+    }
+    // Crossing the z seam exchanges the lanes.  Only the two seam planes of
+    // the pair space do it, and a warp lies in one plane, so one uniform
+    // branch replaces a select per population.
+    if (ODD && (seam_lo || seam_hi)) {
+#pragma unroll
+        for (int i = 1; i < Q; ++i) {
             const int cz = lat_cz(i);
-            const V v = plane[m + pn.off(-lat_cx(i), -lat_cy(i), -cz)];
-            const bool sw = (cz > 0 && seam_lo) || (cz < 0 && seam_hi);
-            in[i] = sw ? PV::swap(v) : v;
+            if ((cz > 0 && seam_lo) || (cz < 0 && seam_hi)) in[i] = PV::swap(in[i]);
         }
     }
     // both nodes as float2 deviations: lane 0 is (x, y, zp), lane 1 (x, y, zp + H)
@@ -1048,17 +1060,19 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
         const int i = ODD ? j : lat_opp(j);
         in[i] = PV::pack2(g[i], Lattice<Q>::w(i), p, r0, r1);
     }
+    if (ODD && (seam_lo || seam_hi)) {   // lanes exchanged across the z seam, as for the loads
+#pragma unroll
+        for (int j = 1; j < Q; ++j) {
+            const int cz = lat_cz(j);
+            if ((cz > 0 && seam_hi) || (cz < 0 && seam_lo)) in[j] = PV::swap(in[j]);
+        }
+    }
     pn.launder();
     V* out = reinterpret_cast<V*>(p.pop);
 #pragma unroll
     for (int j = 0; j < Q; ++j, out += Np) {
-        if (!ODD) {
-            out[m] = in[lat_opp(j)];
-        } else {
-            const int cz = lat_cz(j);
-            const bool sw = (cz > 0 && seam_hi) || (cz < 0 && seam_lo);
-            out[m + pn.off(lat_cx(j), lat_cy(j), cz)] = sw ? PV::swap(in[j]) : in[j];
-        }
+        if (!ODD) out[m] = in[lat_opp(j)];
+        else out[m + pn.off(lat_cx(j), lat_cy(j), lat_cz(j))] = in[j];
     }
 }
 
