@@ -296,6 +296,16 @@ vlbm_status vlbm_get_lagrangian_nodes(vlbm_sim* sim, double* pos, double* force,
  * uz [, fx, fy, fz when export_forces and spheres exist] [, omega when non-Newtonian]. */
 vlbm_status vlbm_write_macr_bin(vlbm_sim* sim, const char* path_files, const char* id_sim,
                                 uint32_t step_label, int32_t export_forces);
+/* Write PATH/ID/ID_info.txt, the run-information file of saveSimInfo /
+ * getSimInfoString (lbmReport.cpp:174-386): simulation, non-Newtonian, IBM and
+ * CUDA sections with the reference's keys and number formats.  The caller
+ * passes what the reference keeps in SimInfo and var.h: steps run, elapsed
+ * seconds (MLUPS = steps * N / 1e6 / seconds), DATA_REPORT, MACR_SAVE and
+ * U_MAX.  "Bandwidht" (sic, the reference's key) is this library's
+ * algorithmic bytes per second in 2^30-byte units; F16/BF16 runs add a
+ * "Population storage" line. */
+vlbm_status vlbm_write_info(vlbm_sim* sim, const char* path_files, const char* id_sim, uint64_t total_steps,
+                            double time_elapsed_s, int32_t report_steps, int32_t save_steps, double u_max);
 
 /* --------------------------------------------------------- checkpoint --- */
 /* Complete state of a simulation as one image (replaces operateSimCheckpoint /

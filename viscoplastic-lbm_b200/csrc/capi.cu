@@ -626,4 +626,74 @@ vlbm_status vlbm_write_macr_bin(vlbm_sim* s, const char* path_files, const char*
     return VLBM_OK;
 }
 
+// Run-information file PATH/ID/ID_info.txt (getSimInfoString and
+// saveSimInfo, lbmReport.cpp:174-386): the same sections, keys and number
+// formats; MLUPS counts every node (main.cu:539-541) and the bandwidth is the
+// algorithmic bytes of this library's step (one read and one write of each
+// stored population) per second in units of 2^30 bytes (the reference's
+// BYTES_PER_GB, main.cu:542-544, for its two-buffer scheme).
+vlbm_status vlbm_write_info(vlbm_sim* s, const char* path_files, const char* id_sim, uint64_t total_steps,
+                            double time_elapsed_s, int32_t report_steps, int32_t save_steps, double u_max) {
+    CHECK_SIM(s);
+    if (!path_files || !id_sim) { set_last_error("null path"); return VLBM_ERR_INVALID; }
+    const vlbm_config& c = s->cfg;
+    const double mlups = time_elapsed_s > 0 ? (double)total_steps * (double)s->N / 1e6 / time_elapsed_s : 0.0;
+    const double bytes = 2.0 * s->Q * s->store_bytes * (double)s->N;
+    const double bw = time_elapsed_s > 0 ? bytes * (double)total_steps / time_elapsed_s / (double)(1u << 30) : 0.0;
+    std::string out;
+    char b[4096];
+    auto add = [&](const char* fmt, auto... args) {
+        const int w = std::snprintf(b, sizeof(b), fmt, args...);
+        if (w > 0) out.append(b, (size_t)(w < (int)sizeof(b) ? w : (int)sizeof(b) - 1));
+    };
+    add("%s", "---------------------------- SIMULATION INFORMATION ----------------------------\n");
+    add("      Simulation ID: %s\n", id_sim);
+    add("       Velocity set: D3Q%d\n", s->Q);
+    add("%s", "          Precision: float\n");
+    if (c.storage != VLBM_STORE_F32)
+        add(" Population storage: %s deviations\n", c.storage == VLBM_STORE_F16 ? "float16" : "bfloat16");
+    add("                 NX: %d\n                 NY: %d\n                 NZ: %d\n           NZ_TOTAL: %d\n",
+        c.nx, c.ny, c.nz, c.nz);
+    add("                Tau: %e\n               Umax: %e\n", c.tau, u_max);
+    add("                 FX: %e\n                 FY: %e\n                 FZ: %e\n", c.fx, c.fy, c.fz);
+    add("       Report steps: %d\n         Save steps: %d\n             Nsteps: %llu\n", report_steps, save_steps,
+        (unsigned long long)total_steps);
+    add("              MLUPS: %.1f\n          Bandwidht: %.1f (Gb/s)\n", mlups, bw);
+    add("       Time elapsed: %.3f (s)\n            threads: (%d , 1, 1)\n", time_elapsed_s, s->block);
+    add("%s", "--------------------------------------------------------------------------------\n");
+    if (c.rheology != VLBM_NEWTONIAN) {
+        add("%s", "\n------------------------------ NON NEWTONIAN FLUID -----------------------------\n");
+        if (c.rheology == VLBM_POWERLAW)
+            add("              Model: Power-Law\n        Power index: %e\n Consistency factor: %e\n"
+                "            Gamma 0: %e\n", c.n_index, c.k_consistency, c.gamma0);
+        else
+            add("              Model: Bingham\n  Plastic viscosity: %e\n       Yield stress: %e\n"
+                "      Plastic omega: %e\n", c.eta_p, c.yield_stress, 1.0 / (3.0 * c.eta_p + 0.5));
+        add("%s", "--------------------------------------------------------------------------------\n");
+    }
+    out += ibm_info_section(s);
+    cudaDeviceProp prop;
+    VLBM_CUDA(cudaGetDeviceProperties(&prop, s->device));
+    add("%s", "\n------------------------------- CUDA INFORMATION -------------------------------\n");
+    add("\t      device number: %d\n\t               name: %s\n\t    multiprocessors: %d\n"
+        "\t compute capability: %d.%d\n\t        ECC enabled: %d\n", s->device, prop.name,
+        prop.multiProcessorCount, prop.major, prop.minor, prop.ECCEnabled);
+    add("%s", "--------------------------------------------------------------------------------\n");
+    const std::string dir = std::string(path_files) + "/" + id_sim;
+    {   // mkdir -p (folderSetup, lbmReport.cpp:25-52)
+        std::string acc;
+        for (size_t k = 0; k <= dir.size(); ++k) {
+            if ((k == dir.size() || dir[k] == '/') && !acc.empty()) mkdir(acc.c_str(), 0777);
+            if (k < dir.size()) acc.push_back(dir[k]);
+        }
+    }
+    const std::string fn = dir + "/" + id_sim + "_info.txt";
+    FILE* f = std::fopen(fn.c_str(), "w");
+    if (!f) { set_last_error("cannot open " + fn); return VLBM_ERR_IO; }
+    const size_t wr = std::fwrite(out.data(), 1, out.size(), f);
+    const int cl = std::fclose(f);
+    if (wr != out.size() || cl != 0) { set_last_error("short write " + fn); return VLBM_ERR_IO; }
+    return VLBM_OK;
+}
+
 }  // extern "C"

@@ -33,6 +33,8 @@
 // Particle state, contacts and integration are FP64; the Eulerian fields FP32.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cstdio>
+#include <string>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -840,6 +842,46 @@ vlbm_status ibm_step(vlbm_sim* s) {
 }
 
 int ibm_iterations(const vlbm_sim* s) { return s->ibm ? s->ibm->cfg.max_iterations : 0; }
+
+std::string ibm_info_section(const vlbm_sim* s) {
+    const IbmState* st = s->ibm;
+    if (!st || st->np == 0) return "";
+    const vlbm_ibm_config& c = st->cfg;
+    char b[2048];
+    const int w = std::snprintf(
+        b, sizeof(b),
+        "\n------------------------------------- IBM --------------------------------------\n"
+        "   Number of particles: %d\n"
+        "        IBM iterations: %d\n"
+        "          Stencil size: %d\n"
+        "         Fluid density: %e\n"
+        "                    GX: %e\n"
+        "                    GY: %e\n"
+        "                    GZ: %e\n"
+        "            Mesh scale: %.2f\n"
+        "         IBM thickness: %.2f\n"
+        " IBM Breugem parameter: %.2f\n"
+        " IBM Movement Disctre.: %.2f\n"
+        "--------------------------------- IBM Collision --------------------------------\n"
+        "\tPart-Part Frict Coef.: %.2f\n"
+        "\tPart-Wall Frict Coef.: %.2f\n"
+        "\tPart-Part Rest. Coef.: %.2f\n"
+        "\tPart-Wall Rest. Coef.: %.2f\n"
+        "\tParticle Young's Mod.: %.2f\n"
+        "\tParticle Poisson Rat.: %.2f\n"
+        "\t    Wall Young's Mod.: %.2f\n"
+        "\t    Wall Poisson Rat.: %.2f\n"
+        "--------------------------------- IBM Boundary Conditions ----------------------\n"
+        "\t        IBM BC. X-Dir: %s \n"
+        "\t        IBM BC. Y-Dir: %s \n"
+        "\t        IBM BC. Z-Dir: %s \n"
+        "--------------------------------------------------------------------------------\n",
+        st->np, c.max_iterations, c.stencil, c.fluid_density, c.gx, c.gy, c.gz, c.mesh_scale, c.thickness,
+        c.breugem, c.movement_alpha, c.pp_friction, c.pw_friction, c.pp_restitution, c.pw_restitution,
+        c.particle_young, c.particle_poisson, c.wall_young, c.wall_poisson, c.wall_x ? "Wall" : "Periodic",
+        c.wall_y ? "Wall" : "Periodic", c.wall_z ? "Wall" : "Periodic");
+    return std::string(b, w > 0 ? (size_t)std::min(w, (int)sizeof(b) - 1) : 0);
+}
 
 uint32_t ibm_record_bytes() { return (uint32_t)sizeof(DPart); }
 

@@ -114,5 +114,7 @@ void ibm_destroy(IbmState* st, DeviceAllocator* allocator);
 void ibm_reset(vlbm_sim* s);
 void ibm_counts(const vlbm_sim* s, int* np, int* nn);
 int ibm_iterations(const vlbm_sim* s);
+// IBM section of the run-information file (lbmReport.cpp:230-340); empty without spheres.
+std::string ibm_info_section(const vlbm_sim* s);
 
 }  // namespace vlbm

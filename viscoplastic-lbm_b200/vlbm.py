@@ -198,6 +198,7 @@ _SIGS = {
     "vlbm_get_particles": [_P, C.POINTER(ParticleState), C.c_int32],
     "vlbm_get_lagrangian_nodes": [_P, _F64P, _F64P, C.c_size_t],
     "vlbm_write_macr_bin": [_P, C.c_char_p, C.c_char_p, C.c_uint32, C.c_int32],
+    "vlbm_write_info": [_P, C.c_char_p, C.c_char_p, C.c_uint64, C.c_double, C.c_int32, C.c_int32, C.c_double],
     "vlbm_checkpoint_save": [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)],
     "vlbm_checkpoint_load": [_P, _P, C.c_size_t],
     "vlbm_save_checkpoint": [_P, C.c_char_p, C.c_char_p],
@@ -390,6 +391,11 @@ class Simulation:
                "vlbm_treat_data")
         return {"step": t.step, "residual": t.residual, "avg_rho": t.avg_rho, "stop": bool(t.stop),
                 "avg_uz_plane_xz": prof}
+
+    def write_info(self, path_files, id_sim, total_steps, time_elapsed_s, report_steps=0, save_steps=0,
+                   u_max=0.1):
+        _check(_lib.vlbm_write_info(self._h, path_files.encode(), id_sim.encode(), total_steps, time_elapsed_s,
+                                    report_steps, save_steps, u_max), "vlbm_write_info")
 
     def autotune(self):
         v = C.c_int32()
