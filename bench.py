@@ -13,6 +13,9 @@ the fused kernel.  Multi-GPU runs are independent replicas (the path is one
 lattice per GPU); value = all ranks' node updates / max-over-ranks time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+`--vel-set 27` and `--size NX NY NZ` run the same channel on another velocity
+set or lattice (the workload name says which); they exist for profiling runs.
 """
 import argparse
 import json
@@ -32,16 +35,25 @@ METRIC = "MLUPS"
 L2_BYTES = 126 * 2 ** 20
 
 
+def set_workload(q, nx, ny, nz):
+    global NX, NY, NZ, Q, WORKLOAD
+    NX, NY, NZ, Q = nx, ny, nz, q
+    WORKLOAD = f"d3q{q}_regularized_bingham_channel_{nx}x{ny}x{nz}"
+
+
 def config_dict(storage="f32"):
-    return {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "velocity_set": "D3Q19",
+    pop_mb = Q * NX * NY * NZ * {"f16": 2, "bf16": 2, "f64": 8}.get(storage, 4) / 1e6
+    rel = "larger" if pop_mb * 1e6 > L2_BYTES else "smaller"
+    return {"workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "velocity_set": f"D3Q{Q}",
             "collision": "regularized", "rheology": "bingham", "tau_p": 0.8, "yield_stress": 1e-5,
             "gx": 5e-6, "walls": "y (half-way bounce-back)", "periodic": "x,z", "storage": storage,
-            "streaming": "AA in-place", "l2_policy": "population array (159 MB) larger than the 126 MB L2",
+            "streaming": "AA in-place",
+            "l2_policy": f"population array ({pop_mb:.0f} MB) {rel} than the 126 MB L2",
             "parallelism": "replicas"}
 
 
 def make_cfg(vlbm, storage=0):
-    return vlbm.Config.default(nx=NX, ny=NY, nz=NZ, vel_set=19, collision=vlbm.OP_REGULARIZED,
+    return vlbm.Config.default(nx=NX, ny=NY, nz=NZ, vel_set=Q, collision=vlbm.OP_REGULARIZED,
                                rheology=vlbm.BINGHAM, eta_p=(0.8 - 0.5) / 3.0, yield_stress=1e-5,
                                fx=5e-6, storage=storage)
 
@@ -65,6 +77,8 @@ TRAFFIC_PROFILES = {
 def committed_traffic(storage, layout):
     """dram read+write bytes per launch of the fused kernel from the committed ncu summary
     of the same storage and layout (None when no capture of that kernel is committed)."""
+    if (Q, NX, NY, NZ) != (19, 256, 128, 64):
+        return None            # captures are committed for the default workload only
     if layout == "auto":   # the library's AUTO rule for D3Q19 with an even nz
         layout = "natural" if storage == "f32" else "zpair"
     name = TRAFFIC_PROFILES.get((storage, layout))
@@ -123,10 +137,24 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def load_oracle():
+    """The FP64 oracle module, oracle/oracle.py, loaded by its path (the
+    repository's oracle/ folder would otherwise import as an empty namespace
+    package when the repository root is on sys.path)."""
+    import importlib.util
+    name = "vlbm_bench_oracle"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(REPO, "oracle", "oracle.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def cpu_baseline(vlbm, seconds_budget=15.0):
     """The FP64 OpenMP oracle (restated reference step) on the host cores."""
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import oracle
+    oracle = load_oracle()
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     cfg = make_cfg(vlbm)
@@ -155,7 +183,7 @@ def storage_accuracy(vlbm, steps=6000, nxz=8):
     """
     import numpy as np
     sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import oracle
+    oracle = load_oracle()
     oracle.set_threads(os.cpu_count() or 1)
     cfg = make_cfg(vlbm)
     cfg.nx, cfg.nz = nxz, nxz
@@ -351,7 +379,6 @@ def run_reference(args, rank, world):
     import vlbm
     if rank != 0:
         return 0
-    import oracle  # noqa: F401  (path added in cpu_baseline)
     base = cpu_baseline(vlbm, seconds_budget=max(5.0, min(60.0, 2.0 * args.steps)))
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": METRIC,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -373,11 +400,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 D3Q19/D3Q27 FP32/FP16 leg")
+    ap.add_argument("--vel-set", type=int, default=19, choices=[19, 27])
+    ap.add_argument("--size", type=int, nargs=3, default=[256, 128, 64], metavar=("NX", "NY", "NZ"))
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-step-scale", type=float, default=0.25)
     ap.add_argument("--serving-rate", type=float, default=200.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    set_workload(args.vel_set, *args.size)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
