@@ -32,6 +32,10 @@ REQS = [
       dict(diameter=4, cx=11.0, cy=9.0, cz=7.0, density=2.0, movable=1)]),
     (7, dict(nx=30, ny=10, nz=14, vel_set=19, rheology=2, n_index=0.7, k_consistency=0.05, fx=2e-5, storage=2), 1,
      33, []),
+    # cylinder ducts: interpolated bounce-back and unused nodes in the batched kernel
+    (8, dict(nx=22, ny=22, nz=12, vel_set=19, rheology=1, eta_p=0.1, yield_stress=1e-6, fz=2e-5, storage=1), 9,
+     140, []),
+    (9, dict(nx=20, ny=24, nz=6, vel_set=27, tau=0.8, fz=1e-5, duct_inner_rotation=0.01), 10, 95, []),
 ]
 IBM_KW = dict(max_iterations=2, gx=0.0, gy=0.0, gz=-1e-5, wall_x=1, wall_y=1, wall_z=1)
 

@@ -89,7 +89,8 @@ struct Resident {
 
 // Device bytes a request will hold: populations, class/slot arrays (5 B per
 // node), the macroscopic read-out scratch used at retirement (20 B per node),
-// the side store of the wall nodes (at most the six faces), the Power-Law
+// the side store of the wall nodes (at most the six faces; cylinder walls are
+// shorter but also carry 96 B of interpolation coefficients), the Power-Law
 // state, the IBM fields and Lagrangian arrays, plus 1 MiB of small allocations.
 size_t estimate_bytes(const vlbm_request& r) {
     const size_t N = (size_t)r.cfg.nx * r.cfg.ny * r.cfg.nz;
@@ -97,6 +98,7 @@ size_t estimate_bytes(const vlbm_request& r) {
     size_t b = (size_t)r.cfg.vel_set * N * sb + 25 * N + (1 << 20);
     const size_t walls = 2 * ((size_t)r.cfg.nx * r.cfg.ny + (size_t)r.cfg.ny * r.cfg.nz + (size_t)r.cfg.nx * r.cfg.nz);
     b += walls * (2 * (size_t)r.cfg.vel_set * 4 + 24);
+    if (r.builder == VLBM_BUILDER_CIRCULAR_DUCT || r.builder == VLBM_BUILDER_ANNULAR_DUCT) b += walls * 96;
     if (r.cfg.rheology == VLBM_POWERLAW) b += 4 * N;
     if (r.n_spheres > 0) b += 56 * N + (size_t)r.n_spheres * 700 * 10 * 8;
     return b;
