@@ -242,6 +242,66 @@ def cube_leg(vlbm, torch, device, steps=200, warmup=10, n=256):
     return out
 
 
+def sphere_pack(n, radius, box, gap=1.0, seed=42):
+    """Non-overlapping sphere centres by rejection sampling: at least `gap`
+    lattice units between spheres and to the walls (numpy default_rng(seed))."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    lo = radius + gap
+    out = []
+    while len(out) < n:
+        c = lo + rng.random(3) * (np.array(box, dtype=float) - 1 - 2 * lo)
+        if all(np.linalg.norm(c - o) >= 2 * radius + gap for o in out):
+            out.append(c)
+    return out
+
+
+def ibm_leg(vlbm, torch, device, steps=50, warmup=5):
+    """The IBM configuration: 192x192x384 closed box, D3Q19 regularized Bingham
+    (tau_p 0.8, yield 1e-5), gravity -z, 64 movable spheres of radius 8
+    (density ratio 1.5, non-overlapping, default_rng(42)), 3 direct-forcing
+    iterations, Hertz-Mindlin contacts (E 1e5, Poisson 0.3, friction 0.3).
+    Timed with and without the spheres on the same lattice."""
+    import numpy as np
+    nx, ny, nz = 192, 192, 384
+    cfg = vlbm.Config.default(nx=nx, ny=ny, nz=nz, vel_set=19, collision=vlbm.OP_REGULARIZED,
+                              rheology=vlbm.BINGHAM, eta_p=0.1, yield_stress=1e-5)
+    cfg.device = device
+    ibm = vlbm.IbmConfig.default(max_iterations=3, gx=0.0, gy=0.0, gz=-1e-5, wall_x=1, wall_y=1, wall_z=1,
+                                 particle_young=1e5, wall_young=1e5, particle_poisson=0.3, wall_poisson=0.3,
+                                 pp_friction=0.3, pw_friction=0.3)
+    centres = sphere_pack(64, 8.0, (nx, ny, nz))
+    spheres = [vlbm.Sphere(diameter=16.0, cx=float(c[0]), cy=float(c[1]), cz=float(c[2]), density=1.5, movable=1)
+               for c in centres]
+    out = {"lattice": f"{nx}x{ny}x{nz}", "spheres": 64, "radius": 8, "mdf_iterations": 3, "steps": steps}
+    for with_spheres in (False, True):
+        sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_CLOSED_BOX)
+        stream = torch.cuda.Stream()
+        sim.set_stream(stream.cuda_stream)
+        sim.autotune()
+        if with_spheres:
+            sim.add_spheres(ibm, spheres)
+        sim.step(warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sim.sync()
+        ms = e0.elapsed_time(e1) / steps
+        key = "with_spheres" if with_spheres else "fluid_only"
+        out[key] = {"ms_per_step": ms, "mlups": nx * ny * nz / (ms / 1e3) / 1e6}
+        if with_spheres:
+            info = sim.info()
+            out["lagrangian_nodes"] = info.n_lagrangian_nodes
+            z = np.array([p.pos[2] for p in sim.particles(64)])
+            out["mean_sphere_z_drop"] = float(np.mean([c[2] for c in centres]) - z.mean())
+        sim.close()
+    out["ibm_ms_per_step"] = out["with_spheres"]["ms_per_step"] - out["fluid_only"]["ms_per_step"]
+    return out
+
+
 def serving_requests(vlbm, n, step_scale, seed=2024):
     """A seeded sample of the Bingham-duct serving stream.
 
@@ -400,6 +460,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 D3Q19/D3Q27 FP32/FP16 leg")
+    ap.add_argument("--no-ibm", action="store_true", help="skip the 64-sphere IBM leg")
     ap.add_argument("--vel-set", type=int, default=19, choices=[19, 27])
     ap.add_argument("--size", type=int, nargs=3, default=[256, 128, 64], metavar=("NX", "NY", "NZ"))
     ap.add_argument("--serving-requests", type=int, default=48)
@@ -502,6 +563,9 @@ def main():
     cube = None
     if rank == 0 and world == 1 and not args.no_cube:
         cube = cube_leg(vlbm, torch, local)
+    ibm_run = None
+    if rank == 0 and world == 1 and not args.no_ibm:
+        ibm_run = ibm_leg(vlbm, torch, local)
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_leg(vlbm, args.serving_requests, args.serving_step_scale, args.serving_rate)
@@ -527,6 +591,7 @@ def main():
             "clocks": clk,
             "storage_accuracy": accuracy,
             "lattice_256": cube,
+            "ibm_64_spheres": ibm_run,
             "serving": serving,
         }
         print(json.dumps(line), flush=True)
