@@ -277,16 +277,27 @@ __device__ void wall_contact(const IbmParams& P, DPart& p, const double wn[3], d
 
 // sphereSphereCollision ibmCollision.cu:1718-1913; slots kept in the lower
 // index i, so one thread per i serialises all slot updates of that particle.
-__device__ void pair_contact(const IbmParams& P, DPart& pi, const DPart& pj, int j, double accF[3], double accM[3],
-                             double* out6) {
-    const int step = P.step;
+// Centre distance of two spheres (periodic axes wrapped), with explicit
+// roundings so the contact screening and the contact itself take the same
+// decision bit for bit.
+__device__ __forceinline__ double centre_dist(const IbmParams& P, const DPart& pi, const DPart& pj, double d[3]) {
     const double L[3] = {(double)P.nx, (double)P.ny, (double)P.nz};
-    double d[3];
     for (int a = 0; a < 3; ++a) {
         d[a] = pi.pos[a] - pj.pos[a];
         if (!P.wall[a]) d[a] = pdelta(d[a], L[a]);
     }
-    const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    return sqrt(__dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2])));
+}
+__device__ __forceinline__ bool spheres_touch(const IbmParams& P, const DPart& pi, const DPart& pj) {
+    double d[3];
+    return !(centre_dist(P, pi, pj, d) > pi.radius + pj.radius);
+}
+
+__device__ void pair_contact(const IbmParams& P, DPart& pi, const DPart& pj, int j, double accF[3], double accM[3],
+                             double* out6) {
+    const int step = P.step;
+    double d[3];
+    const double dist = centre_dist(P, pi, pj, d);
     if (dist > pi.radius + pj.radius) return;
     const double n[3] = {d[0] / dist, d[1] / dist, d[2] / dist};
     const double disp = pi.radius + pj.radius - dist;
@@ -402,8 +413,14 @@ __device__ void update_center(const IbmParams& P, DPart& p) {
     for (int a = 0; a < 3; ++a) p.w[a] = wn[a];
 }
 
+constexpr int IBM_SCREEN_MAX = 256;   // spheres whose pair screening fits the shared bit matrix
+
 __device__ void ibm_contacts(const IbmParams& P, DPart* parts, double* contrib) {
+    // near[i][w] bit b: spheres i and 32w+b touch (the test pair_contact starts with)
+    __shared__ unsigned near[IBM_SCREEN_MAX * (IBM_SCREEN_MAX / 32)];
     const int np = P.np;
+    const bool screen = np <= IBM_SCREEN_MAX;
+    const int W = (np + 31) >> 5;
     // gpuUpdateParticleOldValues ibm.cu:995-1042
     for (int i = threadIdx.x; i < np; i += blockDim.x) {
         DPart& p = parts[i];
@@ -414,15 +431,41 @@ __device__ void ibm_contacts(const IbmParams& P, DPart* parts, double* contrib) 
         }
     }
     __syncthreads();
-    // contacts: thread i owns particle i's slots and its walls
+    if (screen) {   // all pairs at once, a warp per 32 partners, one ballot per word
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int t = warp; t < np * W; t += nw) {
+            const int i = t / W, w = t - i * W, k = 32 * w + lane;
+            const bool hit = k < np && k != i && spheres_touch(P, parts[i], parts[k]);
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) near[i * W + w] = m;
+        }
+        __syncthreads();
+    }
+    // contacts: thread i owns particle i's slots and its walls; partners in
+    // increasing index, only those that touch (the others add nothing)
     for (int i = threadIdx.x; i < np; i += blockDim.x) {
         DPart& pi = parts[i];
         double F[3] = {0, 0, 0}, Mo[3] = {0, 0, 0};
-        for (int j = i + 1; j < np; ++j) {
-            double* o = contrib + ((size_t)i * np + j) * 6;
-            for (int a = 0; a < 6; ++a) o[a] = 0.0;
-            if (!pi.movable && !parts[j].movable) continue;
-            pair_contact(P, pi, parts[j], j, F, Mo, o);
+        if (screen) {
+            for (int w = (i + 1) >> 5; w < W; ++w) {
+                unsigned m = near[i * W + w];
+                if (w == ((i + 1) >> 5)) m &= ~0u << ((i + 1) & 31);   // partners j > i
+                while (m) {
+                    const int j = 32 * w + __ffs(m) - 1;
+                    m &= m - 1;
+                    double* o = contrib + ((size_t)i * np + j) * 6;
+                    for (int a = 0; a < 6; ++a) o[a] = 0.0;
+                    if (!pi.movable && !parts[j].movable) continue;
+                    pair_contact(P, pi, parts[j], j, F, Mo, o);
+                }
+            }
+        } else {
+            for (int j = i + 1; j < np; ++j) {
+                double* o = contrib + ((size_t)i * np + j) * 6;
+                for (int a = 0; a < 6; ++a) o[a] = 0.0;
+                if (!pi.movable && !parts[j].movable) continue;
+                pair_contact(P, pi, parts[j], j, F, Mo, o);
+            }
         }
         if (pi.movable) {
             const int Li[3] = {P.nx, P.ny, P.nz};
@@ -442,9 +485,22 @@ __device__ void ibm_contacts(const IbmParams& P, DPart* parts, double* contrib) 
     __syncthreads();
     for (int j = threadIdx.x; j < np; j += blockDim.x) {
         DPart& pj = parts[j];
-        for (int i = 0; i < j; ++i) {
-            const double* o = contrib + ((size_t)i * np + j) * 6;
-            for (int a = 0; a < 3; ++a) { pj.f[a] += o[a]; pj.M[a] += o[3 + a]; }
+        if (screen) {   // partners i < j that touch, in increasing index
+            for (int w = 0; w <= (j >> 5) && w < W; ++w) {
+                unsigned m = near[j * W + w];
+                if (w == (j >> 5)) m &= (1u << (j & 31)) - 1u;
+                while (m) {
+                    const int i = 32 * w + __ffs(m) - 1;
+                    m &= m - 1;
+                    const double* o = contrib + ((size_t)i * np + j) * 6;
+                    for (int a = 0; a < 3; ++a) { pj.f[a] += o[a]; pj.M[a] += o[3 + a]; }
+                }
+            }
+        } else {
+            for (int i = 0; i < j; ++i) {
+                const double* o = contrib + ((size_t)i * np + j) * 6;
+                for (int a = 0; a < 3; ++a) { pj.f[a] += o[a]; pj.M[a] += o[3 + a]; }
+            }
         }
         update_center(P, pj);  // predictor (ibm.cu:98-103)
     }
