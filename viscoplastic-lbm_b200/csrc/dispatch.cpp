@@ -38,7 +38,7 @@ cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in,
 #undef C_
 }
 
-cudaError_t launch_batched(int Q, int st, const BatchLaunch& L, const BatchState* state, const BatchBlock* table,
+cudaError_t launch_batched(int Q, int st, const BatchLaunch* L, const BatchState* state, const BatchBlock* table,
                            int ntiles, int grid, bool odd, int op, int rheo, cudaStream_t s) {
 #define C_(QQ, SS) launch_batched_st<QQ, SS>(L, state, table, ntiles, grid, odd, op, rheo, s)
     VLBM_SELECT(C_)

@@ -25,7 +25,7 @@ struct BatchLaunch;
 struct BatchState;
 struct BatchBlock;
 template <int Q, int ST>
-cudaError_t launch_batched_st(const BatchLaunch& L, const BatchState* state, const BatchBlock* table, int ntiles,
+cudaError_t launch_batched_st(const BatchLaunch* L, const BatchState* state, const BatchBlock* table, int ntiles,
                               int grid, bool odd, int op, int rheo, cudaStream_t s);
 
 // Run-time selection over (Q, storage).
@@ -38,7 +38,7 @@ cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in,
 // One batched step of the lattices of a (Q, storage, op, rheology) group that
 // share the AA parity `odd`: ntiles table entries walked by `grid` persistent
 // blocks of 256 threads.
-cudaError_t launch_batched(int Q, int st, const BatchLaunch& L, const BatchState* state, const BatchBlock* table,
+cudaError_t launch_batched(int Q, int st, const BatchLaunch* L, const BatchState* state, const BatchBlock* table,
                            int ntiles, int grid, bool odd, int op, int rheo, cudaStream_t s);
 // Resident 256-thread blocks per SM of the batched kernel of a group.
 int batched_blocks_per_sm(int Q, int st, int op, int rheo);

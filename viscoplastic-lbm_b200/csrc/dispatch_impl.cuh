@@ -90,7 +90,7 @@ cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, 
 }
 
 template <int Q, int OP, int RHEO, int ST>
-cudaError_t batched_t(const BatchLaunch& L, const BatchState* state, const BatchBlock* table, int ntiles, int grid,
+cudaError_t batched_t(const BatchLaunch* L, const BatchState* state, const BatchBlock* table, int ntiles, int grid,
                       bool odd, cudaStream_t s) {
     if (odd) k_step_batched<Q, OP, RHEO, ST, true><<<grid, 256, 0, s>>>(L, state, table, ntiles);
     else k_step_batched<Q, OP, RHEO, ST, false><<<grid, 256, 0, s>>>(L, state, table, ntiles);
@@ -98,7 +98,7 @@ cudaError_t batched_t(const BatchLaunch& L, const BatchState* state, const Batch
 }
 
 template <int Q, int OP, int ST>
-cudaError_t batched_rh(const BatchLaunch& L, const BatchState* state, const BatchBlock* table, int ntiles, int grid,
+cudaError_t batched_rh(const BatchLaunch* L, const BatchState* state, const BatchBlock* table, int ntiles, int grid,
                        bool odd, int rheo, cudaStream_t s) {
     switch (rheo) {
     case VLBM_NEWTONIAN: return batched_t<Q, OP, VLBM_NEWTONIAN, ST>(L, state, table, ntiles, grid, odd, s);
@@ -109,7 +109,7 @@ cudaError_t batched_rh(const BatchLaunch& L, const BatchState* state, const Batc
 }
 
 template <int Q, int ST>
-cudaError_t launch_batched_st(const BatchLaunch& L, const BatchState* state, const BatchBlock* table, int ntiles,
+cudaError_t launch_batched_st(const BatchLaunch* L, const BatchState* state, const BatchBlock* table, int ntiles,
                               int grid, bool odd, int op, int rheo, cudaStream_t s) {
     if (ntiles <= 0) return cudaSuccess;
     if (op == VLBM_OP_BGK) return batched_rh<Q, VLBM_OP_BGK, ST>(L, state, table, ntiles, grid, odd, rheo, s);
@@ -149,7 +149,7 @@ int batched_occupancy_st(int op, int rheo) {
     template cudaError_t launch_get_pops_st<QQ, SS>(const StepParams&, bool, float*, cudaStream_t);            \
     template cudaError_t launch_set_pops_st<QQ, SS>(const StepParams&, const float*, float, float, float, float, \
                                                     cudaStream_t);                                              \
-    template cudaError_t launch_batched_st<QQ, SS>(const BatchLaunch&, const BatchState*, const BatchBlock*, int,  \
+    template cudaError_t launch_batched_st<QQ, SS>(const BatchLaunch*, const BatchState*, const BatchBlock*, int,  \
                                                    int, bool, int, int, cudaStream_t);                          \
     template int batched_occupancy_st<QQ, SS>(int, int);
 

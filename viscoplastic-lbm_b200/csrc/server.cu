@@ -110,7 +110,8 @@ size_t estimate_bytes(const vlbm_request& r) {
 // ph (steps since the rebuild, mod 2).
 struct Chunk {
     int part;
-    BatchLaunch L;        // the chunk's lattice parameters (launch arguments)
+    BatchLaunch L;        // the chunk's lattice parameters (uploaded to d_launch[launch_idx])
+    size_t launch_idx;
     size_t table_off;
     int ntiles, grid;
 };
@@ -228,14 +229,16 @@ struct vlbm_server {
     bool dirty = true;
     BatchState* d_state = nullptr;
     BatchBlock* d_table = nullptr;
-    size_t cap_slots = 0, cap_table = 0;
+    BatchLaunch* d_launch = nullptr;    // one parameter block per chunk
+    size_t cap_slots = 0, cap_table = 0, cap_launch = 0;
     std::vector<void*> old_tables;      // outgrown table buffers, freed with the server
     // pinned staging of the tables: a ring, so a rebuild does not wait for the
     // GPU to reach the previous upload (an entry is reused once its upload ran)
     struct Staging {
         BatchState* slots = nullptr;
         BatchBlock* table = nullptr;
-        size_t cap_slots = 0, cap_table = 0;
+        BatchLaunch* launch = nullptr;
+        size_t cap_slots = 0, cap_table = 0, cap_launch = 0;
         cudaEvent_t uploaded = nullptr;
         bool pending = false;
     };
@@ -280,10 +283,12 @@ struct vlbm_server {
         drop_graphs();
         cudaFree(d_state);
         cudaFree(d_table);
+        cudaFree(d_launch);
         for (void* p : old_tables) cudaFree(p);
         for (Staging& g : staging) {
             if (g.slots) cudaFreeHost(g.slots);
             if (g.table) cudaFreeHost(g.table);
+            if (g.launch) cudaFreeHost(g.launch);
             if (g.uploaded) cudaEventDestroy(g.uploaded);
         }
         for (void* p : old_pinned) cudaFreeHost(p);
@@ -390,9 +395,14 @@ vlbm_status server_rebuild(vlbm_server* sv) {
         for (unsigned t = 0; t < nt; ++t) table.push_back(BatchBlock{local, t * (unsigned)BATCH_TILE});
         c.ntiles += (int)nt;
     }
+    std::vector<const BatchLaunch*> launch_src;   // chunk parameter blocks in upload order
     for (Group& g : sv->groups) {
         const int per_sm = std::max(1, batched_blocks_per_sm(g.Q, g.st, g.op, g.rheo));
-        for (Chunk& c : g.chunks) c.grid = std::min(c.ntiles, per_sm * sv->sms);
+        for (Chunk& c : g.chunks) {
+            c.grid = std::min(c.ntiles, per_sm * sv->sms);
+            c.launch_idx = launch_src.size();
+            launch_src.push_back(&c.L);
+        }
     }
     sv->branch_res = sv->ibm_res;
     sv->branch_res.insert(sv->branch_res.end(), sv->own_res.begin(), sv->own_res.end());
@@ -449,6 +459,18 @@ vlbm_status server_rebuild(vlbm_server* sv) {
         sv->d_table = static_cast<BatchBlock*>(d);
         sv->cap_table = cap;
     }
+    if (launch_src.size() > sv->cap_launch) {
+        const size_t cap = std::max<size_t>(16, launch_src.size() * 2);
+        void* d = nullptr;
+        if (cudaMalloc(&d, cap * sizeof(BatchLaunch)) != cudaSuccess) {
+            cudaGetLastError();
+            set_last_error("server launch table allocation failed");
+            return VLBM_ERR_NOMEM;
+        }
+        if (sv->d_launch) sv->old_tables.push_back(sv->d_launch);
+        sv->d_launch = static_cast<BatchLaunch*>(d);
+        sv->cap_launch = cap;
+    }
     if (!slots.empty()) {
         vlbm_server::Staging& g = sv->staging[sv->next_staging];
         sv->next_staging = (sv->next_staging + 1) % 4;
@@ -473,6 +495,15 @@ vlbm_status server_rebuild(vlbm_server* sv) {
                 g.cap_table = sv->cap_table;
             }
         }
+        if (e == cudaSuccess && launch_src.size() > g.cap_launch) {
+            void* h = nullptr;
+            e = cudaHostAlloc(&h, sv->cap_launch * sizeof(BatchLaunch), cudaHostAllocDefault);
+            if (e == cudaSuccess) {
+                if (g.launch) sv->old_pinned.push_back(g.launch);
+                g.launch = static_cast<BatchLaunch*>(h);
+                g.cap_launch = sv->cap_launch;
+            }
+        }
         if (e == cudaSuccess && !g.uploaded) e = cudaEventCreateWithFlags(&g.uploaded, cudaEventDisableTiming);
         if (e == cudaSuccess) {
             std::memcpy(g.slots, slots.data(), slots.size() * sizeof(BatchState));
@@ -483,6 +514,11 @@ vlbm_status server_rebuild(vlbm_server* sv) {
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(sv->d_table, g.table, table.size() * sizeof(BatchBlock), cudaMemcpyHostToDevice,
                                 sv->stream);
+        if (e == cudaSuccess && !launch_src.empty()) {
+            for (size_t k = 0; k < launch_src.size(); ++k) std::memcpy(&g.launch[k], launch_src[k], sizeof(BatchLaunch));
+            e = cudaMemcpyAsync(sv->d_launch, g.launch, launch_src.size() * sizeof(BatchLaunch),
+                                cudaMemcpyHostToDevice, sv->stream);
+        }
         if (e == cudaSuccess) e = cudaEventRecord(g.uploaded, sv->stream);
         if (e != cudaSuccess) return cuda_status(e, "server table upload");
         g.pending = true;
@@ -531,7 +567,8 @@ vlbm_status enqueue_steps(vlbm_server* sv, int n) {
         for (const Group& g : sv->groups)
             for (const Chunk& c : g.chunks) {
                 const bool odd = (c.part ^ sv->phase) != 0;
-                e = launch_batched(g.Q, g.st, c.L, sv->d_state, sv->d_table + c.table_off, c.ntiles, c.grid, odd, g.op,
+                e = launch_batched(g.Q, g.st, sv->d_launch + c.launch_idx, sv->d_state, sv->d_table + c.table_off,
+                                   c.ntiles, c.grid, odd, g.op,
                                    g.rheo, sv->stream);
                 if (e != cudaSuccess) return cuda_status(e, "batched step");
                 launches += 1.0;

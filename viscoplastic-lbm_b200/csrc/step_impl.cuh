@@ -710,9 +710,11 @@ struct BatchBlock {
     int slot;           // lattice of this tile: index into the launch's parameters
     unsigned first;     // first node of this tile
 };
-// Arguments of one batched launch: the step parameters of up to
-// BATCH_MAX_SLOTS lattices (side_prev / side_next hold side[0] / side[1]) in
-// the kernel's constant parameter space, read with uniform indices.
+// Parameters of one batched launch: the step parameters of up to
+// BATCH_MAX_SLOTS lattices (side_prev / side_next hold side[0] / side[1]).
+// They stay in device memory between table rebuilds and the launch passes a
+// pointer: 12 KB of launch arguments would cost host time on every launch,
+// while a block reads a lattice's 200 bytes once per lattice change.
 struct BatchLaunch {
     StepParams p[BATCH_MAX_SLOTS];
     int state_base;     // index of p[0]'s entry in the state array
@@ -723,7 +725,7 @@ struct BatchLaunch {
 template <int Q> constexpr int batch_min_blocks() { return Q == 19 ? 5 : 4; }
 
 template <int Q, int OP, int RHEO, int ST, bool ODD>
-__global__ void __launch_bounds__(256, batch_min_blocks<Q>()) k_step_batched(const __grid_constant__ BatchLaunch L,
+__global__ void __launch_bounds__(256, batch_min_blocks<Q>()) k_step_batched(const BatchLaunch* __restrict__ L,
                                                                             const BatchState* __restrict__ state,
                                                                             const BatchBlock* __restrict__ table,
                                                                             int ntiles) {
@@ -745,10 +747,10 @@ __global__ void __launch_bounds__(256, batch_min_blocks<Q>()) k_step_batched(con
             __syncthreads();   // the previous lattice's tiles are done with sp
             if (threadIdx.x < WORDS)
                 reinterpret_cast<unsigned*>(&sp)[threadIdx.x] =
-                    reinterpret_cast<const unsigned*>(&L.p[e.slot])[threadIdx.x];
+                    reinterpret_cast<const unsigned*>(&L->p[e.slot])[threadIdx.x];
             if (threadIdx.x == WORDS) {
-                const BatchState st = state[L.state_base + e.slot];
-                const StepParams& q = L.p[e.slot];
+                const BatchState st = state[L->state_base + e.slot];
+                const StepParams& q = L->p[e.slot];
                 sides[0] = st.side_cur ? const_cast<float*>(q.side_next) : const_cast<float*>(q.side_prev);
                 sides[1] = st.side_cur ? const_cast<float*>(q.side_prev) : q.side_next;
                 use_bc = st.apply_bc;
