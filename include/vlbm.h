@@ -3,9 +3,11 @@
  *
  * Plain C linkage, plain pointers and sizes, no CUDA or torch types in any
  * signature.  Every call returns a vlbm_status (0 = ok); nothing calls exit().
- * One simulation handle per host thread; the library holds no global state
- * besides the per-device kernel caches.  Host buffers are owned by the
- * caller, device buffers by the library.
+ * One simulation handle per host thread.  The library's only global state is
+ * the per-device kernel caches and one fixed device array that
+ * vlbm_moments_sum_noalloc uses as scratch (calls of it that overlap on a
+ * device race; see its declaration).  Host buffers are owned by the caller,
+ * device buffers by the library.
  *
  * The reference has no library boundary: its hot path is entered through
  * CUDA kernels and compile-time macros.  Each entry point below names the
@@ -32,7 +34,7 @@ enum {
     VLBM_ERR_UNSUPPORTED = 4,  /* combination the reference does not define */
     VLBM_ERR_DIVERGED = 5,     /* non-finite or non-positive density seen  */
     VLBM_ERR_STATE = 6,        /* call out of order (e.g. no geometry yet) */
-    VLBM_ERR_TIMEOUT = 7,      /* a bounded device wait gave up            */
+    /* 7 is not used */
     VLBM_ERR_NOT_FOUND = 8,    /* unknown name / missing file              */
     VLBM_ERR_IO = 9            /* host file I/O failed                     */
 };
@@ -116,11 +118,11 @@ typedef struct vlbm_config {
     double tau;                  /* var.h:104 TAU (Newtonian relaxation time)       */
     double rho0;                 /* var.h:107 RHO_0                                 */
     double fx, fy, fz;           /* var.h:109-111 body force FX, FY, FZ             */
-    double eta_p;                /* nnf.h:125 ETA_P (Bingham plastic viscosity)     */
-    double yield_stress;         /* nnf.h:126 S_Y                                   */
-    double n_index;              /* nnf.h:116 N_INDEX (Power-Law)                   */
-    double k_consistency;        /* nnf.h:117 K_CONSISTENCY                         */
-    double gamma0;               /* nnf.h:118 GAMMA_0 (truncation)                  */
+    double eta_p;                /* nnf.h:20 ETA_P (Bingham plastic viscosity)      */
+    double yield_stress;         /* nnf.h:21 S_Y                                    */
+    double n_index;              /* nnf.h:11 N_INDEX (Power-Law)                    */
+    double k_consistency;        /* nnf.h:12 K_CONSISTENCY                          */
+    double gamma0;               /* nnf.h:13 GAMMA_0 (truncation)                   */
     double ux_bc[8], uy_bc[8], uz_bc[8], rho_bc[8]; /* var.h:114-117 UX_BC..RHO_BC */
     double storage_scale;        /* F16/BF16 deviation scale; 0 = library default (F16: a power of two 1..2^24) */
     int32_t layout;              /* VLBM_LAYOUT_*: population storage order          */
@@ -293,7 +295,9 @@ vlbm_status vlbm_get_lagrangian_nodes(vlbm_sim* sim, double* pos, double* force,
 
 /* ------------------------------------------------------------ outputs --- */
 /* Write PATH/ID/ID_<var><step>.bin files (lbmReport.cpp:55-172) for rho, ux, uy,
- * uz [, fx, fy, fz when export_forces and spheres exist] [, omega when non-Newtonian]. */
+ * uz [, fx, fy, fz when export_forces and spheres exist] [, omega when non-Newtonian].
+ * The step field is getVarFilename's: six digits (ID_rho000100.bin), seven for
+ * step 0 (ID_rho0000000.bin), the plain number from 1,000,000 on. */
 vlbm_status vlbm_write_macr_bin(vlbm_sim* sim, const char* path_files, const char* id_sim,
                                 uint32_t step_label, int32_t export_forces);
 /* Write PATH/ID/ID_info.txt, the run-information file of saveSimInfo /
@@ -306,6 +310,75 @@ vlbm_status vlbm_write_macr_bin(vlbm_sim* sim, const char* path_files, const cha
  * "Population storage" line. */
 vlbm_status vlbm_write_info(vlbm_sim* sim, const char* path_files, const char* id_sim, uint64_t total_steps,
                             double time_elapsed_s, int32_t report_steps, int32_t save_steps, double u_max);
+
+/* Particle files of saveParticlesInfo (IBM/ibmReport.cpp:26-102):
+ * PATH/ID/ID_pCenters<step>.csv (one row per sphere: p_number, step, pos, vel,
+ * w, f, M, I, S, radius, volume, movable, semi-axes; %e numbers) and, when
+ * save_nodes, PATH/ID/ID_pNodes<step>.csv (particle_index, pos, S per
+ * Lagrangian node).  The step field is getVarFilename's, as for the .bin files.
+ * VLBM_ERR_STATE when the simulation has no spheres. */
+vlbm_status vlbm_write_particles_csv(vlbm_sim* sim, const char* path_files, const char* id_sim, uint32_t step_label,
+                                     int32_t save_nodes);
+
+/* ------------------------------------------------- run configuration --- */
+/* The run configuration of the drop-in driver (driver/vlbm_run.cpp), read from
+ * the YAML file of the reference's configuration tool: a list whose first item
+ * maps the keys of pyvisc's SchemeVarH (pyvisc/schemes.py:53-74,
+ * examples/all_options.yaml) -- precision, NX, NY, NZ (per GPU), tau, vel_set,
+ * use_ibm, non_newtonian_model (null / BINGHAM / POWERLAW), sim_id, path_save,
+ * steps, macr_save, data_report, FX, FY, FZ, data_stop, data_save, pop_save,
+ * ini_step, n_gpus, resid_max -- with SchemeVarH's defaults and type checks.
+ * Extension keys carry the other compile-time constants the reference keeps in
+ * var.h, nnf.h and ibmVar.h: rho_0, u_max, ux_bc/uy_bc/uz_bc/rho_bc (lists),
+ * collision (regularized / bgk), eta_p, yield_stress, n_index, k_consistency,
+ * gamma_0, storage (f32 / f16 / bf16), device, builder (a VLBM_BUILDER_* name:
+ * periodic, plates_y, lid_driven, closed_box (default, the builder compiled by
+ * default), square_duct, duct_yz, lid_cavity_closed, plates_y_free_slip,
+ * plates_y_zouhe, circular_duct, annular_duct), outer_radius, inner_radius,
+ * outer_velocity, outer_rotation, inner_velocity, inner_rotation,
+ * checkpoint_save, load_checkpoint, checkpoint_folder, and a mapping `ibm`
+ * (max_iterations, stencil, thickness, movement_discretization, fluid_density,
+ * gx, gy, gz, wall_x/y/z, pp/pw_friction, pp/pw_restitution, particle/wall
+ * young and poisson, mesh_scale, breugem, particles_save, particles_nodes_save,
+ * export_forces, particle_density, spheres: a list of {diameter, center: [x,y,z],
+ * velocity, angular_velocity, density, movable}).  Other keys are ignored, as
+ * pydantic ignores them.  precision: double and n_gpus > 1 return
+ * VLBM_ERR_UNSUPPORTED; a malformed file or value VLBM_ERR_INVALID with the key
+ * and line in vlbm_last_error. */
+typedef struct vlbm_run_config {
+    vlbm_config cfg;             /* lattice and physics                            */
+    vlbm_ibm_config ibm;         /* IBM parameters (key `ibm`)                      */
+    int32_t builder;             /* VLBM_BUILDER_*                                  */
+    int32_t use_ibm;             /* use_ibm                                         */
+    int32_t precision_double;    /* precision == "double" (rejected)                */
+    int32_t n_gpus;              /* n_gpus (1)                                      */
+    int64_t steps;               /* steps (N_STEPS)                                 */
+    int64_t ini_step;            /* ini_step (INI_STEP)                             */
+    int64_t macr_save;           /* macr_save (MACR_SAVE; 0 = off)                  */
+    int64_t data_report;         /* data_report (DATA_REPORT; 0 = off)              */
+    int64_t checkpoint_save;     /* CHECKPOINT_SAVE (0 = off)                       */
+    int64_t particles_save;      /* IBM_PARTICLES_SAVE (0 = off)                    */
+    int32_t data_stop, data_save, pop_save, load_checkpoint;
+    int32_t particles_nodes_save;/* IBM_PARTICLES_NODES_SAVE                        */
+    int32_t export_forces;       /* EXPORT_FORCES                                   */
+    int32_t n_spheres;           /* entries under ibm.spheres                       */
+    int32_t reserved0;
+    double resid_max;            /* resid_max (RESID_MAX)                           */
+    double u_max;                /* U_MAX                                           */
+    char sim_id[32];             /* ID_SIM: sim_id as '%03d' (var.h.j2)              */
+    char path_save[256];         /* PATH_FILES                                      */
+    char load_folder[256];       /* SIMULATION_FOLDER_LOAD_CHECKPOINT               */
+    int32_t reserved[16];
+} vlbm_run_config;
+
+/* Parse YAML text (or read the file at `path`) into `out`; the spheres listed
+ * are written to `spheres` (up to max_spheres; out->n_spheres counts them all).
+ * Replaces pyvisc's read_configs + render (pyvisc/conf_handler.py:15-24,
+ * pyvisc/__main__.py:6-9) and the compile step. */
+vlbm_status vlbm_run_config_parse(const char* yaml_text, vlbm_run_config* out, vlbm_sphere* spheres,
+                                  int32_t max_spheres);
+vlbm_status vlbm_run_config_load(const char* path, vlbm_run_config* out, vlbm_sphere* spheres,
+                                 int32_t max_spheres);
 
 /* --------------------------------------------------------- checkpoint --- */
 /* Complete state of a simulation as one image (replaces operateSimCheckpoint /

@@ -131,15 +131,15 @@ double feq(int Q, int i, double rho, double ux, double uy, double uz) {
 double calc_omega(const OSim& s, double omegaOld, double auxStressMag) {
     const vlbm_config& c = s.cfg;
     if (c.rheology == VLBM_BINGHAM) {
-        double omegaP = 1.0 / (3.0 * c.eta_p + 0.5);           // nnf.h:128
-        return omegaP * std::max(0.0, 1.0 - c.yield_stress / auxStressMag);  // nnf.h:188
+        double omegaP = 1.0 / (3.0 * c.eta_p + 0.5);           // nnf.h:23
+        return omegaP * std::max(0.0, 1.0 - c.yield_stress / auxStressMag);  // nnf.h:83
     }
     if (c.rheology == VLBM_POWERLAW) {
-        double eta = ((1.0 / omegaOld) - 0.5) / 3.0;            // nnf.h:146
-        double gammaDot = (1.0 - 0.5 * omegaOld) * auxStressMag / eta;  // nnf.h:149
-        if (gammaDot <= c.gamma0) eta = c.k_consistency;        // nnf.h:151-153
-        else eta = c.k_consistency * std::pow(gammaDot, c.n_index - 1.0);  // nnf.h:155
-        return 1.0 / (0.5 + 3.0 * eta);                         // nnf.h:158
+        double eta = ((1.0 / omegaOld) - 0.5) / 3.0;            // nnf.h:41
+        double gammaDot = (1.0 - 0.5 * omegaOld) * auxStressMag / eta;  // nnf.h:44
+        if (gammaDot <= c.gamma0) eta = c.k_consistency;        // nnf.h:46-48
+        else eta = c.k_consistency * std::pow(gammaDot, c.n_index - 1.0);  // nnf.h:50
+        return 1.0 / (0.5 + 3.0 * eta);                         // nnf.h:53
     }
     return 1.0 / c.tau;                                         // var.h:105
 }

@@ -107,6 +107,59 @@ def free_slip_source(q, direction, i):
     return j, [off[0], off[1], off[2]]
 
 
+class Config(C.Structure):
+    """The oracle's configuration: the field layout of vlbm_config (include/vlbm.h),
+    which oracle.cpp reads, filled here without loading libvlbm so that CPU
+    baselines built on the oracle alone map no product library."""
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("vel_set", C.c_int32), ("collision", C.c_int32), ("rheology", C.c_int32),
+        ("storage", C.c_int32), ("device", C.c_int32),
+        ("tau", C.c_double), ("rho0", C.c_double),
+        ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double),
+        ("eta_p", C.c_double), ("yield_stress", C.c_double),
+        ("n_index", C.c_double), ("k_consistency", C.c_double), ("gamma0", C.c_double),
+        ("ux_bc", C.c_double * 8), ("uy_bc", C.c_double * 8),
+        ("uz_bc", C.c_double * 8), ("rho_bc", C.c_double * 8),
+        ("storage_scale", C.c_double),
+        ("layout", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+        ("duct_outer_radius", C.c_double), ("duct_inner_radius", C.c_double),
+        ("duct_outer_velocity", C.c_double), ("duct_outer_rotation", C.c_double),
+        ("duct_inner_velocity", C.c_double), ("duct_inner_rotation", C.c_double),
+    ]
+
+    @classmethod
+    def default(cls, **kw):
+        """Reference defaults (var.h:95-117, nnf.h:11-21), then the given fields."""
+        c = cls()
+        c.nx, c.ny, c.nz = 128, 128, 384
+        c.vel_set, c.tau, c.rho0 = 19, 0.6, 1.0
+        c.eta_p, c.yield_stress, c.n_index = 0.3, 1e-4, 0.5
+        c.k_consistency = c.rho0 * (c.tau - 0.5) / 3.0
+        u = 0.1
+        for i, (a, b, d) in enumerate(zip([0, u, 0, 0, 0, 0, 0, 0], [0, u / 2, -u / 2, 0, 0, 0, 0, 0],
+                                          [0, u, -u, 0, 0, 0, 0, 0])):
+            c.ux_bc[i], c.uy_bc[i], c.uz_bc[i], c.rho_bc[i] = a, b, d, 1.0
+        for k, v in kw.items():
+            if k in ("ux_bc", "uy_bc", "uz_bc", "rho_bc"):
+                arr = getattr(c, k)
+                for i, val in enumerate(v):
+                    arr[i] = val
+            else:
+                setattr(c, k, v)
+        return c
+
+
+def plates_y_map(nx, ny, nz):
+    """Node map of parallelPlatesBounceBack_Y.cu (bounce-back SOUTH at y=0, NORTH
+    at y=NY-1), vectorised; equal to reference_builder_map("plates_y", ...)."""
+    m = np.full((nz, ny, nx), USED, dtype=np.uint32)
+    m[:, 0, :] = _w(BB, S_)
+    m[:, ny - 1, :] = _w(BB, N_)
+    return m.ravel()
+
+
 class Oracle:
     """One lattice advanced by the FP64 restatement (reference push/AB scheme)."""
 
@@ -326,6 +379,39 @@ def _builder_word(name, x, y, z, NX, NY, NZ, outer_radius=None, inner_radius=Non
     if name in ("circular_duct", "annular_duct"):
         return _duct_word(name == "annular_duct", x, y, NX, NY, outer_radius, inner_radius)
     raise KeyError(name)
+
+
+FACE_CODES = {"NORTH": N_, "SOUTH": S_, "WEST": W_, "EAST": E_, "FRONT": F_, "BACK": B_}
+SCHEME_CODES = {"BC_SCHEME_VEL_ZOUHE": VELZH, "BC_SCHEME_PRES_ZOUHE": 3}
+
+
+def harness_map(face, scheme, nx, ny, nz):
+    """Node map of oracle/ref_harness_builder.cu: `scheme` on `face` with value
+    index 1 (UX_BC on west/east, UZ_BC on front/back, UY_BC on north/south,
+    RHO_BC for pressure), bounce-back walls on the faces normal to y (normal to
+    z when the face is north or south) taking the shared edges, the other axes
+    periodic.  [nz][ny][nx] uint32 in the reference's bit layout."""
+    d, s = FACE_CODES[face], SCHEME_CODES[scheme]
+    m = np.full((nz, ny, nx), USED, dtype=np.uint32)
+    if s == 3:
+        val = 1
+    elif d in (W_, E_):
+        val = 1 << UX_OFF
+    elif d in (F_, B_):
+        val = 1 << UZ_OFF
+    else:
+        val = 1 << UY_OFF
+    sel = {N_: (slice(None), ny - 1, slice(None)), S_: (slice(None), 0, slice(None)),
+           W_: (slice(None), slice(None), 0), E_: (slice(None), slice(None), nx - 1),
+           F_: (nz - 1, slice(None), slice(None)), B_: (0, slice(None), slice(None))}[d]
+    m[sel] = USED | (s << SCHEME_OFF) | (d << DIR_OFF) | val
+    if d in (N_, S_):
+        m[0, :, :] = _w(BB, B_)
+        m[nz - 1, :, :] = _w(BB, F_)
+    else:
+        m[:, 0, :] = _w(BB, S_)
+        m[:, ny - 1, :] = _w(BB, N_)
+    return m.ravel()
 
 
 INTERP, IS_SAVE = 6, 1 << 22

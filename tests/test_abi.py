@@ -34,7 +34,7 @@ def test_config_defaults_match_reference_var_h(vlbm):
     assert (c.nx, c.ny, c.nz) == (128, 128, 384)      # var.h:95-100
     assert c.vel_set == 19 and abs(c.tau - 0.6) < 1e-15 and c.rho0 == 1.0
     assert list(c.ux_bc)[:2] == [0.0, 0.1]            # var.h:114
-    assert abs(c.eta_p - 0.3) < 1e-15 and abs(c.yield_stress - 1e-4) < 1e-18  # nnf.h:125-126
+    assert abs(c.eta_p - 0.3) < 1e-15 and abs(c.yield_stress - 1e-4) < 1e-18  # nnf.h:20-21
     assert vlbm.lib().vlbm_abi_version() == 2
 
 

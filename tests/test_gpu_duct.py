@@ -112,3 +112,20 @@ def test_hagen_poiseuille(vlbm):
     ana = g * (R * R - r * r) / (4 * nu)
     err = np.linalg.norm((uz - ana)[inside]) / np.linalg.norm(ana[inside])
     assert err < 5e-3, err   # the FP64 oracle gives 1.8e-3 on this lattice
+
+
+def test_annular_duct_matches_reference_runs(vlbm):
+    """The reference's published D3Q19 annular-duct profiles (outer radius
+    NY/2 - 0.5, inner a quarter of it), run on the GPU in FP32: within 1e-5 of
+    the peak velocity."""
+    cases = json.load(open(os.path.join(HERE, "golden", "duct_interp_profiles.json")))["annular_cases"]
+    for c in cases:
+        ro = c["ny"] / 2.0 - 0.5
+        cfg = vlbm.Config.default(nx=c["nx"], ny=c["ny"], nz=c["nz"], vel_set=19, tau=c["tau"], fz=c["fz"],
+                                  duct_outer_radius=ro, duct_inner_radius=ro / 4.0)
+        sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_ANNULAR_DUCT)
+        sim.step(c["steps"])
+        uz = sim.macroscopics()["uz"][0].astype(np.float64)
+        sim.close()
+        ns = np.array([v for _, v in c["uz_north_south"]])
+        assert np.abs(uz[:, c["nx"] // 2] - ns).max() <= 1e-5 * ns.max(), c["id"]

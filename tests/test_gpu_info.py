@@ -37,3 +37,49 @@ def test_info_file_keys_and_values(vlbm, tmp_path):
     assert d["Model"] == "Bingham" and float(d["Plastic omega"]) == pytest.approx(1 / 0.8, rel=1e-6)
     assert d["Number of particles"] == "1" and d["IBM iterations"] == "2" and d["Stencil size"] == "4"
     assert "CUDA INFORMATION" in text and d["compute capability"] == "10.0"
+
+
+def read_macr(path, nx, ny, nz):
+    """Raw little-endian float32 [NZ][NY][NX], as fileTreat.readFileMacr3D reads it
+    (src/Post Processing/fileTreat.py:146-168)."""
+    a = np.fromfile(path, dtype="<f4")
+    assert a.size == nx * ny * nz, (path, a.size)
+    return a.reshape(nz, ny, nx)
+
+
+@pytest.mark.parametrize("rheology", [0, 2])
+def test_macr_bin_names_and_contents(vlbm, tmp_path, rheology):
+    """vlbm_write_macr_bin: getVarFilename's names (lbmReport.cpp:55-83; step 0 has
+    seven digits, later steps six) and the fields of vlbm_get_macroscopics."""
+    nx, ny, nz = 20, 12, 8
+    kw = dict(n_index=0.7, k_consistency=0.05) if rheology == 2 else {}
+    cfg = vlbm.Config.default(nx=nx, ny=ny, nz=nz, rheology=rheology, fx=2e-5, fz=-1e-5, **kw)
+    sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+    sim.write_macr_bin(str(tmp_path), "042", 0)
+    sim.step(37)
+    sim.sync()
+    sim.write_macr_bin(str(tmp_path), "042", 37)
+    m = sim.macroscopics()
+    sim.close()
+    names = ["rho", "ux", "uy", "uz"] + (["omega"] if rheology else [])
+    got = sorted(p.name for p in (tmp_path / "042").iterdir())
+    want = sorted([f"042_{v}0000000.bin" for v in names] + [f"042_{v}000037.bin" for v in names])
+    assert got == want
+    for v in names:
+        a = read_macr(tmp_path / "042" / f"042_{v}000037.bin", nx, ny, nz)
+        np.testing.assert_array_equal(a, m[v])
+    r0 = read_macr(tmp_path / "042" / "042_rho0000000.bin", nx, ny, nz)
+    np.testing.assert_array_equal(r0, np.ones_like(r0))
+    assert np.abs(m["ux"]).max() > 0
+
+
+def test_macr_bin_step_field(vlbm, tmp_path):
+    """Step fields of getVarFilename for steps of one to seven digits."""
+    cfg = vlbm.Config.default(nx=4, ny=4, nz=4)
+    sim = vlbm.Simulation(cfg)
+    cases = {1: "000001", 99: "000099", 12345: "012345", 100000: "100000", 999999: "999999",
+             1234567: "1234567"}
+    for step, field in cases.items():
+        sim.write_macr_bin(str(tmp_path), "s", step)
+        assert (tmp_path / "s" / f"s_rho{field}.bin").exists(), step
+    sim.close()

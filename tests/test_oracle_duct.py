@@ -42,3 +42,28 @@ def test_oracle_circular_duct_matches_reference_runs(vlbm, oracle, case):
     # the wall rule is the interpolated one: nodes next to the cylinder carry it
     interp = ((m >> 18) & 7) == 6
     assert interp.sum() > 0
+
+
+ANNULAR = json.load(open(os.path.join(HERE, "golden", "duct_interp_profiles.json")))["annular_cases"]
+
+
+def annular_radii(ny):
+    """The runs' cylinders: outer radius NY/2 - 0.5 (as the circular-duct runs)
+    and the inner radius a quarter of it (var.h:154, INNER_RADIUS = OUTER_RADIUS/4)."""
+    r_out = ny / 2.0 - 0.5
+    return r_out, r_out / 4.0
+
+
+@pytest.mark.parametrize("case", ANNULAR, ids=[c["id"] for c in ANNULAR])
+def test_oracle_annular_duct_matches_reference_runs(vlbm, oracle, case):
+    ro, ri = annular_radii(case["ny"])
+    cfg = vlbm.Config.default(nx=case["nx"], ny=case["ny"], nz=case["nz"], vel_set=19, tau=case["tau"],
+                              fz=case["fz"], duct_outer_radius=ro, duct_inner_radius=ri)
+    m = oracle.reference_builder_map("annular_duct", case["nx"], case["ny"], case["nz"], outer_radius=ro,
+                                     inner_radius=ri)
+    o = oracle.Oracle(cfg, m)
+    o.step(case["steps"])
+    uz = o.macroscopics()["uz"][0]
+    ns = np.array([v for _, v in case["uz_north_south"]])
+    assert np.abs(uz[:, case["nx"] // 2] - ns).max() <= 1e-6 * ns.max()
+    assert (ns == 0).sum() >= 3        # the line crosses the inner cylinder

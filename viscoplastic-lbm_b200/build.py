@@ -3,7 +3,9 @@
 Every .cu / .cpp file under csrc/ is compiled by nvcc with
 `-gencode arch=compute_100a,code=sm_100a`, in parallel, into _build/, and linked
 into viscoplastic-lbm_b200/libvlbm.so (static CUDA runtime).  Objects are
-rebuilt when their source or any csrc/ header is newer.
+rebuilt when their source or any csrc/ header is newer.  The drop-in host
+program driver/vlbm_run.cpp is then linked against it into
+viscoplastic-lbm_b200/vlbm_run.
 
 Usage: python viscoplastic-lbm_b200/build.py [-j N] [--force]
 """
@@ -18,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libvlbm.so")
+DRIVER = os.path.join(HERE, "vlbm_run")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -79,6 +82,15 @@ def build(jobs=None, force=False, verbose_ptxas=False, quiet=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    drv_src = os.path.join(HERE, "driver", "vlbm_run.cpp")
+    if os.path.exists(drv_src) and (not os.path.exists(DRIVER) or os.path.getmtime(DRIVER) < max(
+            os.path.getmtime(LIB), os.path.getmtime(drv_src), newest_header())):
+        # the drop-in host program, linked against the library next to it
+        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", INCLUDE, drv_src, "-o", DRIVER, "-L", HERE, "-lvlbm",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
     if not quiet:
         print(f"built {LIB} from {len(objs)} objects")
     return LIB, "\n".join(logs)

@@ -14,6 +14,32 @@ namespace vlbm {
 
 static thread_local std::string g_last_error;
 
+// Step field of getVarFilename (lbmReport.cpp:55-83): the zeros counted by its
+// loop (k >= 1 while step * 10^k < 10^6, unsigned arithmetic), then the step;
+// step 0 gets six zeros before its "0", so the first save reads
+// ..._rho0000000.bin and later ones ..._rho000100.bin.
+std::string step_field(uint32_t step) {
+    std::string num;
+    if (step == 0) {
+        num = "000000";
+    } else {
+        uint32_t pot = 10;
+        for (int k = 0; k < 12 && step * pot < 1000000u; ++k, pot *= 10) num.push_back('0');
+    }
+    return num + std::to_string(step);
+}
+
+// mkdir -p (folderSetup, lbmReport.cpp:25-52)
+void mkdir_p(const std::string& dir) {
+    std::string acc;
+    for (size_t k = 0; k <= dir.size(); ++k) {
+        if (k == dir.size() || dir[k] == '/') {
+            if (!acc.empty()) mkdir(acc.c_str(), 0777);
+        }
+        if (k < dir.size()) acc.push_back(dir[k]);
+    }
+}
+
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 vlbm_status cuda_status(cudaError_t e, const char* what) {
@@ -73,7 +99,7 @@ StepParams make_params(vlbm_sim* s) {
     p.ctr = s->step_ctr;
     p.omega_newt = (float)(1.0 / c.tau);                 // var.h:105 OMEGA
     p.fx = (float)c.fx; p.fy = (float)c.fy; p.fz = (float)c.fz;
-    p.omega_p = (float)(1.0 / (3.0 * c.eta_p + 0.5));    // nnf.h:128 OMEGA_P
+    p.omega_p = (float)(1.0 / (3.0 * c.eta_p + 0.5));    // nnf.h:23 OMEGA_P
     p.yield = (float)c.yield_stress;
     p.n_index = (float)c.n_index;
     p.k_cons = (float)c.k_consistency;
@@ -271,11 +297,11 @@ vlbm_status vlbm_config_default(vlbm_config* c) {
     c->device = 0;
     c->tau = 0.6;                          // var.h:104
     c->rho0 = 1.0;                         // var.h:107
-    c->eta_p = 0.3;                        // nnf.h:125
-    c->yield_stress = 1e-4;                // nnf.h:126
-    c->n_index = 0.5;                      // nnf.h:116
-    c->k_consistency = c->rho0 * (c->tau - 0.5) / 3.0;  // nnf.h:117
-    c->gamma0 = 0.0;                       // nnf.h:118
+    c->eta_p = 0.3;                        // nnf.h:20
+    c->yield_stress = 1e-4;                // nnf.h:21
+    c->n_index = 0.5;                      // nnf.h:11
+    c->k_consistency = c->rho0 * (c->tau - 0.5) / 3.0;  // nnf.h:12
+    c->gamma0 = 0.0;                       // nnf.h:13
     const double umax = 0.1;               // var.h:102 U_MAX
     const double ux[8] = {0, umax, 0, 0, 0, 0, 0, 0};            // var.h:114
     const double uy[8] = {0, umax / 2, -umax / 2, 0, 0, 0, 0, 0}; // var.h:115
@@ -590,18 +616,9 @@ vlbm_status vlbm_write_macr_bin(vlbm_sim* s, const char* path_files, const char*
     bool nnf = s->cfg.rheology != VLBM_NEWTONIAN;
     vlbm_status st = vlbm_get_macroscopics(s, rho.data(), ux.data(), uy.data(), uz.data(), nnf ? om.data() : nullptr);
     if (st != VLBM_OK) return st;
-    std::string dir = std::string(path_files) + "/" + id_sim;
-    {   // mkdir -p (folderSetup, lbmReport.cpp:25-52)
-        std::string acc;
-        for (size_t k = 0; k <= dir.size(); ++k) {
-            if (k == dir.size() || dir[k] == '/') {
-                if (!acc.empty()) mkdir(acc.c_str(), 0777);
-            }
-            if (k < dir.size()) acc.push_back(dir[k]);
-        }
-    }
-    char num[32];
-    std::snprintf(num, sizeof(num), "%06u", step_label);
+    const std::string dir = std::string(path_files) + "/" + id_sim;
+    vlbm::mkdir_p(dir);
+    const std::string num = vlbm::step_field(step_label);
     auto write = [&](const char* var, const float* data) -> vlbm_status {
         std::string fn = dir + "/" + id_sim + "_" + var + num + ".bin";
         FILE* f = std::fopen(fn.c_str(), "wb");

@@ -40,7 +40,7 @@ namespace vlbm {
 namespace {
 
 constexpr char kMagic[8] = {'V', 'L', 'B', 'M', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kVersion = 1;
+constexpr uint32_t kVersion = 2;   // 2: FP32 populations stored as deviations f_i - w_i rho0
 
 struct CkptHeader {
     char magic[8];

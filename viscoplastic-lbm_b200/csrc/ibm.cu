@@ -1201,4 +1201,65 @@ vlbm_status vlbm_get_lagrangian_nodes(vlbm_sim* s, double* pos, double* force, s
     return VLBM_OK;
 }
 
+// saveParticlesInfo (IBM/ibmReport.cpp:26-102): the particle centres and,
+// optionally, the Lagrangian nodes as CSV, numbers in std::scientific (%e).
+// Spheres carry the collision semi-axes (r, r, r), (0, 0, 0), (0, 0, 0) of
+// makeSpherePolar (particle.cpp:778).
+vlbm_status vlbm_write_particles_csv(vlbm_sim* s, const char* path_files, const char* id_sim, uint32_t step_label,
+                                     int32_t save_nodes) {
+    if (!s || !path_files || !id_sim) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    if (!s->ibm) { set_last_error("no spheres in this simulation"); return VLBM_ERR_STATE; }
+    IbmState* st = s->ibm;
+    IBM_CUDA(cudaSetDevice(s->device));
+    std::vector<DPart> h(st->np);
+    IBM_CUDA(cudaMemcpyAsync(h.data(), st->parts, h.size() * sizeof(DPart), cudaMemcpyDeviceToHost, s->stream));
+    const size_t nn = (size_t)st->nnodes;
+    std::vector<double> px(nn), py(nn), pz(nn), pS(nn);
+    std::vector<int> pid(nn);
+    if (save_nodes) {
+        IBM_CUDA(cudaMemcpyAsync(px.data(), st->nx, nn * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(py.data(), st->ny, nn * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(pz.data(), st->nz, nn * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(pS.data(), st->nS, nn * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        IBM_CUDA(cudaMemcpyAsync(pid.data(), st->npid, nn * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    }
+    IBM_CUDA(cudaStreamSynchronize(s->stream));
+    const std::string dir = std::string(path_files) + "/" + id_sim;
+    mkdir_p(dir);
+    const std::string stem = dir + "/" + id_sim + "_";
+    const std::string num = step_field(step_label);
+    {
+        const std::string fn = stem + "pCenters" + num + ".csv";
+        FILE* f = std::fopen(fn.c_str(), "w");
+        if (!f) { set_last_error("cannot open " + fn); return VLBM_ERR_IO; }
+        std::fprintf(f, "p_number,step,pos_x,pos_y,pos_z,vel_x,vel_y,vel_z,w_x,w_y,w_z,f_x,f_y,f_z,M_x,M_y,M_z,"
+                        "I_xx,I_yy,I_zz,I_xy,I_xz,I_yz,S,radius,volume,movable,semi1x,semi1y,semi1z,"
+                        "semi2x,semi2y,semi2z,semi3x,semi3y,semi3z\n");
+        for (int k = 0; k < st->np; ++k) {
+            const DPart& p = h[k];
+            std::fprintf(f, "%d,%u", k, step_label);
+            const double* v3[5] = {p.pos, p.vel, p.w, p.f, p.M};
+            for (const double* v : v3) std::fprintf(f, ",%e,%e,%e", v[0], v[1], v[2]);
+            for (int a = 0; a < 6; ++a) std::fprintf(f, ",%e", p.I[a]);
+            std::fprintf(f, ",%e,%e,%e,%d", p.S, p.radius, p.volume, p.movable ? 1 : 0);
+            std::fprintf(f, ",%e,%e,%e,%e,%e,%e,%e,%e,%e\n", p.radius, p.radius, p.radius, 0.0, 0.0, 0.0, 0.0,
+                         0.0, 0.0);
+        }
+        const bool bad = std::ferror(f) != 0;
+        std::fclose(f);
+        if (bad) { set_last_error("write failed " + fn); return VLBM_ERR_IO; }
+    }
+    if (save_nodes) {
+        const std::string fn = stem + "pNodes" + num + ".csv";
+        FILE* f = std::fopen(fn.c_str(), "w");
+        if (!f) { set_last_error("cannot open " + fn); return VLBM_ERR_IO; }
+        std::fprintf(f, "particle_index,pos_x,pos_y,pos_z,S\n");
+        for (size_t i = 0; i < nn; ++i) std::fprintf(f, "%d,%e,%e,%e,%e\n", pid[i], px[i], py[i], pz[i], pS[i]);
+        const bool bad = std::ferror(f) != 0;
+        std::fclose(f);
+        if (bad) { set_last_error("write failed " + fn); return VLBM_ERR_IO; }
+    }
+    return VLBM_OK;
+}
+
 }  // extern "C"

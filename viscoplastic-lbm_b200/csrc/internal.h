@@ -106,5 +106,7 @@ bool builder_word(int builder, int x, int y, int z, int nx, int ny, int nz, uint
 int bb_role(int dir, int i);
 
 void set_last_error(const std::string& msg);
+std::string step_field(uint32_t step);      // getVarFilename's step digits (capi.cu)
+void mkdir_p(const std::string& dir);       // folderSetup's mkdir -p (capi.cu)
 
 }  // namespace vlbm

@@ -71,15 +71,21 @@ __device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, unsigned r) {
 // post-collision deviation directly.  Summing full populations instead (values
 // w_i + small, whose trailing bits are those of w_i on every node) makes the
 // FP32 rounding of rho systematic: with half-precision storage that created
-// ~1e-7 of mass per node and step.  FP32 storage keeps the populations
-// themselves (the reference's state); half storage keeps g_i * scale.
+// ~1e-7 of mass per node and step.  Every storage keeps deviations: FP32 g_i,
+// half precision g_i * scale.  Storing the full FP32 population (the
+// reference's state, ~w_i) would round the increments a slow flow gets every
+// step (~1e-7 against an ulp of ~4e-9 at f ~ 0.05) on every store; the
+// rounding bias built up to a -0.5 % velocity error in a 64x32x32 BGK
+// Poiseuille channel at u ~ 1e-3 (the reference's own FP32 build: +0.2 %;
+// FP64: 1e-4).  A deviation (~1e-4 there) keeps those increments to FP32
+// precision.  Entry points that take or return populations convert.
 template <int ST> struct Store;
 template <> struct Store<VLBM_STORE_F32> {
     using T = float;
-    static __device__ __forceinline__ float ld(const T* p, float w, const StepParams& s) { return *p - w * s.rho0; }
-    static __device__ __forceinline__ void st(T* p, float g, float w, const StepParams& s, Rng&) { *p = g + w * s.rho0; }
+    static __device__ __forceinline__ float ld(const T* p, float, const StepParams&) { return *p; }
+    static __device__ __forceinline__ void st(T* p, float g, float, const StepParams&, Rng&) { *p = g; }
     // a full population (initial state, user state)
-    static __device__ __forceinline__ void st_abs(T* p, float v, float, const StepParams&) { *p = v; }
+    static __device__ __forceinline__ void st_abs(T* p, float v, float w, const StepParams& s) { *p = v - w * s.rho0; }
 };
 template <> struct Store<VLBM_STORE_F16> {
     using T = __half;
@@ -691,15 +697,16 @@ __global__ void __launch_bounds__(256) k_step(const StepParams p) {
 // advance in one launch.  The launch walks a table of tiles (lattice slot,
 // first node; BATCH_TILE consecutive nodes each) with a grid-stride loop, so a
 // grid of a few blocks per SM is persistent over all lattices.  The lattices'
-// parameters are the launch's own arguments (constant bank, no shared-memory
-// copy and no barrier per tile).  Lattices whose
+// parameters sit in a device-resident BatchLaunch table whose address is the
+// launch's argument; a block copies a lattice's parameters into shared memory
+// when its tile belongs to another lattice than its previous one.  Lattices whose
 // AA parity differs go to different tables (the parity is a template argument,
 // as in k_step); the side-store buffer index and the boundary flag of every
 // lattice live in its slot in device memory and are advanced by
 // k_batch_advance after the group launches, so a captured step can be
 // replayed any number of times.
 constexpr int BATCH_TILE = 256;
-constexpr int BATCH_MAX_SLOTS = 64;   // lattices per launch (their parameters are the launch's arguments)
+constexpr int BATCH_MAX_SLOTS = 64;   // lattices per launch (parameters in one BatchLaunch table)
 
 // Per-lattice state that changes every step (advanced by k_batch_advance).
 struct BatchState {
@@ -865,21 +872,16 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
 template <int ST> struct Pair;
 template <> struct Pair<VLBM_STORE_F32> {
     using V = float2;
-    static __device__ __forceinline__ float get(const V& v, int lane, float w, const StepParams& s) {
-        return (lane ? v.y : v.x) - w * s.rho0;
+    static __device__ __forceinline__ float get(const V& v, int lane, float, const StepParams&) {
+        return lane ? v.y : v.x;
     }
-    static __device__ __forceinline__ void set(V& v, int lane, float g, float w, const StepParams& s, Rng&) {
-        const float f = g + w * s.rho0;
-        if (lane) v.y = f; else v.x = f;
+    static __device__ __forceinline__ void set(V& v, int lane, float g, float, const StepParams&, Rng&) {
+        if (lane) v.y = g; else v.x = g;
     }
     static __device__ __forceinline__ V swap(const V& v) { return make_float2(v.y, v.x); }
-    // both lanes as deviations / packed from deviations
-    static __device__ __forceinline__ float2 get2(const V& v, float w, const StepParams& s) {
-        return sub2(v, f2(w * s.rho0));
-    }
-    static __device__ __forceinline__ V pack2(float2 g, float w, const StepParams& s, Rng&, Rng&) {
-        return add2(g, f2(w * s.rho0));
-    }
+    // both lanes as deviations / packed from deviations (stored as they are)
+    static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams&) { return v; }
+    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams&, Rng&, Rng&) { return g; }
 };
 template <> struct Pair<VLBM_STORE_F16> {
     using V = __half2;

@@ -22,8 +22,8 @@ if not os.path.exists(_LIB_PATH):
 _lib = C.CDLL(_LIB_PATH)
 
 # ----------------------------------------------------------------- enums --
-OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE, \
-    ERR_TIMEOUT, ERR_NOT_FOUND, ERR_IO = range(10)
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE = range(7)
+ERR_NOT_FOUND, ERR_IO = 8, 9
 D3Q19, D3Q27 = 19, 27
 OP_REGULARIZED, OP_BGK = 0, 1
 NEWTONIAN, BINGHAM, POWERLAW = 0, 1, 2
@@ -169,6 +169,22 @@ class Completion(C.Structure):
     ]
 
 
+class RunConfig(C.Structure):
+    """vlbm_run_config (include/vlbm.h): the drop-in driver's configuration,
+    read from the reference's pyvisc YAML file."""
+    _fields_ = [
+        ("cfg", Config), ("ibm", IbmConfig), ("builder", C.c_int32), ("use_ibm", C.c_int32),
+        ("precision_double", C.c_int32), ("n_gpus", C.c_int32),
+        ("steps", C.c_int64), ("ini_step", C.c_int64), ("macr_save", C.c_int64), ("data_report", C.c_int64),
+        ("checkpoint_save", C.c_int64), ("particles_save", C.c_int64),
+        ("data_stop", C.c_int32), ("data_save", C.c_int32), ("pop_save", C.c_int32), ("load_checkpoint", C.c_int32),
+        ("particles_nodes_save", C.c_int32), ("export_forces", C.c_int32), ("n_spheres", C.c_int32),
+        ("reserved0", C.c_int32), ("resid_max", C.c_double), ("u_max", C.c_double),
+        ("sim_id", C.c_char * 32), ("path_save", C.c_char * 256), ("load_folder", C.c_char * 256),
+        ("reserved", C.c_int32 * 16),
+    ]
+
+
 _P = C.c_void_p
 _F32P = C.POINTER(C.c_float)
 _U32P = C.POINTER(C.c_uint32)
@@ -199,6 +215,9 @@ _SIGS = {
     "vlbm_get_lagrangian_nodes": [_P, _F64P, _F64P, C.c_size_t],
     "vlbm_write_macr_bin": [_P, C.c_char_p, C.c_char_p, C.c_uint32, C.c_int32],
     "vlbm_write_info": [_P, C.c_char_p, C.c_char_p, C.c_uint64, C.c_double, C.c_int32, C.c_int32, C.c_double],
+    "vlbm_write_particles_csv": [_P, C.c_char_p, C.c_char_p, C.c_uint32, C.c_int32],
+    "vlbm_run_config_parse": [C.c_char_p, C.POINTER(RunConfig), C.POINTER(Sphere), C.c_int32],
+    "vlbm_run_config_load": [C.c_char_p, C.POINTER(RunConfig), C.POINTER(Sphere), C.c_int32],
     "vlbm_checkpoint_save": [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)],
     "vlbm_checkpoint_load": [_P, _P, C.c_size_t],
     "vlbm_save_checkpoint": [_P, C.c_char_p, C.c_char_p],
@@ -247,6 +266,23 @@ def lib_path():
 
 def _fptr(a):
     return a.ctypes.data_as(_F32P)
+
+
+def load_run_config(path=None, text=None):
+    """Read a pyvisc YAML configuration (file `path` or string `text`):
+    returns (RunConfig, [Sphere])."""
+    rc = RunConfig()
+    fn, arg = (_lib.vlbm_run_config_load, path.encode()) if path is not None else \
+        (_lib.vlbm_run_config_parse, text.encode())
+    _check(fn(arg, C.byref(rc), None, 0), "vlbm_run_config")
+    spheres = (Sphere * max(1, rc.n_spheres))()
+    _check(fn(arg, C.byref(rc), spheres, rc.n_spheres), "vlbm_run_config")
+    return rc, list(spheres)[:rc.n_spheres]
+
+
+def driver_path():
+    """The drop-in host program built next to the library (driver/vlbm_run.cpp)."""
+    return os.path.join(_HERE, "vlbm_run")
 
 
 def build_node_map(builder, nx, ny, nz):
@@ -358,6 +394,10 @@ class Simulation:
                                               frc.ctypes.data_as(_F64P), n),
                "vlbm_get_lagrangian_nodes")
         return pos.reshape(3, n), frc.reshape(3, n)
+
+    def write_particles_csv(self, path_files, id_sim, step_label, save_nodes=True):
+        _check(_lib.vlbm_write_particles_csv(self._h, path_files.encode(), id_sim.encode(), step_label,
+                                             int(save_nodes)), "vlbm_write_particles_csv")
 
     def write_macr_bin(self, path_files, id_sim, step_label, export_forces=False):
         _check(_lib.vlbm_write_macr_bin(self._h, path_files.encode(), id_sim.encode(),
