@@ -219,6 +219,47 @@ def cube_leg(vlbm, torch, device, steps=200, warmup=10, n=256):
     return out
 
 
+def cavity_leg(vlbm, torch, device, steps=200, warmup=10, n=256):
+    """The Power-Law lid-driven cavity: D3Q27 regularized, closed box of n^3
+    nodes (all six faces half-way bounce-back, the lid y = NY-1 moving at
+    u = 0.05 in x), flow index 0.5 / 1.0 / 1.5 with the consistency that makes
+    Re = U^(2-n) L^n / K = 400 (L = n nodes), FP32 / FP16 / BF16 deviation
+    storage, AUTO layout and an autotuned launch.  MLUPS and the fraction of the
+    measured copy bandwidth for the 2*Q*s population bytes (the Power-Law
+    viscosity state adds 8 B per node, reported beside them)."""
+    peak, _ = measured_peak()
+    out = {"lattice": f"{n}x{n}x{n}", "steps": steps, "velocity_set": "D3Q27", "re": 400, "lid_u": 0.05}
+    for n_index in (0.5, 1.0, 1.5):
+        k = 0.05 ** (2.0 - n_index) * n ** n_index / 400.0
+        for name, st in (("f32", vlbm.STORE_F32), ("f16", vlbm.STORE_F16), ("bf16", vlbm.STORE_BF16)):
+            cfg = vlbm.Config.default(nx=n, ny=n, nz=n, vel_set=27, collision=vlbm.OP_REGULARIZED,
+                                      rheology=vlbm.POWERLAW, n_index=n_index, k_consistency=k, gamma0=0.0,
+                                      ux_bc=[0, 0.05], storage=st)
+            cfg.device = device
+            sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_LID_CAVITY_CLOSED)
+            stream = torch.cuda.Stream()
+            sim.set_stream(stream.cuda_stream)
+            variant = sim.autotune()
+            sim.init_equilibrium(1.0, 0, 0, 0)
+            sim.step(warmup)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.step(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sim.sync()
+            ms = e0.elapsed_time(e1)
+            bpn = sim.info().bytes_per_node_step
+            mlups = n ** 3 * steps / (ms / 1e3) / 1e6
+            gbs = bpn * mlups * 1e6 / 1e9
+            out[f"n{n_index}_{name}"] = {"mlups": mlups, "achieved_gbs": gbs, "frac": gbs / peak,
+                                         "bytes_per_node": bpn, "state_bytes_per_node": 8, "k_consistency": k,
+                                         "variant": variant}
+            sim.close()
+    return out
+
+
 def sphere_pack(n, radius, box, gap=1.0, seed=42):
     """Non-overlapping sphere centres by rejection sampling: at least `gap`
     lattice units between spheres and to the walls (numpy default_rng(seed))."""
@@ -442,6 +483,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 D3Q19/D3Q27 FP32/FP16 leg")
     ap.add_argument("--no-ibm", action="store_true", help="skip the 64-sphere IBM leg")
+    ap.add_argument("--no-cavity", action="store_true", help="skip the 256^3 Power-Law lid-cavity leg")
     ap.add_argument("--vel-set", type=int, default=19, choices=[19, 27])
     ap.add_argument("--size", type=int, nargs=3, default=[256, 128, 64], metavar=("NX", "NY", "NZ"))
     ap.add_argument("--e2e-steps", type=int, default=3000,
@@ -543,6 +585,9 @@ def main():
     cube = None
     if rank == 0 and world == 1 and not args.no_cube:
         cube = cube_leg(vlbm, torch, local)
+    cavity = None
+    if rank == 0 and world == 1 and not args.no_cavity:
+        cavity = cavity_leg(vlbm, torch, local)
     ibm_run = None
     if rank == 0 and world == 1 and not args.no_ibm:
         ibm_run = ibm_leg(vlbm, torch, local)
@@ -570,6 +615,7 @@ def main():
             "kernel_variant": variant,
             "clocks": clk,
             "lattice_256": cube,
+            "powerlaw_cavity_256": cavity,
             "ibm_64_spheres": ibm_run,
             "serving": serving,
         }

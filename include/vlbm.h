@@ -470,7 +470,9 @@ vlbm_status vlbm_server_fetch(vlbm_server* srv, uint64_t tag, float* ux, size_t 
  * included), [3] waiting for the GPU (queue depth limit, idle read-outs),
  * [4] completing read-outs; then [5] batch steps, [6] kernels launched
  * directly, [7] graph launches, [8] graph captures, [9] host seconds in graph
- * captures (part of [2]).  Writes min(n, 10) values. */
+ * captures (part of [2]); then the device bytes of the server's memory cache,
+ * [10] held by resident and retiring lattices and [11] cached for reuse (their
+ * sum stays within the HBM budget).  Writes min(n, 12) values. */
 vlbm_status vlbm_server_profile(vlbm_server* srv, double* seconds, int32_t n);
 /* Tuning: sphere-free lattices with at least `nodes` nodes get their own
  * single-lattice launch each step instead of sharing the batched launch.

@@ -135,8 +135,14 @@ double calc_omega(const OSim& s, double omegaOld, double auxStressMag) {
         return omegaP * std::max(0.0, 1.0 - c.yield_stress / auxStressMag);  // nnf.h:83
     }
     if (c.rheology == VLBM_POWERLAW) {
-        double eta = ((1.0 / omegaOld) - 0.5) / 3.0;            // nnf.h:41
-        double gammaDot = (1.0 - 0.5 * omegaOld) * auxStressMag / eta;  // nnf.h:44
+        // nnf.h:41-44: eta_old = (1/omega_old - 1/2)/3, gammaDot = (1 - omega_old/2)|S|/eta_old.
+        // Since 1 - omega_old/2 = 3 omega_old eta_old, gammaDot = 3 omega_old |S|: the same value
+        // in exact arithmetic, evaluated in that form because the quotient is 0/0 where
+        // omega_old rounds to 2 (shear-thickening fluid at rest), and omega_old = 0 (the
+        // initial state, lbmInitialization.cu:111) gives gammaDot = 0 as the reference's
+        // |S|/inf does.
+        double eta;
+        const double gammaDot = 3.0 * omegaOld * auxStressMag;
         if (gammaDot <= c.gamma0) eta = c.k_consistency;        // nnf.h:46-48
         else eta = c.k_consistency * std::pow(gammaDot, c.n_index - 1.0);  // nnf.h:50
         return 1.0 / (0.5 + 3.0 * eta);                         // nnf.h:53

@@ -179,3 +179,28 @@ def test_many_lattices_share_persistent_blocks(vlbm):
         np.testing.assert_array_equal(srv.fetch(k, kw["nx"] * kw["ny"] * kw["nz"]),
                                       alone_in_server(vlbm, kw, 5, 40 + k, []), err_msg=f"request {k}")
     srv.close()
+
+
+def test_device_footprint_stays_within_budget(vlbm):
+    """Live and cached device bytes of the server's memory cache stay at or
+    below the HBM budget through admit / retire cycles of lattices of
+    different sizes (the cache frees what it holds beyond the budget)."""
+    budget = int(request_bytes(19, 40, 32, 32) * 1.3)
+    srv = vlbm.Server(device=0, hbm_budget_bytes=budget, max_resident=8)
+    sizes = [(40, 32, 32), (24, 24, 24), (36, 30, 28), (16, 40, 40), (40, 32, 32), (20, 20, 20)]
+    for tag, (nx, ny, nz) in enumerate(sizes):
+        srv.submit(cfg_of(vlbm, dict(nx=nx, ny=ny, nz=nz, tau=0.8, fx=1e-5)), vlbm.BUILDER_PLATES_Y, 30 + 5 * tag, tag)
+    done, peak = [], 0.0
+    for _ in range(2000):
+        done += srv.pump(5)
+        p = srv.profile()
+        held = p["device_live_bytes"] + p["device_cached_bytes"]
+        peak = max(peak, held)
+        assert held <= budget, (held, budget)
+        st = srv.stats()
+        if st["resident"] == 0 and st["queued"] == 0:
+            break
+    assert sorted(c.tag for c in done) == list(range(len(sizes)))
+    assert all(c.status == vlbm.OK for c in done)
+    assert peak > 0
+    srv.close()

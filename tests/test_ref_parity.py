@@ -39,7 +39,15 @@ REF = os.path.join(REPO, "oracle", "_ref")
 
 # velocity relative L2 bounds per comparison
 REF64_VS_ORACLE = 1e-9    # both FP64, different summation orders
-LIB_VS_REF64 = 1e-4       # the library's FP32 error
+# Power-Law: the reference evaluates gammaDot = (1 - omega/2)|S| / ((1/omega - 1/2)/3)
+# (nnf.h:41-44), whose difference 1/omega - 1/2 cancels as omega nears 2; the
+# oracle evaluates the equal 3 omega |S|.  FP64 round-off amplified by that
+# cancellation over thousands of steps: measured 3e-8 (n = 0.5), 3e-14 (n = 1.5).
+REF64_VS_ORACLE_POWERLAW = 1e-7
+# the library's FP32 error: relative L2 <= 1e-4, or an RMS velocity error of at
+# most 2e-7 (FP32 resolution of the populations) in flows slower than ~2e-3
+LIB_VS_REF64 = 1e-4
+LIB_VS_REF64_RMS = 2e-7
 RHO_LIB_REF64 = 1e-5      # density max abs, library vs reference FP64
 # libvlbm vs reference FP32: within the reference's own FP32 error (reference
 # FP32 vs FP64) plus the library's, with a margin
@@ -115,6 +123,11 @@ def u_rel(a, b):
     return float(du / nb)
 
 
+def u_rms_err(a, b):
+    du = sum(np.sum((a[k].astype(np.float64) - b[k]) ** 2) for k in ("ux", "uy", "uz"))
+    return float(np.sqrt(du / a["ux"].size))
+
+
 def rho_max(a, b):
     return float(np.abs(a["rho"].astype(np.float64) - b["rho"]).max())
 
@@ -128,7 +141,8 @@ def test_matches_reference_build(vlbm, oracle, case, tmp_path):
     oracle.set_threads(os.cpu_count() or 1)
     fp64 = run_oracle(oracle, case)
     res = dict(ref64_fp64=u_rel(ref64, fp64), lib_ref64=u_rel(lib, ref64), ref32_ref64=u_rel(ref32, ref64),
-               lib_ref32=u_rel(lib, ref32), rho_lib_ref64=rho_max(lib, ref64), rho_ref32_ref64=rho_max(ref32, ref64),
+               lib_ref32=u_rel(lib, ref32), lib_ref64_rms=u_rms_err(lib, ref64),
+               rho_lib_ref64=rho_max(lib, ref64), rho_ref32_ref64=rho_max(ref32, ref64),
                u_max=float(max(np.abs(ref64[k]).max() for k in ("ux", "uy", "uz"))))
     if "omega" in ref64:
         scale = float(np.abs(ref64["omega"]).max())
@@ -139,8 +153,9 @@ def test_matches_reference_build(vlbm, oracle, case, tmp_path):
         for k in ("rho", "ux", "uy", "uz"):
             assert np.all(np.isfinite(f[k])), f"{name} {k} not finite"
     assert res["u_max"] > 1e-4
-    assert res["ref64_fp64"] <= REF64_VS_ORACLE, res
-    assert res["lib_ref64"] <= LIB_VS_REF64, res
+    tol = REF64_VS_ORACLE_POWERLAW if ref_cases.CASES[case]["rheo"] == "powerlaw" else REF64_VS_ORACLE
+    assert res["ref64_fp64"] <= tol, res
+    assert res["lib_ref64"] <= LIB_VS_REF64 or res["lib_ref64_rms"] <= LIB_VS_REF64_RMS, res
     assert res["rho_lib_ref64"] <= RHO_LIB_REF64, res
     assert res["lib_ref32"] <= LIB_VS_REF32_FACTOR * res["ref32_ref64"] + LIB_VS_REF32_FLOOR, res
     if "omega_mean" in res:

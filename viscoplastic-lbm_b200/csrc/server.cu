@@ -123,22 +123,29 @@ struct Group {
 // Device memory cache of the server.  Buffers released by retired lattices are
 // kept and handed out again (best fit, at most 25 % + 2 MiB larger than asked);
 // only trim() calls cudaFree.  A buffer is released only after the GPU has
-// finished with its lattice (its read-out event completed).
+// finished with its lattice (its read-out event completed).  The device memory
+// the cache holds, live and cached together, stays within `cap` (the server's
+// HBM budget) as long as the live buffers fit in it: a larger cached buffer is
+// handed out only when it fits, and cached buffers are freed before a new
+// allocation would pass the cap.
 struct DevCache final : DeviceAllocator {
     std::multimap<size_t, void*> free_;
     std::unordered_map<void*, size_t> size_of;
     size_t free_bytes = 0, live_bytes = 0;
+    size_t cap = ~(size_t)0;
 
     cudaError_t allocate(void** p, size_t bytes) override {
         const size_t need = (bytes + 511) & ~(size_t)511;
         auto it = free_.lower_bound(need);
-        if (it != free_.end() && it->first <= need + need / 4 + ((size_t)2 << 20)) {
+        if (it != free_.end() && it->first <= need + need / 4 + ((size_t)2 << 20) &&
+            (it->first == need || live_bytes + it->first <= cap)) {
             *p = it->second;
             free_bytes -= it->first;
             live_bytes += it->first;
             free_.erase(it);
             return cudaSuccess;
         }
+        if (free_bytes + live_bytes + need > cap) trim(cap > live_bytes + need ? cap - live_bytes - need : 0);
         cudaError_t e = cudaMalloc(p, need);
         if (e == cudaErrorMemoryAllocation && !free_.empty()) {   // give the cached buffers back and retry
             cudaGetLastError();
@@ -224,7 +231,7 @@ struct vlbm_server {
     double lattice_updates = 0.0;
     // admit, rebuild, enqueue (incl. graph captures), wait, read-out [s];
     // batch steps, direct kernel launches, graph launches, graph captures
-    double prof[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double prof[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // batch tables (rebuilt when the membership changes)
     bool dirty = true;
     BatchState* d_state = nullptr;
@@ -696,7 +703,9 @@ void fail_request(vlbm_server* sv, const Pending& p, vlbm_status st) {
 vlbm_status server_admit(vlbm_server* sv) {
     while (!sv->queue.empty() && (int)sv->res.size() < sv->max_resident) {
         Pending& p = sv->queue.front();
-        if (sv->bytes_in_use + p.bytes > sv->budget) break;
+        // admission by the budget: the estimate of the resident lattices, or the
+        // buffers they actually hold (best-fit reuse can hand out a little more)
+        if (std::max(sv->bytes_in_use, sv->cache.live_bytes) + p.bytes > sv->budget) break;
         vlbm_config cfg = p.req.cfg;
         cfg.device = sv->device;
         cfg.layout = VLBM_LAYOUT_NATURAL;   // the batched kernel streams one node per thread
@@ -839,6 +848,7 @@ vlbm_status vlbm_server_create(int device, size_t budget, int32_t max_resident, 
     vlbm_server* sv = new vlbm_server();
     sv->device = device;
     sv->budget = budget;
+    sv->cache.cap = budget;
     sv->max_resident = max_resident;
     cudaDeviceGetAttribute(&sv->sms, cudaDevAttrMultiProcessorCount, device);
     e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
@@ -922,7 +932,8 @@ vlbm_status vlbm_server_pump(vlbm_server* sv, uint32_t steps, vlbm_completion* o
         sv->prof[3] += now_s() - t0;
     }
     // cached memory above the budget goes back to the device
-    if (sv->cache.free_bytes + sv->cache.live_bytes > sv->budget + sv->budget / 2) sv->cache.trim(sv->budget / 2);
+    if (sv->cache.free_bytes + sv->cache.live_bytes > sv->budget)
+        sv->cache.trim(sv->budget > sv->cache.live_bytes ? sv->budget - sv->cache.live_bytes : 0);
     int32_t n = 0;
     while (!sv->done.empty() && n < max_out) {
         out[n++] = sv->done.front();
@@ -958,7 +969,9 @@ vlbm_status vlbm_server_fetch(vlbm_server* sv, uint64_t tag, float* ux, size_t n
 vlbm_status vlbm_server_profile(vlbm_server* sv, double* seconds, int32_t n) {
     if (!sv || (n > 0 && !seconds)) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
     sv->prof[9] = sv->capture_s;
-    for (int32_t i = 0; i < n && i < 10; ++i) seconds[i] = sv->prof[i];
+    sv->prof[10] = (double)sv->cache.live_bytes;
+    sv->prof[11] = (double)sv->cache.free_bytes;
+    for (int32_t i = 0; i < n && i < 12; ++i) seconds[i] = sv->prof[i];
     return VLBM_OK;
 }
 

@@ -483,11 +483,13 @@ class Server:
         return {"resident": r.value, "queued": q.value, "bytes": b.value, "lattice_updates": lu.value}
 
     def profile(self):
-        """Host seconds per phase of the serving loop and launch counters."""
-        out = (C.c_double * 10)()
-        _check(_lib.vlbm_server_profile(self._h, out, 10), "vlbm_server_profile")
+        """Host seconds per phase of the serving loop, launch counters and the
+        device bytes of the memory cache (live, cached)."""
+        out = (C.c_double * 12)()
+        _check(_lib.vlbm_server_profile(self._h, out, 12), "vlbm_server_profile")
         return dict(zip(("admit_s", "rebuild_s", "enqueue_s", "wait_s", "readout_s", "batch_steps",
-                         "direct_launches", "graph_launches", "graph_captures", "capture_s"), list(out)))
+                         "direct_launches", "graph_launches", "graph_captures", "capture_s",
+                         "device_live_bytes", "device_cached_bytes"), list(out)))
 
     def set_own_launch_min(self, nodes):
         """Lattices of at least `nodes` nodes get their own launch (-1: default rule)."""
