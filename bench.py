@@ -366,15 +366,19 @@ def serving_requests(vlbm, n, step_scale, seed=2024):
 SERVING_IBM = dict(max_iterations=1, gx=0.0, gy=0.0, gz=-1e-5, wall_x=0, wall_y=1, wall_z=1)
 
 
-def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_resident=64, seed=2024):
+def serving_leg(vlbm, n_req=512, step_scale=0.25, rate=20.0, budget_gb=64.0, max_resident=64, seed=2024,
+                plain_repeats=1):
     """Continuous batching against plain one-at-a-time solves on one arrival stream.
 
-    Both arms see the same Poisson arrivals (rate requests/s) and use the same
-    population layout, so they compute the same numbers (checked: ux fields
-    compared bit for bit).  The plain arm serves the requests first-in
-    first-out with one simulation at a time through the public API (create,
-    node map, spheres, step, read ux, destroy); the batched arm submits each
-    request to a vlbm_server when it arrives and pumps it.
+    Both arms see the same Poisson arrivals (rate requests/s).  The plain arm
+    serves the requests first-in first-out with one simulation at a time
+    through the public API (create, node map, spheres, step, read ux,
+    destroy), each in its own best layout (LAYOUT_AUTO: z-paired FP16 where NZ
+    is even); it runs `plain_repeats` times and the fastest run is compared.
+    The batched arm submits each request to a vlbm_server when it arrives,
+    pumps it and fetches each result when it completes (the server keeps the
+    last 256 results).  The two arms round half-precision stores with
+    different random streams, so their ux fields are compared by relative L2.
     Latency = time the result is handed back - arrival time; solves/s =
     requests / (last completion - first arrival).
     """
@@ -387,28 +391,34 @@ def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_
 
     def natural(cfg):
         c = vlbm.Config.from_buffer_copy(cfg)
-        c.layout = vlbm.LAYOUT_NATURAL   # the server's layout: both arms compute the same numbers
+        c.layout = vlbm.LAYOUT_NATURAL   # the server's layout
         return c
 
-    t0 = time.perf_counter()
-    plain_lat, plain_ux = [], {}
-    for r, a in zip(reqs, arrivals):
-        now = time.perf_counter() - t0
-        if now < a:
-            time.sleep(a - now)
-        sim = vlbm.Simulation(natural(r["cfg"]), builder=vlbm.BUILDER_DUCT_YZ)
-        if r["spheres"]:
-            sim.add_spheres(ibm, r["spheres"])
-        sim.step(r["steps"])
-        sim.sync()
-        plain_ux[r["tag"]] = sim.macroscopics()["ux"].ravel().copy()
-        sim.close()
-        plain_lat.append(time.perf_counter() - t0 - a)
-    plain_span = time.perf_counter() - t0
+    def plain_run():
+        t0 = time.perf_counter()
+        lat, ux = [], {}
+        for r, a in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if now < a:
+                time.sleep(a - now)
+            sim = vlbm.Simulation(r["cfg"], builder=vlbm.BUILDER_DUCT_YZ)
+            if r["spheres"]:
+                sim.add_spheres(ibm, r["spheres"])
+            sim.step(r["steps"])
+            sim.sync()
+            ux[r["tag"]] = sim.macroscopics()["ux"].ravel().copy()
+            sim.close()
+            lat.append(time.perf_counter() - t0 - a)
+        return time.perf_counter() - t0, lat, ux
+
+    plain_runs = [plain_run() for _ in range(max(1, plain_repeats))]
+    plain_span, plain_lat, plain_ux = min(plain_runs, key=lambda t: t[0])
+    plain_spans = [t[0] for t in plain_runs]
 
     srv = vlbm.Server(device=0, hbm_budget_bytes=int(budget_gb * 2 ** 30), max_resident=max_resident)
     t0 = time.perf_counter()
-    nxt, done, arrive_at = 0, [], {}
+    nxt, done, arrive_at, got_ux = 0, [], {}, {}
+    nodes = {r["tag"]: r["nodes"] for r in reqs}
     while len(done) < n_req:
         now = time.perf_counter() - t0
         while nxt < n_req and arrivals[nxt] <= now:
@@ -423,21 +433,14 @@ def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_
         for c in srv.pump(200):
             if c.status != vlbm.OK:
                 raise RuntimeError(f"serving request {c.tag} failed with status {c.status}")
+            got_ux[c.tag] = srv.fetch(c.tag, nodes[c.tag])
             done.append((c, time.perf_counter() - t0))
     batched_span = time.perf_counter() - t0
     host_profile = srv.profile()
-    same, dev, differing = 0, 0.0, []
-    by_tag = {r["tag"]: r for r in reqs}
+    rels = []
     for c, _ in done:
-        ref = plain_ux[c.tag]
-        got = srv.fetch(c.tag, ref.size)
-        same += int(np.array_equal(got, ref))
-        rel = float(np.linalg.norm(got - ref) / max(1e-30, np.linalg.norm(ref)))
-        dev = max(dev, rel)
-        if rel > 0:
-            r = by_tag[c.tag]
-            differing.append({"tag": c.tag, "q": r["cfg"].vel_set, "nodes": r["nodes"], "steps": r["steps"],
-                              "spheres": len(r["spheres"]), "rel_l2": rel})
+        ref, got = plain_ux[c.tag], got_ux[c.tag]
+        rels.append(float(np.linalg.norm(got - ref) / max(1e-30, np.linalg.norm(ref))))
     srv.close()
     batched_lat = [t_ret - arrive_at[c.tag] for c, t_ret in done]
 
@@ -446,10 +449,12 @@ def serving_leg(vlbm, n_req=48, step_scale=0.25, rate=20.0, budget_gb=64.0, max_
                 "p99_s": float(np.percentile(lat, 99)), "mlups": lu / span / 1e6, "makespan_s": span}
 
     batched, plain = arm(batched_span, batched_lat), arm(plain_span, plain_lat)
+    plain["solves_per_s_runs"] = [n_req / t for t in plain_spans]
     return {"requests": n_req, "step_scale": step_scale, "arrival_rate_per_s": rate, "seed": seed,
             "with_spheres": sum(1 for r in reqs if r["spheres"]), "lattice_updates": lu,
             "batched": batched, "plain": plain, "speedup_solves": batched["solves_per_s"] / plain["solves_per_s"],
-            "server_host_seconds": host_profile, "results_bitwise_equal": same, "max_rel_l2_diff_ux": dev, "differing": differing,
+            "server_host_seconds": host_profile, "ux_rel_l2_vs_plain": {"median": float(np.median(rels)),
+                                                                        "max": float(np.max(rels))},
             "sample": f"{n_req} requests of the Bingham-duct serving stream, step counts x{step_scale}"}
 
 
@@ -488,7 +493,9 @@ def main():
     ap.add_argument("--size", type=int, nargs=3, default=[256, 128, 64], metavar=("NX", "NY", "NZ"))
     ap.add_argument("--e2e-steps", type=int, default=3000,
                     help="steps of the end-to-end leg (its host copies are amortised over them)")
-    ap.add_argument("--serving-requests", type=int, default=48)
+    ap.add_argument("--serving-requests", type=int, default=512)
+    ap.add_argument("--serving-plain-repeats", type=int, default=1,
+                    help="runs of the plain one-at-a-time arm; the fastest is compared")
     ap.add_argument("--serving-step-scale", type=float, default=0.25)
     ap.add_argument("--serving-rate", type=float, default=200.0)
     args = ap.parse_args()
@@ -593,7 +600,8 @@ def main():
         ibm_run = ibm_leg(vlbm, torch, local)
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
-        serving = serving_leg(vlbm, args.serving_requests, args.serving_step_scale, args.serving_rate)
+        serving = serving_leg(vlbm, args.serving_requests, args.serving_step_scale, args.serving_rate,
+                              plain_repeats=args.serving_plain_repeats)
 
     if rank == 0:
         dtype = {"f32": "f32", "f16": "f32 arithmetic, f16 storage", "bf16": "f32 arithmetic, bf16 storage"}

@@ -223,11 +223,11 @@ def harness_defines(c):
     return [f"-DHARNESS_FACE={face}", f"-DHARNESS_SCHEME={scheme}"]
 
 
-def sphere_defines(c):
-    if not c.get("spheres"):
-        return []
-    flat = ",".join(f"{d!r},{x!r},{y!r},{z!r}" for d, x, y, z in c["spheres"])
-    return [f"-DREF_SPHERES={flat}"]
+def gen_spheres_h(c):
+    """ref_spheres.h for ref_particles.cpp: the case's spheres as one list
+    (a header, since nvcc splits -D values at commas)."""
+    flat = ", ".join(f"{float(d)!r}, {float(x)!r}, {float(y)!r}, {float(z)!r}" for d, x, y, z in c["spheres"])
+    return f"#pragma once\n#define REF_SPHERES {flat}\n"
 
 
 def build_case(case, ref_root, force=False, jobs=None, log=print, precision="f32"):
@@ -260,6 +260,8 @@ def build_case(case, ref_root, force=False, jobs=None, log=print, precision="f32
         os.path.join("IBM", "ibmVar.h"): gen_ibm_var_h(rd(os.path.join("IBM", "ibmVar.h")), c),
         "mkdir_shim.h": MKDIR_SHIM,
     }
+    if c.get("spheres"):
+        files["ref_spheres.h"] = gen_spheres_h(c)
     for name, text in files.items():
         with open(os.path.join(gen, name), "w") as f:
             f.write(text)
@@ -268,7 +270,7 @@ def build_case(case, ref_root, force=False, jobs=None, log=print, precision="f32
                  os.path.join("IBM", "ibmVar.h")):
         pre += ["-include", os.path.join(gen, name)]
     incs = ["-I", gen, "-I", ref_cuda, "-I", os.path.join(ref_cuda, "IBM")]
-    defs = harness_defines(c) + sphere_defines(c)
+    defs = harness_defines(c)
     srcs = source_list(ref_cuda, c, scratch, precision)
 
     def one(src):

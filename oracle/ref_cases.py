@@ -105,6 +105,48 @@ for _face in ("WEST", "SOUTH", "BACK"):
         nx=12, ny=10, nz=12, tau=0.8, fx=0.0, fy=0.0, fz=0.0, u_max=0.1, rho_bc=[1.0, 1.002, 1, 1, 1, 1, 1, 1],
         steps=300, oracle=(12, 10, 12))
 
+# Spheres settling in a closed box (IBM, IBM_BC walls on every axis), at most
+# three spheres kept apart from each other and from the walls: no contact
+# forms, so the reference's contact slots are never filled, and the collision
+# kernel launches exactly N(N+1)/2 threads (ibmVar.h:167-175), all inside the
+# particle array.  With spheres the final save is made after the last IBM
+# step: the program's files labelled N_STEPS hold the state after N_STEPS steps
+# (main.cu:293-296, 369-393, 524-535; IBM/ibm.cu:545-648).
+IBM_CLOSED = dict(iterations=3, density=2.0, gx=0.0, gy=0.0, gz=-5e-5, walls=(1, 1, 1))
+CASES["ibm_settling_closed_box_q19"] = dict(
+    q=19, op="reg", rheo=None, builder="closedBoxBounceBack", lib_builder=3, nx=32, ny=32, nz=48,
+    tau=0.8, fx=0.0, fy=0.0, fz=0.0, u_max=0.1, steps=301, oracle=(32, 32, 48),
+    spheres=[(10.0, 15.5, 16.0, 31.0), (10.0, 16.3, 15.4, 15.0)], ibm=IBM_CLOSED)
+CASES["ibm_bingham_closed_box_q19"] = dict(
+    q=19, op="reg", rheo="bingham", builder="closedBoxBounceBack", lib_builder=3, nx=32, ny=32, nz=48,
+    tau=0.8, eta_p=0.1, s_y=1e-6, fx=0.0, fy=0.0, fz=0.0, u_max=0.1, steps=301, oracle=(32, 32, 48),
+    spheres=[(8.0, 10.0, 10.0, 24.0), (8.0, 21.5, 12.0, 30.0), (8.0, 16.0, 22.0, 18.0)], ibm=IBM_CLOSED)
+
+
+def fluid_cases():
+    return [k for k, c in CASES.items() if not c.get("spheres")]
+
+
+def sphere_cases():
+    return [k for k, c in CASES.items() if c.get("spheres")]
+
+
+def ibm_config_kwargs(case):
+    """vlbm.IbmConfig.default keyword arguments (ibmVar.h / ibmBoundaryCondition.h
+    values the reference build of the case is configured with)."""
+    ib = CASES[case]["ibm"]
+    wx, wy, wz = ib["walls"]
+    return dict(max_iterations=ib["iterations"], gx=ib["gx"], gy=ib["gy"], gz=ib["gz"],
+                wall_x=wx, wall_y=wy, wall_z=wz)
+
+
+def sphere_kwargs(case):
+    """vlbm.Sphere keyword arguments: makeSpherePolar's diameter and centre, at
+    rest, movable, PARTICLE_DENSITY (oracle/ref_particles.cpp)."""
+    c = CASES[case]
+    return [dict(diameter=d, cx=x, cy=y, cz=z, density=c["ibm"]["density"], movable=1)
+            for d, x, y, z in c["spheres"]]
+
 
 def lib_config_kwargs(case):
     """vlbm.Config.default keyword arguments for a case."""

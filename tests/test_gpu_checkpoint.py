@@ -29,6 +29,10 @@ CASES = [
                                        k_consistency=0.02, ux_bc=[0, 0.05], storage=1), 6, None, 9),
     ("bf16_duct_q19", dict(nx=20, ny=10, nz=10, vel_set=19, tau=0.9, fx=1e-4, storage=2), 5, None, 5),
     ("ibm_contacts_q27", dict(nx=24, ny=20, nz=24, vel_set=27, tau=0.7), 3, SPHERES, 11),
+    # NX a multiple of 32: z-paired populations in blocks of 32 pair-nodes
+    ("f16_blocked_pairs_channel", dict(nx=32, ny=12, nz=8, vel_set=19, rheology=1, eta_p=0.1,
+                                       yield_stress=1e-6, fx=2e-4, storage=1), 1, None, 7),
+    ("ibm_blocked_pairs_q27", dict(nx=32, ny=20, nz=24, vel_set=27, tau=0.7), 3, SPHERES, 9),
 ]
 
 

@@ -43,6 +43,12 @@ CASES = [
     ("free_slip_q19", 19, 0, 0, 7, (10, 12, 6), 70, dict(tau=0.8, fx=2e-4)),
     ("free_slip_q27", 27, 1, 0, 7, (10, 12, 6), 51, dict(tau=0.8, fx=2e-4)),
     ("zouhe_couette_q19", 19, 0, 0, 8, (8, 12, 8), 60, dict(tau=0.8, uz_bc=[0, 0.02, -0.02])),
+    # NX a multiple of 32 with D3Q27 FP32 and even NZ: the z-paired layout in
+    # blocks of 32 pair-nodes (x neighbours across block edges, walls, the z seam)
+    ("closed_box_reg_q27_blocked", 27, 0, 0, 3, (32, 9, 8), 61, dict(tau=0.8, fx=1e-4, fy=-2e-4, fz=3e-4)),
+    ("plates_bingham_q27_blocked", 27, 0, 1, 1, (64, 10, 6), 60, dict(fx=5e-4, eta_p=0.1, yield_stress=2e-6)),
+    ("lid_cavity_powerlaw_q27_blocked", 27, 0, 2, 6, (32, 12, 10), 50,
+     dict(n_index=1.5, k_consistency=0.05, ux_bc=[0, 0.05])),
 ]
 
 
@@ -180,9 +186,11 @@ def test_poiseuille_gpu_against_analytic(vlbm):
     assert np.linalg.norm(ux - ana) / np.linalg.norm(ana) < 2e-2  # 10k steps: not fully developed
 
 
+# nx 16: plain z-paired layout; nx 32: pairs in blocks of 32
+@pytest.mark.parametrize("nx", [16, 32])
 @pytest.mark.parametrize("storage,tol", [(1, 2e-3), (2, 2e-2)])
-def test_half_precision_storage_close_to_fp64(vlbm, oracle, storage, tol):
-    cfg, sim, o = run_pair(vlbm, oracle, 19, 0, 1, 1, (16, 24, 4), 400,
+def test_half_precision_storage_close_to_fp64(vlbm, oracle, storage, tol, nx):
+    cfg, sim, o = run_pair(vlbm, oracle, 19, 0, 1, 1, (nx, 24, 4), 400,
                            dict(fx=5e-5, eta_p=0.1, yield_stress=1e-6), storage=storage)
     ug = sim.macroscopics()["ux"].astype(np.float64)
     uo = o.macroscopics()["ux"]

@@ -80,7 +80,7 @@ def run_reference(case, workdir, precision="f32"):
     if mlups:
         print(f"REFRUN {case} {precision} {mlups[-1]}")
     c = ref_cases.CASES[case]
-    out = {}
+    out = {"dir": os.path.join(wd, "out", case)}
     names = ["rho", "ux", "uy", "uz"] + (["omega"] if c["rheo"] else [])
     for v in names:
         p = os.path.join(wd, "out", case, f"{case}_{v}{_label(c['steps'])}.bin")
@@ -133,7 +133,7 @@ def rho_max(a, b):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", list(ref_cases.CASES))
+@pytest.mark.parametrize("case", ref_cases.fluid_cases())
 def test_matches_reference_build(vlbm, oracle, case, tmp_path):
     ref32 = run_reference(case, str(tmp_path), "f32")
     ref64 = run_reference(case, str(tmp_path), "f64")
@@ -161,3 +161,134 @@ def test_matches_reference_build(vlbm, oracle, case, tmp_path):
     if "omega_mean" in res:
         assert res["omega_mean"] <= OMEGA_MEAN, res
         assert res["omega_p99"] <= OMEGA_P99, res
+
+
+# ------------------------------------------------------------------ spheres ---
+# Sphere cases: the reference program writes its particle state with
+# saveParticlesInfo (IBM/ibmReport.cpp:26-102) after the final step, in
+# std::scientific with 7 significant digits; the library writes the same files
+# through vlbm_write_particles_csv.  Bounds (lattice units):
+#   reference FP64 vs FP64 oracle: fluid velocity relative L2 <= 1e-8; particle
+#     position within the CSV resolution (|dx| <= 2e-5), velocity and rotation
+#     within 1e-5 of their largest magnitude, Lagrangian nodes |dx| <= 2e-5;
+#   library (FP32 fluid, FP64 particles) vs reference FP64: the bounds of the
+#     oracle comparison in tests/test_gpu_ibm.py: fluid relative L2 <= 5e-3,
+#     position |dx| <= 2e-5 + 1e-3 |x - x0|, velocity and rotation
+#     <= 2e-3 of their largest magnitude;
+#   library vs reference FP32: within 1.5x the reference's own FP32 error plus
+#     the library-vs-FP64 bound.
+IBM_REF64_VS_ORACLE_U = 1e-8
+IBM_CSV_POS = 2e-5
+IBM_REF64_VS_ORACLE_V = 1e-5
+IBM_LIB_U = 5e-3
+IBM_LIB_V = 2e-3
+
+
+def _pfile(d, case, var, step):
+    return os.path.join(d, f"{case}_{var}{_label(step)}.csv")
+
+
+def read_pcenters(path):
+    """pCenters CSV -> header line and {pos, vel, w, f, M} arrays [n][3]."""
+    with open(path) as f:
+        header = f.readline().strip()
+    a = np.atleast_1d(np.genfromtxt(path, delimiter=",", names=True))
+    out = {"header": header}
+    for key in ("pos", "vel", "w", "f", "M"):
+        out[key] = np.stack([a[f"{key}_{ax}"] for ax in "xyz"], axis=1)
+    out["radius"] = a["radius"]
+    return out
+
+
+def read_pnodes(path):
+    with open(path) as f:
+        header = f.readline().strip()
+    a = np.atleast_1d(np.genfromtxt(path, delimiter=",", names=True))
+    return header, np.stack([a["pos_x"], a["pos_y"], a["pos_z"]]), a["particle_index"]
+
+
+def run_library_spheres(vlbm, case, outdir):
+    c = ref_cases.CASES[case]
+    cfg = vlbm.Config.default(device=0, **ref_cases.lib_config_kwargs(case))
+    m = ref_cases.node_map(case, vlbm.build_node_map)
+    sim = vlbm.Simulation(cfg, node_map=m)
+    sim.add_spheres(vlbm.IbmConfig.default(**ref_cases.ibm_config_kwargs(case)),
+                    [vlbm.Sphere(**s) for s in ref_cases.sphere_kwargs(case)])
+    sim.step(c["steps"])
+    sim.sync()
+    out = sim.macroscopics()
+    sim.write_particles_csv(outdir, case, c["steps"], save_nodes=True)
+    out["dir"] = os.path.join(outdir, case)
+    sim.close()
+    return out
+
+
+def run_oracle_spheres(vlbm, oracle, case):
+    c = ref_cases.CASES[case]
+    cfg = oracle.Config.default(**ref_cases.lib_config_kwargs(case))
+    m = ref_cases.node_map(case, lambda b, *s: oracle.reference_builder_map(oracle.BUILDER_NAMES[b], *s))
+    sp = [vlbm.Sphere(**s) for s in ref_cases.sphere_kwargs(case)]
+    o = oracle.OracleIbm(cfg, m, vlbm.IbmConfig.default(**ref_cases.ibm_config_kwargs(case)), sp)
+    o.step(c["steps"])
+    out = o.macroscopics()
+    out["particles"] = o.particles()
+    out["nodes"] = o.nodes()
+    o.close()
+    return out
+
+
+def _pdiff(a, b, key):
+    return float(np.abs(np.asarray(a[key], dtype=np.float64) - b[key]).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ref_cases.sphere_cases())
+def test_sphere_case_matches_reference_build(vlbm, oracle, case, tmp_path):
+    c = ref_cases.CASES[case]
+    steps = c["steps"]
+    ref32 = run_reference(case, str(tmp_path), "f32")
+    ref64 = run_reference(case, str(tmp_path), "f64")
+    lib = run_library_spheres(vlbm, case, str(tmp_path / "lib"))
+    oracle.set_threads(os.cpu_count() or 1)
+    fp64 = run_oracle_spheres(vlbm, oracle, case)
+    p32 = read_pcenters(_pfile(ref32["dir"], case, "pCenters", steps))
+    p64 = read_pcenters(_pfile(ref64["dir"], case, "pCenters", steps))
+    plib = read_pcenters(_pfile(lib["dir"], case, "pCenters", steps))
+    po = fp64["particles"]
+    x0 = np.array([[x, y, z] for _, x, y, z in c["spheres"]])
+    h64, n64, idx64 = read_pnodes(_pfile(ref64["dir"], case, "pNodes", steps))
+    hlib, nlib, idxlib = read_pnodes(_pfile(lib["dir"], case, "pNodes", steps))
+    vmax = float(np.abs(p64["vel"]).max())
+    wmax = max(float(np.abs(p64["w"]).max()), 1e-12)
+    res = dict(
+        ref64_fp64=u_rel(ref64, fp64), lib_ref64=u_rel(lib, ref64), ref32_ref64=u_rel(ref32, ref64),
+        lib_ref32=u_rel(lib, ref32), rho_lib_ref64=rho_max(lib, ref64),
+        pos_ref64_fp64=_pdiff(p64, po, "pos"), vel_ref64_fp64=_pdiff(p64, po, "vel") / vmax,
+        w_ref64_fp64=_pdiff(p64, po, "w") / wmax,
+        nodes_ref64_fp64=float(np.abs(n64 - fp64["nodes"]).max()),
+        nodes_lib_ref64=float(np.abs(nlib - n64).max()),
+        pos_lib_ref64=_pdiff(plib, p64, "pos"), vel_lib_ref64=_pdiff(plib, p64, "vel") / vmax,
+        w_lib_ref64=_pdiff(plib, p64, "w") / wmax,
+        vel_ref32_ref64=_pdiff(p32, p64, "vel") / vmax, vel_lib_ref32=_pdiff(plib, p32, "vel") / vmax,
+        disp=float(np.abs(p64["pos"] - x0).max()), v_max=vmax)
+    print(f"REFPARITY {case} " + " ".join(f"{k}={v:.3e}" for k, v in res.items()))
+    # the library's files are the reference's files: same columns, same rows
+    assert plib["header"] == p64["header"]
+    assert hlib == h64 and np.array_equal(idxlib, idx64)
+    assert np.array_equal(plib["radius"], p64["radius"])
+    for name, f in (("ref32", ref32), ("ref64", ref64), ("lib", lib)):
+        for k in ("rho", "ux", "uy", "uz"):
+            assert np.all(np.isfinite(f[k])), f"{name} {k} not finite"
+    assert res["v_max"] > 1e-5 and res["disp"] > 1e-2, res   # the spheres did move
+    assert res["ref64_fp64"] <= IBM_REF64_VS_ORACLE_U, res
+    assert res["pos_ref64_fp64"] <= IBM_CSV_POS, res
+    assert res["vel_ref64_fp64"] <= IBM_REF64_VS_ORACLE_V and res["w_ref64_fp64"] <= IBM_REF64_VS_ORACLE_V, res
+    assert res["nodes_ref64_fp64"] <= IBM_CSV_POS, res
+    assert res["lib_ref64"] <= IBM_LIB_U, res
+    assert res["rho_lib_ref64"] <= RHO_LIB_REF64, res
+    dx = np.abs(plib["pos"] - p64["pos"])
+    assert np.all(dx <= IBM_CSV_POS + 1e-3 * np.abs(p64["pos"] - x0)), (res, dx)
+    assert res["nodes_lib_ref64"] <= IBM_CSV_POS + 1e-3 * res["disp"] * 2, res
+    assert res["vel_lib_ref64"] <= IBM_LIB_V and res["w_lib_ref64"] <= IBM_LIB_V, res
+    assert res["lib_ref32"] <= LIB_VS_REF32_FACTOR * res["ref32_ref64"] + IBM_LIB_U, res
+    assert res["vel_lib_ref32"] <= LIB_VS_REF32_FACTOR * res["vel_ref32_ref64"] + IBM_LIB_V, res

@@ -46,3 +46,45 @@ def test_noalloc_rejects_lattices_beyond_its_scratch(vlbm):
     assert st == vlbm.ERR_INVALID
     assert b"67108864" in lib.vlbm_last_error()
     sim.close()
+
+
+def test_noalloc_first_on_a_fresh_simulation_allocates_nothing(vlbm):
+    """Called first on a fresh simulation (no earlier vlbm_moments_sum), the
+    allocation-free path leaves the simulation's device bytes and the device's
+    free memory (cudaMemGetInfo) unchanged, and then agrees with the allocating
+    entry point."""
+    import torch
+    lib = vlbm.lib()
+    # CUDA loads a module's code and device globals (the scratch array among
+    # them) at its first use in the process; a call on another simulation does
+    # that first, so the measurement below sees only what the call itself does
+    warm = vlbm.Simulation(vlbm.Config.default(nx=8, ny=8, nz=8))
+    _sums(vlbm, lib.vlbm_moments_sum_noalloc, warm)
+    warm.close()
+    cfg = vlbm.Config.default(nx=48, ny=20, nz=16, vel_set=19, tau=0.7, fx=2e-5)
+    sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+    sim.step(9)
+    sim.sync()
+    torch.cuda.synchronize()
+    before_sim = sim.info().device_bytes
+    before_free = torch.cuda.mem_get_info(0)[0]
+    got = [_sums(vlbm, lib.vlbm_moments_sum_noalloc, sim) for _ in range(2)]
+    torch.cuda.synchronize()
+    assert sim.info().device_bytes == before_sim
+    assert torch.cuda.mem_get_info(0)[0] == before_free
+    np.testing.assert_array_equal(got[0], got[1])
+    np.testing.assert_array_equal(got[0], _sums(vlbm, lib.vlbm_moments_sum, sim))
+    sim.close()
+
+
+def test_noalloc_accepts_the_largest_lattice_its_scratch_covers(vlbm):
+    """67,108,864 nodes (16384 partial sums, the whole scratch array) is
+    accepted and agrees with the allocating entry point."""
+    lib = vlbm.lib()
+    cfg = vlbm.Config.default(nx=4096, ny=128, nz=128, storage=vlbm.STORE_F16, fx=1e-5)
+    sim = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
+    sim.step(2)
+    got = _sums(vlbm, lib.vlbm_moments_sum_noalloc, sim)
+    np.testing.assert_array_equal(got, _sums(vlbm, lib.vlbm_moments_sum, sim))
+    assert abs(got[0] - 4096 * 128 * 128) < 1e-6 * 4096 * 128 * 128
+    sim.close()

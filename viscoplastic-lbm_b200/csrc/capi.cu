@@ -95,6 +95,10 @@ StepParams make_params(vlbm_sim* s) {
     p.N = s->N;
     p.nbc = s->nbc;
     p.pairH = s->pairH;
+    p.pairBlk = s->pairBlk;
+    p.tile_special = s->tile_special;
+    p.special_tiles = s->special_tiles;
+    p.n_special = s->n_special;
     p.apply_bc = s->apply_bc;
     p.ctr = s->step_ctr;
     p.omega_newt = (float)(1.0 / c.tau);                 // var.h:105 OMEGA
@@ -183,6 +187,46 @@ static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
     return VLBM_OK;
 }
 
+// Pair-step tiles: 32 consecutive pair-nodes m (one warp; nodes m and m + M,
+// M = N/2).  A tile is special when one of its 64 nodes is a boundary or
+// unused node; the list of special tiles is filled in any order (every node
+// pair reads and writes only its own slots, so the order of the tiles does
+// not change the result).
+__global__ void k_tile_flags(const uint8_t* cls, long long M, uint8_t* flag, int32_t* list, int* count) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (M + 31) / 32) return;
+    bool sp = false;
+    for (int k = 0; k < 32 && !sp; ++k) {
+        const long long m = t * 32 + k;
+        if (m < M) sp = ((cls[m] | cls[m + M]) & (NODE_BC | NODE_UNUSED)) != 0;
+    }
+    flag[t] = sp ? 1 : 0;
+    if (sp) list[atomicAdd(count, 1)] = (int32_t)t;
+}
+
+static vlbm_status build_pair_tiles(vlbm_sim* s) {
+    if (s->pairH <= 0) return VLBM_OK;
+    const long long M = s->N / 2, T = (M + 31) / 32;
+    vlbm_status st;
+    void* p;
+    if (!s->tile_special) {
+        if ((st = alloc_dev(s, &p, (size_t)T)) != VLBM_OK) return st;
+        s->tile_special = static_cast<uint8_t*>(p);
+        if ((st = alloc_dev(s, &p, (size_t)T * sizeof(int32_t) + sizeof(int32_t))) != VLBM_OK) return st;
+        s->special_tiles = static_cast<int32_t*>(p);
+    }
+    int* count = s->special_tiles + T;   // the counter sits behind the list
+    VLBM_CUDA(cudaMemsetAsync(count, 0, sizeof(int), s->stream));
+    k_tile_flags<<<(unsigned)((T + 255) / 256), 256, 0, s->stream>>>(s->cls, M, s->tile_special, s->special_tiles,
+                                                                    count);
+    VLBM_CUDA(cudaGetLastError());
+    int n = 0;
+    VLBM_CUDA(cudaMemcpyAsync(&n, count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    s->n_special = n;
+    return VLBM_OK;
+}
+
 // Install boundary tables: class bytes and slots (bulk everywhere, then the
 // boundary nodes scattered on the device), the records and the side store.
 static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
@@ -236,6 +280,8 @@ static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
     } else {
         VLBM_CUDA(cudaStreamSynchronize(s->stream));
     }
+    vlbm_status st = build_pair_tiles(s);
+    if (st != VLBM_OK) return st;
     s->geometry = true;
     return VLBM_OK;
 }
@@ -269,7 +315,7 @@ vlbm_sim::~vlbm_sim() {
     if (ibm) { ibm_destroy(ibm, allocator); ibm = nullptr; }
     for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)bc_node, (void*)side[0], (void*)side[1],
                     (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch, (void*)bc_q,
-                    (void*)treat_prev, (void*)treat_red})
+                    (void*)treat_prev, (void*)treat_red, (void*)tile_special, (void*)special_tiles})
         free_with(allocator, p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -349,6 +395,11 @@ vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator,
                                                                                       : VLBM_LAYOUT_NATURAL;
         if (lay == VLBM_LAYOUT_ZPAIR && !even_z) { delete s; set_last_error("the z-paired layout needs an even nz"); return VLBM_ERR_INVALID; }
         s->pairH = lay == VLBM_LAYOUT_ZPAIR ? cfg->nz / 2 : 0;
+        // pairs in blocks of 32 (one warp's pair-nodes, all Q populations
+        // together) where NX is a multiple of 32 and the blocked offsets fit
+        // 32 bits: the pair step then addresses every population from one
+        // pointer (D3Q19 FP16 256^3: 57.6k against 53.3k MLUPS)
+        s->pairBlk = (s->pairH > 0 && cfg->nx % 32 == 0 && (s->N / 2) * s->Q < (1ll << 31)) ? 1 : 0;
     }
     e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete s; return cuda_status(e, "cudaStreamCreate"); }
@@ -357,7 +408,7 @@ vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator,
     void* p;
     if ((st = alloc_dev(s, &p, (size_t)s->Q * N * s->store_bytes)) != VLBM_OK) { delete s; return st; }
     s->pop = p;
-    // class bytes padded to whole 32-bit words (the IBM marks nodes with atomicOr on words)
+    // class bytes, padded to whole 32-bit words
     const size_t cls_bytes = (N + 3) & ~(size_t)3;
     if ((st = alloc_dev(s, &p, cls_bytes)) != VLBM_OK) { delete s; return st; }
     s->cls = static_cast<uint8_t*>(p);

@@ -47,7 +47,7 @@ struct CkptHeader {
     uint32_t version;
     uint32_t header_bytes;
     int32_t nx, ny, nz, q;
-    int32_t storage, store_bytes, pair_h, nbc;
+    int32_t storage, store_bytes, pair_h, nbc;   // pair_h: NZ/2 of a z-paired layout, bit 30 = blocked pairs
     float scale;
     int32_t rheology;
     int32_t parity, side_cur, apply_bc, has_omega;
@@ -115,7 +115,7 @@ vlbm_status geometry_hash(vlbm_sim* s, uint64_t* out) {
     std::vector<uint8_t> cls(N);
     cudaError_t e = ckpt_copy(s, cls.data(), s->cls, N, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_status(e, "checkpoint: read node classes");
-    for (auto& c : cls) c &= (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
+    for (auto& c : cls) c &= (uint8_t)~NODE_IBM_FORCE;
     Hash64 h;
     h.add(cls.data(), N);
     if (s->nbc > 0) {
@@ -138,7 +138,7 @@ vlbm_status fill_header(vlbm_sim* s, const std::vector<StateRegion>& regions, Ck
     h->version = kVersion;
     h->header_bytes = sizeof(CkptHeader);
     h->nx = s->cfg.nx; h->ny = s->cfg.ny; h->nz = s->cfg.nz; h->q = s->Q;
-    h->storage = s->cfg.storage; h->store_bytes = s->store_bytes; h->pair_h = s->pairH; h->nbc = s->nbc;
+    h->storage = s->cfg.storage; h->store_bytes = s->store_bytes; h->pair_h = s->pairH | (s->pairBlk << 30); h->nbc = s->nbc;
     h->scale = effective_scale(s);
     h->rheology = s->cfg.rheology;
     h->parity = s->parity; h->side_cur = s->side_cur; h->apply_bc = s->apply_bc;

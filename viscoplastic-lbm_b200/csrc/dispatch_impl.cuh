@@ -9,10 +9,20 @@ inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block 
 
 template <int Q, int OP, int RHEO, int ST>
 cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s) {
-    if (p.pairH > 0) {  // z-paired layout: one thread per node pair
+    if (p.pairH > 0) {  // z-paired layout: one thread per node pair; bulk tiles, then the listed ones
         const unsigned g = grid_for(p.N / 2, ls.block);
-        if (odd) k_step2<Q, OP, RHEO, ST, true><<<g, ls.block, 0, s>>>(p);
-        else k_step2<Q, OP, RHEO, ST, false><<<g, ls.block, 0, s>>>(p);
+        const unsigned gs = grid_for((long long)p.n_special * 32, 256);
+        if (p.pairBlk) {
+            if (odd) k_step2_bulk<Q, OP, RHEO, ST, true, true><<<g, ls.block, 0, s>>>(p);
+            else k_step2_bulk<Q, OP, RHEO, ST, false, true><<<g, ls.block, 0, s>>>(p);
+            if (gs && odd) k_step2<Q, OP, RHEO, ST, true, true><<<gs, 256, 0, s>>>(p);
+            else if (gs) k_step2<Q, OP, RHEO, ST, false, true><<<gs, 256, 0, s>>>(p);
+        } else {
+            if (odd) k_step2_bulk<Q, OP, RHEO, ST, true, false><<<g, ls.block, 0, s>>>(p);
+            else k_step2_bulk<Q, OP, RHEO, ST, false, false><<<g, ls.block, 0, s>>>(p);
+            if (gs && odd) k_step2<Q, OP, RHEO, ST, true, false><<<gs, 256, 0, s>>>(p);
+            else if (gs) k_step2<Q, OP, RHEO, ST, false, false><<<gs, 256, 0, s>>>(p);
+        }
         return cudaGetLastError();
     }
     const unsigned g = grid_for(p.N, ls.block);

@@ -9,14 +9,14 @@
 //
 //   k_ibm_begin      CTAs 0..np-1: unwrapped node extent -> Eulerian box of
 //                    each sphere, node forces reset (gpuResetNodesForces
-//                    ibm.cu:651-668); CTA np: touched-node count reset, old
-//                    values, Hertz-Mindlin contacts with deterministic slot
-//                    updates and sums, predictor
+//                    ibm.cu:651-668); CTA np: old values, Hertz-Mindlin
+//                    contacts with deterministic slot updates and sums,
+//                    predictor
 //   k_ibm_gather     several CTAs per sphere: rho,u of the post-boundary
 //                    populations with the constant body force
 //                    (gpuUpdateMacrIBM ibm.cu:544-648) for the box nodes,
-//                    written to dense fields; each node is appended once to a
-//                    compact list (atomicOr on its class bit)
+//                    written to dense fields; each node's owner becomes the
+//                    lowest index of the spheres whose box holds it
 //   per multi-direct-forcing iteration:
 //     k_ibm_interp_spread  several CTAs per sphere, one warp per Lagrangian
 //                    node with its 64 stencil points split over the lanes:
@@ -26,9 +26,9 @@
 //     k_ibm_update   partials added in a fixed order, particle velocity and
 //                    rotation update; in the last iteration also the particle
 //                    movement and the step clock
-//     k_ibm_euler    over the node list: u += fAux/(2 rho), F += fAux,
-//                    fAux = 0; in the last iteration also the Lagrangian node
-//                    movement
+//     k_ibm_euler    over the boxes, each node by its owner sphere's CTAs:
+//                    u += fAux/(2 rho), F += fAux, fAux = 0; in the last
+//                    iteration also the Lagrangian node movement
 //
 // Particle state, contacts and integration are FP64; the Eulerian fields FP32.
 #include <cuda_runtime.h>
@@ -48,6 +48,7 @@ constexpr int IBM_THREADS = 256;
 constexpr int IBM_NODES_PER_CTA = 32;       // Lagrangian nodes per CTA of k_ibm_interp_spread (4 per warp)
 constexpr int IBM_MAX_SPLIT = 32;           // CTAs per sphere, at most
 constexpr int IBM_MAX_PARTICLES = 1024;   // pair buffer np*np*6 doubles <= 50 MB
+constexpr unsigned IBM_NO_OWNER = 0xFFFFFFFFu;   // owner[] of a node in no sphere's box
 
 struct DPart {
     double pos[3], pos_old[3], vel[3], vel_old[3], w[3], w_avg[3], w_old[3], w_pos[3];
@@ -79,13 +80,13 @@ struct IbmState {
     int* npid = nullptr;
     float* fields = nullptr;      // [4][N] rho,ux,uy,uz (IBM macroscopics)
     unsigned long long* faux = nullptr;   // [3][N] spread force, fixed point (IBM_FIX_SCALE)
-    int* list = nullptr;          // [N] touched Eulerian nodes
-    int* count = nullptr;         // [0]: touched-node count, [1]: IBM steps taken (contact history clock)
+    unsigned* owner = nullptr;    // [N] lowest sphere index whose box holds the node, during a step;
+                                  // IBM_NO_OWNER everywhere between steps
+    int* clock = nullptr;         // IBM steps taken (contact history clock)
     double* contrib = nullptr;    // [np][np][6] pair force/torque on the row particle
     double* fpart = nullptr;      // [np][split][6] per-CTA force/torque partials
     int split = 1;                // CTAs per sphere in k_ibm_interp_spread
-    int gsplit = 1;               // CTAs per sphere in k_ibm_gather
-    long long euler_blocks = 1;   // grid of k_ibm_euler (grid-stride over the node list)
+    int gsplit = 1;               // CTAs per sphere in k_ibm_gather, k_ibm_euler and k_ibm_fixup
     std::vector<DPart> initial;   // for vlbm_init_equilibrium
     std::vector<double> init_nodes;
     size_t bytes = 0;
@@ -190,11 +191,25 @@ __device__ void ibm_box(const IbmParams& P, DPart* parts, int sphere, const doub
 }
 
 // -------------------------------------------------------------- gather --
+// Box node k (x fastest) of a sphere's box, wrapped onto the lattice.
+__device__ __forceinline__ unsigned box_node(const IbmParams& P, const DPart& p, long long k) {
+    const int bx = p.box_n[0], by = p.box_n[1];
+    const int ix = (int)(k % bx), iy = (int)((k / bx) % by), iz = (int)(k / ((long long)bx * by));
+    const int x = wrapi(p.box_lo[0] + ix, P.nx), y = wrapi(p.box_lo[1] + iy, P.ny), z = wrapi(p.box_lo[2] + iz, P.nz);
+    return (unsigned)(((size_t)z * P.ny + y) * P.nx + x);
+}
+
+// IBM macroscopics of every node of the spheres' boxes (gpuUpdateMacrIBM,
+// ibm.cu:545-648, restricted to the boxes).  owner[n] becomes the lowest index
+// of the spheres whose box holds node n: the Eulerian pass of each forcing
+// iteration updates a node once, from that sphere's CTAs, and the last pass
+// sets it back to IBM_NO_OWNER.
 template <int Q, int ST, bool ODD, bool PAIRED>
 __global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmParams P, const DPart* parts,
-                                                             float* fields, int* list, int* count, int split) {
+                                                             float* fields, unsigned* owner, int split) {
     // `split` CTAs per sphere share its box
-    const DPart& p = parts[blockIdx.x / split];
+    const unsigned sphere = blockIdx.x / split;
+    const DPart& p = parts[sphere];
     const int sub = blockIdx.x % split;
     const int bx = p.box_n[0], by = p.box_n[1], bz = p.box_n[2];
     const long long tot = (long long)bx * by * bz;
@@ -213,9 +228,7 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmPa
         fields[N + n] = m.ux;
         fields[2 * N + n] = m.uy;
         fields[3 * N + n] = m.uz;
-        unsigned* word = reinterpret_cast<unsigned*>(sp.cls + (n & ~3u));
-        const unsigned bit = (unsigned)NODE_IBM_SET << (8u * (n & 3u));
-        if (!(atomicOr(word, bit) & bit)) list[atomicAdd(count, 1)] = (int)n;
+        atomicMin(&owner[n], sphere);
     }
 }
 
@@ -508,20 +521,19 @@ __device__ void ibm_contacts(const IbmParams& P, DPart* parts, double* contrib) 
 
 // One launch for the start of the IBM step: blocks 0..np-1 find the Eulerian
 // box of their sphere and reset its node forces (k_ibm_box part), block np
-// resets the touched-node count and runs the old-value copy, the contacts and
-// the predictor (they read positions only, which the boxes do not change).
+// runs the old-value copy, the contacts and the predictor (they read
+// positions only, which the boxes do not change).
 __global__ void __launch_bounds__(IBM_THREADS) k_ibm_begin(IbmParams P, DPart* parts, const double* X, const double* Y,
                                                             const double* Z, double* fx, double* fy, double* fz,
                                                             double* dx, double* dy, double* dz, double* contrib,
-                                                            int* count) {
+                                                            const int* clock) {
     if ((int)blockIdx.x < P.np) {
         ibm_box(P, parts, blockIdx.x, X, Y, Z, fx, fy, fz, dx, dy, dz);
         return;
     }
     // index of the fluid step just taken (main.cu:270), kept on the device so
     // a captured IBM step can be replayed
-    P.step = count[1];
-    if (threadIdx.x == 0) count[0] = 0;
+    P.step = *clock;
     ibm_contacts(P, parts, contrib);
 }
 
@@ -709,7 +721,7 @@ __device__ void move_particle(const IbmParams& P, DPart& p) {
 // Sphere force/torque partials added in a fixed order, velocity and rotation
 // update; after the last forcing iteration also the particle movement
 // (gpuParticleMovement ibm.cu:899-993) and the step clock.
-__global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int split, int last, int* count) {
+__global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int split, int last, int* clock) {
     for (int i = threadIdx.x; i < P.np; i += blockDim.x) {
         DPart& p = parts[i];
         double t[6] = {0, 0, 0, 0, 0, 0};
@@ -719,7 +731,7 @@ __global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int
         update_center(P, p);
         if (last) move_particle(P, p);
     }
-    if (last && threadIdx.x == 0) count[1] += 1;   // read by the next step's contacts
+    if (last && threadIdx.x == 0) *clock += 1;   // read by the next step's contacts
 }
 
 // gpuParticleNodeMovement ibm.cu:1044-1197
@@ -756,25 +768,35 @@ __device__ void move_node(const IbmParams& P, const DPart* parts, const int* pid
     for (int a = 0; a < 3; ++a) *Pp[a] = P.wall[a] ? np3[a] : fmod(np3[a] + L[a], L[a]);
 }
 
-// Over the touched-node list: u += fAux/(2 rho), F += fAux, fAux = 0
-// (gpuEulerSumIBMAuxsReset restricted to the touched nodes); after the last
-// forcing iteration the same launch moves the Lagrangian nodes
+// Over the spheres' boxes, each node once (by the sphere owner[] names):
+// u += fAux/(2 rho), F += fAux, fAux = 0 (gpuEulerSumIBMAuxsReset, restricted
+// to the boxes); nodes that received no spread force are left as they are.
+// After the last forcing iteration the same launch moves the Lagrangian nodes
 // (gpuParticleNodeMovement ibm.cu:1044-1197), which k_ibm_update's particle
-// movement precedes.
-__global__ void k_ibm_euler(IbmParams P, float* fields, unsigned long long* faux, float* fibm, uint8_t* cls,
-                            const int* list, const int* count, const DPart* parts, const int* pid, double* X,
-                            double* Y, double* Z, int move_nodes) {
-    const int cnt = *count;
+// movement precedes, and releases the owners.  `split` CTAs per sphere.
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_euler(IbmParams P, float* fields, unsigned long long* faux,
+                                                            float* fibm, uint8_t* cls, unsigned* owner,
+                                                            const DPart* parts, const int* pid, double* X, double* Y,
+                                                            double* Z, int split, int last) {
     const size_t N = (size_t)P.nx * P.ny * P.nz;
-    if (move_nodes)
+    if (last)
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P.nnodes; k += gridDim.x * blockDim.x)
             move_node(P, parts, pid, X, Y, Z, k);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
-        const int n = list[k];
+    const unsigned sphere = blockIdx.x / split;
+    const DPart& p = parts[sphere];
+    const int sub = blockIdx.x % split;
+    const long long tot = (long long)p.box_n[0] * p.box_n[1] * p.box_n[2];
+    for (long long k = (long long)sub * blockDim.x + threadIdx.x; k < tot; k += (long long)split * blockDim.x) {
+        const unsigned n = box_node(P, p, k);
+        if (owner[n] != sphere) continue;
+        if (last) owner[n] = IBM_NO_OWNER;
+        const unsigned long long a0 = faux[n], a1 = faux[N + n], a2 = faux[2 * N + n];
+        if ((a0 | a1 | a2) == 0ull) continue;
         const float rho = fields[n];
+        const unsigned long long av[3] = {a0, a1, a2};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float v = from_fix(faux[a * N + n]);
+            const float v = from_fix(av[a]);
             fields[(1 + a) * N + n] += 0.5f * v / rho;
             fibm[a * N + n] += v;
             faux[a * N + n] = 0ull;
@@ -783,16 +805,20 @@ __global__ void k_ibm_euler(IbmParams P, float* fields, unsigned long long* faux
     }
 }
 
-
-__global__ void k_ibm_fixup(const float* fields, long long N, const int* list, const int* count, float* rho, float* ux,
-                            float* uy, float* uz) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= *count) return;
-    const int n = list[k];
-    if (rho) rho[n] = fields[n];
-    if (ux) ux[n] = fields[N + n];
-    if (uy) uy[n] = fields[2 * N + n];
-    if (uz) uz[n] = fields[3 * N + n];
+// The IBM macroscopics of this step's box nodes into the caller's arrays.
+__global__ void __launch_bounds__(IBM_THREADS) k_ibm_fixup(IbmParams P, const DPart* parts, const float* fields,
+                                                            int split, float* rho, float* ux, float* uy, float* uz) {
+    const size_t N = (size_t)P.nx * P.ny * P.nz;
+    const DPart& p = parts[blockIdx.x / split];
+    const int sub = blockIdx.x % split;
+    const long long tot = (long long)p.box_n[0] * p.box_n[1] * p.box_n[2];
+    for (long long k = (long long)sub * blockDim.x + threadIdx.x; k < tot; k += (long long)split * blockDim.x) {
+        const unsigned n = box_node(P, p, k);
+        if (rho) rho[n] = fields[n];
+        if (ux) ux[n] = fields[N + n];
+        if (uy) uy[n] = fields[2 * N + n];
+        if (uz) uz[n] = fields[3 * N + n];
+    }
 }
 
 // ---------------------------------------------------------------- host --
@@ -845,11 +871,11 @@ static cudaError_t launch_gather(vlbm_sim* s, IbmState* st) {
     const StepParams sp = make_params(s);
     const bool pr = sp.pairH > 0;
     if (s->parity == 1) {
-        if (pr) k_ibm_gather<Q, ST, true, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
-        else k_ibm_gather<Q, ST, true, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
+        if (pr) k_ibm_gather<Q, ST, true, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
+        else k_ibm_gather<Q, ST, true, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
     } else {
-        if (pr) k_ibm_gather<Q, ST, false, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
-        else k_ibm_gather<Q, ST, false, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->list, st->count, st->gsplit);
+        if (pr) k_ibm_gather<Q, ST, false, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
+        else k_ibm_gather<Q, ST, false, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
     }
     return cudaGetLastError();
 }
@@ -872,14 +898,9 @@ vlbm_status ibm_step(vlbm_sim* s) {
     const IbmParams& P = st->prm;
     cudaStream_t cs = s->stream;
     k_ibm_begin<<<st->np + 1, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nfx, st->nfy, st->nfz,
-                                                     st->ndx, st->ndy, st->ndz, st->contrib, st->count);
+                                                     st->ndx, st->ndy, st->ndz, st->contrib, st->clock);
     IBM_CUDA(cudaGetLastError());
     IBM_CUDA(gather_dispatch(s, st));
-    // grid-stride over the touched-node list (and the Lagrangian nodes in the
-    // last iteration): enough blocks for the boxes of all spheres, at most one
-    // per 256 lattice nodes
-    const int euler_blocks = (int)std::min<long long>(
-        (s->N + 255) / 256, std::max<long long>(std::max<long long>(1, st->euler_blocks), (st->nnodes + 255) / 256));
     const int iters = std::max(1, st->cfg.max_iterations);
     for (int it = 0; it < iters; ++it) {
         const int last = it == iters - 1;
@@ -888,10 +909,11 @@ vlbm_status ibm_step(vlbm_sim* s) {
                                                                          st->ndz, st->fields, st->faux, st->fpart,
                                                                          st->split);
         IBM_CUDA(cudaGetLastError());
-        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->fpart, st->split, last, st->count);
+        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->fpart, st->split, last, st->clock);
         IBM_CUDA(cudaGetLastError());
-        k_ibm_euler<<<euler_blocks, 256, 0, cs>>>(P, st->fields, st->faux, s->fibm, s->cls, st->list, st->count,
-                                                  st->parts, st->npid, st->nx, st->ny, st->nz, last);
+        k_ibm_euler<<<st->np * st->gsplit, IBM_THREADS, 0, cs>>>(P, st->fields, st->faux, s->fibm, s->cls, st->owner,
+                                                                 st->parts, st->npid, st->nx, st->ny, st->nz,
+                                                                 st->gsplit, last);
         IBM_CUDA(cudaGetLastError());
     }
     return VLBM_OK;
@@ -943,9 +965,10 @@ uint32_t ibm_record_bytes() { return (uint32_t)sizeof(DPart); }
 
 // The IBM state that carries from one step to the next: particle records
 // (positions, velocities, rotation, forces of the previous step, contact
-// history), Lagrangian nodes, the macroscopics of the touched nodes with their
-// list, and the step clock.  Per-step scratch (spread accumulators, pair and
-// per-CTA partials) is zero or rewritten before it is read, so it is not saved.
+// history, the boxes of the step taken), Lagrangian nodes, the IBM
+// macroscopics, and the step clock.  Per-step scratch (spread accumulators,
+// box owners, pair and per-CTA partials) is zero, IBM_NO_OWNER or rewritten
+// before it is read, so it is not saved.
 void ibm_state_regions(vlbm_sim* s, std::vector<StateRegion>& out) {
     IbmState* st = s->ibm;
     if (!st || st->np == 0) return;
@@ -956,8 +979,7 @@ void ibm_state_regions(vlbm_sim* s, std::vector<StateRegion>& out) {
         out.push_back({id++, p, nn * sizeof(double)});
     out.push_back({111, st->npid, nn * sizeof(int)});
     out.push_back({112, st->fields, 4 * N * sizeof(float)});
-    out.push_back({113, st->list, N * sizeof(int)});
-    out.push_back({114, st->count, 2 * sizeof(int)});
+    out.push_back({114, st->clock, sizeof(int)});
 }
 
 void ibm_counts(const vlbm_sim* s, int* np, int* nn) {
@@ -968,7 +990,8 @@ void ibm_counts(const vlbm_sim* s, int* np, int* nn) {
 vlbm_status ibm_macroscopics_fixup(vlbm_sim* s, float* rho, float* ux, float* uy, float* uz) {
     IbmState* st = s->ibm;
     if (!st || st->np == 0 || s->step == 0) return VLBM_OK;
-    k_ibm_fixup<<<(int)((s->N + 255) / 256), 256, 0, s->stream>>>(st->fields, s->N, st->list, st->count, rho, ux, uy, uz);
+    k_ibm_fixup<<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(st->prm, st->parts, st->fields, st->gsplit, rho,
+                                                                    ux, uy, uz);
     return cuda_status(cudaGetLastError(), "ibm macroscopics fixup");
 }
 
@@ -978,8 +1001,8 @@ void ibm_destroy(IbmState* st, DeviceAllocator* a) {
     for (double* p : {st->nx, st->ny, st->nz, st->nS, st->nfx, st->nfy, st->nfz, st->ndx, st->ndy, st->ndz, st->contrib,
                       st->fpart})
         free_with(a, p);
-    free_with(a, st->npid); free_with(a, st->fields); free_with(a, st->faux); free_with(a, st->list);
-    free_with(a, st->count);
+    free_with(a, st->npid); free_with(a, st->fields); free_with(a, st->faux); free_with(a, st->owner);
+    free_with(a, st->clock);
     delete st;
 }
 
@@ -993,7 +1016,8 @@ void ibm_reset(vlbm_sim* s) {
     cudaMemcpyAsync(st->nz, st->init_nodes.data() + 2 * nn, nn * sizeof(double), cudaMemcpyHostToDevice, s->stream);
     cudaMemsetAsync(st->fields, 0, (size_t)4 * s->N * sizeof(float), s->stream);
     cudaMemsetAsync(st->faux, 0, (size_t)3 * s->N * sizeof(unsigned long long), s->stream);
-    cudaMemsetAsync(st->count, 0, 2 * sizeof(int), s->stream);   // no touched nodes, step clock 0
+    cudaMemsetAsync(st->owner, 0xFF, (size_t)s->N * sizeof(unsigned), s->stream);   // IBM_NO_OWNER
+    cudaMemsetAsync(st->clock, 0, sizeof(int), s->stream);
 }
 
 }  // namespace vlbm
@@ -1104,8 +1128,8 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
     if (e == cudaSuccess) e = dalloc((void**)&st->npid, nn * sizeof(int));
     if (e == cudaSuccess) e = dalloc((void**)&st->fields, 4 * N * sizeof(float));
     if (e == cudaSuccess) e = dalloc((void**)&st->faux, 3 * N * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = dalloc((void**)&st->list, N * sizeof(int));
-    if (e == cudaSuccess) e = dalloc((void**)&st->count, 2 * sizeof(int));
+    if (e == cudaSuccess) e = dalloc((void**)&st->owner, N * sizeof(unsigned));
+    if (e == cudaSuccess) e = dalloc((void**)&st->clock, sizeof(int));
     if (e == cudaSuccess) e = dalloc((void**)&st->contrib, (size_t)n * n * 6 * sizeof(double));
     {   // CTAs per sphere of the interpolation/spreading kernel: about
         // IBM_NODES_PER_CTA Lagrangian nodes each for the largest sphere
@@ -1116,7 +1140,7 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
         st->split = std::min(IBM_MAX_SPLIT, std::max(1, (most + IBM_NODES_PER_CTA - 1) / IBM_NODES_PER_CTA));
     }
     if (e == cudaSuccess) e = dalloc((void**)&st->fpart, (size_t)n * st->split * 6 * sizeof(double));
-    {   // CTAs per sphere of the gather: about two box nodes per thread for the largest sphere
+    {   // CTAs per sphere of the box passes: about two box nodes per thread for the largest sphere
         long long maxbox = 1;
         for (int k = 0; k < n; ++k) {
             const long long side = (long long)std::ceil(sp[k].diameter) + 6;
@@ -1124,7 +1148,6 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
                                           std::min<long long>(side, c.nz));
         }
         st->gsplit = (int)std::min<long long>(IBM_MAX_SPLIT, std::max<long long>(1, maxbox / (2 * IBM_THREADS)));
-        st->euler_blocks = ((long long)n * maxbox + 255) / 256;
     }
     if (e == cudaSuccess && !s->fibm) {
         e = sim_malloc(s, (void**)&s->fibm, 3 * N * sizeof(float));
@@ -1139,10 +1162,10 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
     if (e == cudaSuccess) e = cudaMemcpy(st->npid, pid.data(), nn * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(st->fields, 0, 4 * N * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(st->faux, 0, 3 * N * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(st->count, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(st->owner, 0xFF, N * sizeof(unsigned));   // IBM_NO_OWNER
     if (e == cudaSuccess) {   // the contact history clock starts at the lattice's step count
         const int clock = (int)s->step;
-        e = cudaMemcpy(st->count + 1, &clock, sizeof(int), cudaMemcpyHostToDevice);
+        e = cudaMemcpy(st->clock, &clock, sizeof(int), cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) e = cudaMemset(s->fibm, 0, 3 * N * sizeof(float));
     if (e != cudaSuccess) { ibm_destroy(st, s->allocator); return cuda_status(e, "IBM setup"); }

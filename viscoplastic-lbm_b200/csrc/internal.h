@@ -13,7 +13,6 @@ enum : uint8_t {
     NODE_BULK = 0,       // plain periodic streaming, no boundary rule
     NODE_BC = 1,         // boundary node: look up bc_slot / BcRec
     NODE_UNUSED = 2,     // outside the fluid (map bit IS_USED clear): not updated
-    NODE_IBM_SET = 0x20,  // node listed by this step's IBM gather
     NODE_IBM_FORCE = 0x40 // IBM force present in the dense force field
 };
 
@@ -69,6 +68,12 @@ struct StepParams {
     long long N;
     int nbc;
     int pairH;                  // z-paired population layout: NZ/2, or 0 for the natural layout
+    int pairBlk;                // z-paired layout stored in blocks of 32 pair-nodes (NX % 32 == 0)
+    // pair step tiles (32 consecutive pair-nodes, one warp): 1 where a tile holds
+    // a boundary or unused node, and the list of those tiles
+    const uint8_t* tile_special;
+    const int32_t* special_tiles;
+    int n_special;
     int apply_bc;               // 0 on the first step after (re)initialisation
     float omega_newt;           // 1/tau
     float fx, fy, fz;           // body force

@@ -29,8 +29,12 @@ struct Mom2 {
     float2 pxx, pyy, pzz, pxy, pxz, pyz;
 };
 
-template <int Q, bool NEED_PI>
-__device__ __forceinline__ Mom2 moments2(const float2 (&g)[Q], float2 fx, float2 fy, float2 fz, float rho0) {
+// SCALED: g holds the stored half-precision values, deviations times a power
+// of two (1 / inv_scale); the ten sums are scaled back instead of the Q
+// populations, which gives the same bits (a power-of-two scale is exact).
+template <int Q, bool NEED_PI, bool SCALED = false>
+__device__ __forceinline__ Mom2 moments2(const float2 (&g)[Q], float2 fx, float2 fy, float2 fz, float rho0,
+                                         float inv_scale = 1.f) {
     Mom2 m;
     float2 rho = g[0], jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
     float2 sxx = f2(0.f), syy = f2(0.f), szz = f2(0.f), sxy = f2(0.f), sxz = f2(0.f), syz = f2(0.f);
@@ -49,6 +53,15 @@ __device__ __forceinline__ Mom2 moments2(const float2 (&g)[Q], float2 fx, float2
             if (cx && cy) sxy = (cx * cy > 0) ? add2(sxy, e) : sub2(sxy, e);
             if (cx && cz) sxz = (cx * cz > 0) ? add2(sxz, e) : sub2(sxz, e);
             if (cy && cz) syz = (cy * cz > 0) ? add2(syz, e) : sub2(syz, e);
+        }
+    }
+    if (SCALED) {
+        const float2 k = f2(inv_scale);
+        rho = mul2(rho, k);
+        jx = mul2(jx, k); jy = mul2(jy, k); jz = mul2(jz, k);
+        if (NEED_PI) {
+            sxx = mul2(sxx, k); syy = mul2(syy, k); szz = mul2(szz, k);
+            sxy = mul2(sxy, k); sxz = mul2(sxz, k); syz = mul2(syz, k);
         }
     }
     m.drho = rho;
@@ -88,9 +101,12 @@ __device__ __forceinline__ float2 stress_aux2(const Mom2& m, float2 fx, float2 f
 }
 
 // Collision in place on deviations, both lanes (the formulas of collide()).
+// The result is in deviation units; `gscale` is what the incoming g must be
+// multiplied by to be deviations (inv_scale for stored half values, 1
+// otherwise), a power of two that BGK folds into its (1 - omega) factor.
 template <int Q, int OP>
 __device__ __forceinline__ void collide2(float2 (&g)[Q], const Mom2& m, float2 omega, float2 fx, float2 fy,
-                                         float2 fz) {
+                                         float2 fz, float gscale = 1.f) {
     const float2 B = fma2(omega, f2(-0.5f), f2(1.f));
     const float2 uu = fma2(m.ux, m.ux, fma2(m.uy, m.uy, mul2(m.uz, m.uz)));
     const float2 uF = fma2(m.ux, fx, fma2(m.uy, fy, mul2(m.uz, fz)));
@@ -132,7 +148,7 @@ __device__ __forceinline__ void collide2(float2 (&g)[Q], const Mom2& m, float2 o
             g[i + 1] = mul2(w, sub2(E, O));
         }
     } else {
-        const float2 om1 = sub2(f2(1.f), omega);
+        const float2 om1 = mul2(sub2(f2(1.f), omega), f2(gscale));
         const float2 base = fma2(omega, fma2(mul2(m.rho, uu), f2(-1.5f), m.drho), mul2(BuF, f2(-3.f)));
         const float2 orho = mul2(omega, m.rho);
         const float2 r45 = mul2(orho, f2(4.5f)), r3 = mul2(orho, f2(3.f)), b9 = mul2(B, f2(9.f)),

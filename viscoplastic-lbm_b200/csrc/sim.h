@@ -47,6 +47,10 @@ struct vlbm_sim {
     float* side[2] = {nullptr, nullptr};  // [Q][nbc] post-collision at boundary nodes
     int nbc = 0;
     int pairH = 0;                   // z-paired layout (NZ/2) or 0
+    int pairBlk = 0;                 // z-paired pairs stored in blocks of 32 (pair_elem)
+    uint8_t* tile_special = nullptr; // [M/32] pair-step tiles with a boundary or unused node
+    int32_t* special_tiles = nullptr;  // indices of those tiles (n_special)
+    int n_special = 0;
     float* omega = nullptr;          // [N] Power-Law state
     float* fibm = nullptr;           // [3][N] IBM force (allocated with spheres)
     unsigned int* err = nullptr;     // device error word

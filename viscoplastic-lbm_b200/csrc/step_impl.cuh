@@ -375,12 +375,18 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int
     apply_bc<Q>(f, p, p.side_prev, slot, x, y, z, nb, n);
 }
 
-// Storage index of node (x, y, z) in the z-paired layout: nodes z and z+H
-// (H = NZ/2) of one (x, y) column are neighbours in memory.
-__device__ __forceinline__ size_t pair_index(const StepParams& p, int x, int y, int z) {
+// Element index of population i of node (x, y, z) in the z-paired layouts:
+// nodes z and z+H (H = NZ/2) of one (x, y) column are neighbours in memory
+// (lane 0 / 1 of pair-node m).  Plain pairs: Q planes of N/2 pairs.  Blocked
+// pairs (NX % 32 == 0): blocks of 32 consecutive pair-nodes, each holding
+// all Q populations of its nodes, [m / 32][Q][32][2].
+template <int Q>
+__device__ __forceinline__ size_t pair_elem(const StepParams& p, int i, int x, int y, int z) {
     const int lane = z >= p.pairH ? 1 : 0;
     const int zp = z - lane * p.pairH;
-    return ((((size_t)zp * p.ny + y) * p.nx + x) << 1) | (size_t)lane;
+    const size_t m = ((size_t)zp * p.ny + y) * p.nx + x;
+    if (p.pairBlk) return (((((m >> 5) * Q + (size_t)i) << 5) | (m & 31u)) << 1) | (size_t)lane;
+    return (size_t)i * (size_t)p.N + ((m << 1) | (size_t)lane);
 }
 __device__ __forceinline__ int wrap1(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
@@ -397,11 +403,11 @@ __device__ __forceinline__ int gather(const StepParams& p, const float* side_pre
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             if (!ODD) {
-                f[i] = S::ld(A + (size_t)i * N + pair_index(p, x, y, z), Lattice<Q>::w(i), p);
+                f[i] = S::ld(A + pair_elem<Q>(p, i, x, y, z), Lattice<Q>::w(i), p);
             } else {
-                const size_t src = pair_index(p, wrap1(x - lat_cx(i), p.nx), wrap1(y - lat_cy(i), p.ny),
-                                              wrap1(z - lat_cz(i), p.nz));
-                f[i] = S::ld(A + (size_t)lat_opp(i) * N + src, Lattice<Q>::w(i), p);
+                const size_t src = pair_elem<Q>(p, lat_opp(i), wrap1(x - lat_cx(i), p.nx), wrap1(y - lat_cy(i), p.ny),
+                                                wrap1(z - lat_cz(i), p.nz));
+                f[i] = S::ld(A + src, Lattice<Q>::w(i), p);
             }
         }
         cls = p.cls[n];
@@ -523,7 +529,11 @@ __device__ __forceinline__ float relax(const StepParams& p, float eta_old, float
         return p.omega_p * fmaxf(0.f, 1.f - __fdividef(p.yield, aux));
     } else if (RHEO == VLBM_POWERLAW) {
         const float gd = 3.f * aux / (0.5f + 3.f * eta_old);
-        eta_new = (gd <= p.gamma0) ? p.k_cons : p.k_cons * powf(gd, p.n_index - 1.f);
+        // gd^(n-1): the flow indices 0.5, 1 and 1.5 take a square root, a
+        // reciprocal square root (<= 2 ulp) or nothing instead of powf
+        const float e = p.n_index - 1.f;
+        const float pw = e == -0.5f ? rsqrtf(gd) : (e == 0.5f ? sqrtf(gd) : (e == 0.f ? 1.f : powf(gd, e)));
+        eta_new = (gd <= p.gamma0) ? p.k_cons : p.k_cons * pw;
         return 1.f / (0.5f + 3.f * eta_new);
     }
     return p.omega_newt;
@@ -599,16 +609,17 @@ __device__ __forceinline__ void collide(float (&f)[Q], const Mom& m, float omega
 
 // Everything after the gather for one node: IBM force read and reset
 // (lbm.cu:45-58), moments, relaxation (lbm.cu:192-222), collision, and the
-// post-collision copy of boundary nodes (lbm.cu:463-470).
+// post-collision copy of boundary nodes (lbm.cu:463-470).  `eta_old` is the
+// node's Power-Law state p.omega[n], loaded by the caller ahead of the gather.
 template <int Q, int OP, int RHEO>
 __device__ __forceinline__ void relax_and_collide(const StepParams& p, float* side_next, unsigned n, uint8_t cls,
-                                                  int slot, float (&f)[Q]) {
+                                                  int slot, float (&f)[Q], float eta_old) {
     float fx = p.fx, fy = p.fy, fz = p.fz;
     if (cls & NODE_IBM_FORCE) {
         const size_t N = (size_t)p.N;
         fx += p.fibm[n]; fy += p.fibm[N + n]; fz += p.fibm[2 * N + n];
         p.fibm[n] = 0.f; p.fibm[N + n] = 0.f; p.fibm[2 * N + n] = 0.f;
-        p.cls[n] = cls & (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
+        p.cls[n] = cls & (uint8_t)~NODE_IBM_FORCE;
     }
     constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
     const Mom m = moments<Q, NEED_PI>(f, fx, fy, fz, p.rho0);
@@ -616,9 +627,8 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, float* si
     float omega = p.omega_newt;
     if (RHEO != VLBM_NEWTONIAN) {
         const float aux = stress_aux(m, fx, fy, fz);
-        const float old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;
         float eta = 0.f;
-        omega = relax<RHEO>(p, old, aux, eta);
+        omega = relax<RHEO>(p, eta_old, aux, eta);
         if (RHEO == VLBM_POWERLAW) p.omega[n] = eta;  // state update, lbm.cu:215-219
     }
     collide<Q, OP>(f, m, omega, fx, fy, fz);
@@ -635,7 +645,7 @@ __device__ __forceinline__ void relax_and_collide(const StepParams& p, float* si
 template <int Q, int OP, int RHEO>
 __device__ __forceinline__ void relax_and_collide(const StepParams& p, unsigned n, uint8_t cls, int slot,
                                                   float (&f)[Q]) {
-    relax_and_collide<Q, OP, RHEO>(p, p.side_next, n, cls, slot, f);
+    relax_and_collide<Q, OP, RHEO>(p, p.side_next, n, cls, slot, f, (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f);
 }
 
 // ------------------------------------------------------------ kernels --
@@ -654,10 +664,11 @@ __device__ __forceinline__ void step_node(const StepParams& p, const float* side
     Nbr nb;
     nb.init(x, y, z, p.nx, p.ny, p.nz);
 
+    const float eta_old = (RHEO == VLBM_POWERLAW) ? p.omega[n] : 0.f;   // loaded with the populations
     float f[Q];
     uint8_t cls;
     const int slot = gather<Q, ST, ODD>(p, side_prev, use_bc, n, nb, x, y, z, f, cls);
-    relax_and_collide<Q, OP, RHEO>(p, side_next, n, cls, slot, f);
+    relax_and_collide<Q, OP, RHEO>(p, side_next, n, cls, slot, f, eta_old);
     nb.launder();
     Rng rng(n, seed);
     T* plane = static_cast<T*>(p.pop);
@@ -846,12 +857,9 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
     if (n >= (unsigned)p.N) return;
     T* A = static_cast<T*>(p.pop);
     const size_t N = (size_t)p.N;
-    size_t sidx = n;
-    if (PAIRED) {
-        const int x = (int)(n % (unsigned)p.nx);
-        const unsigned t = n / (unsigned)p.nx;
-        sidx = pair_index(p, x, (int)(t % (unsigned)p.ny), (int)(t / (unsigned)p.ny));
-    }
+    const int x = (int)(n % (unsigned)p.nx);
+    const unsigned t = n / (unsigned)p.nx;
+    const int y = (int)(t % (unsigned)p.ny), z = (int)(t / (unsigned)p.ny);
     const float uu = ux * ux + uy * uy + uz * uz;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
@@ -862,7 +870,8 @@ __global__ void __launch_bounds__(256) k_set_pops(const StepParams p, const floa
             const float cu = lat_cx(i) * ux + lat_cy(i) * uy + lat_cz(i) * uz;
             v = Lattice<Q>::w(i) * rho * (1.f - 1.5f * uu + 3.f * cu * (1.f + 1.5f * cu));
         }
-        S::st_abs(A + (size_t)i * N + sidx, v, Lattice<Q>::w(i), p);
+        const size_t e = PAIRED ? pair_elem<Q>(p, i, x, y, z) : (size_t)i * N + n;
+        S::st_abs(A + e, v, Lattice<Q>::w(i), p);
     }
     if (p.omega) p.omega[n] = __int_as_float(0x7f800000);  // eta = +inf <=> omega = 0 (lbmInitialization.cu:111)
 }
@@ -880,7 +889,9 @@ template <> struct Pair<VLBM_STORE_F32> {
     }
     static __device__ __forceinline__ V swap(const V& v) { return make_float2(v.y, v.x); }
     // both lanes as deviations / packed from deviations (stored as they are)
+    static constexpr bool kScaled = false;
     static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams&) { return v; }
+    static __device__ __forceinline__ float2 raw2(const V& v) { return v; }
     static __device__ __forceinline__ V pack2(float2 g, float, const StepParams&, Rng&, Rng&) { return g; }
 };
 template <> struct Pair<VLBM_STORE_F16> {
@@ -896,6 +907,10 @@ template <> struct Pair<VLBM_STORE_F16> {
     static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams& s) {
         return mul2(__half22float2(v), f2(s.inv_scale));
     }
+    // the stored values times `scale` (a power of two): k_step2 scales the moment
+    // sums instead of every population, which gives the same bits
+    static constexpr bool kScaled = true;
+    static __device__ __forceinline__ float2 raw2(const V& v) { return __half22float2(v); }
     // both lanes rounded stochastically (13 random bits each, two slices of one
     // draw) and packed with one conversion.  The FP16 scale is 2^k with
     // 0 <= k <= 24 (checked at creation), so g * scale is k added to the
@@ -926,6 +941,8 @@ template <> struct Pair<VLBM_STORE_BF16> {
     static __device__ __forceinline__ float2 get2(const V& v, float, const StepParams& s) {
         return mul2(__bfloat1622float2(v), f2(s.inv_scale));
     }
+    static constexpr bool kScaled = true;
+    static __device__ __forceinline__ float2 raw2(const V& v) { return __bfloat1622float2(v); }
     static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
         const float2 v = mul2(g, f2(s.scale));
         const unsigned r = r0.next();
@@ -936,17 +953,49 @@ template <> struct Pair<VLBM_STORE_BF16> {
     }
 };
 
-// One thread advances the node pair (x, y, zp) / (x, y, zp+H).  Every access is
-// one aligned vector of the two nodes, also for the x-shifted neighbours of
-// the odd step; crossing the periodic z seam swaps the two lanes.
-template <int Q, int OP, int RHEO, int ST, bool ODD>
-__global__ void __launch_bounds__(256) k_step2(const StepParams p) {
+// Neighbour offsets of a pair-node in blocked storage, in pairs: own(m') -
+// own(m) with own(m) = (m / 32) * 32 Q + m % 32.  A y or z neighbour keeps m %
+// 32 (rows hold whole blocks), so its offset is the pair-space offset times
+// Q; an x neighbour may sit in the next or previous block.  Offsets along the
+// axes add up for the diagonal neighbours.
+struct BlkNbr {
+    int xm, xp, ym, yp, zm, zp;
+    template <int Q>
+    __device__ __forceinline__ void init(const Nbr& pn, unsigned m) {
+        const int own = (int)((m >> 5) * (Q * 32u) + (m & 31u));
+        const unsigned a = (unsigned)((int)m + pn.xm), b = (unsigned)((int)m + pn.xp);
+        xm = (int)((a >> 5) * (Q * 32u) + (a & 31u)) - own;
+        xp = (int)((b >> 5) * (Q * 32u) + (b & 31u)) - own;
+        ym = pn.ym * Q; yp = pn.yp * Q; zm = pn.zm * Q; zp = pn.zp * Q;
+    }
+    __device__ __forceinline__ void launder() {
+        asm volatile("" : "+r"(xm), "+r"(xp), "+r"(ym), "+r"(yp), "+r"(zm), "+r"(zp));
+    }
+    __device__ __forceinline__ int off(int dx, int dy, int dz) const {
+        return (dx > 0 ? xp : (dx < 0 ? xm : 0)) + (dy > 0 ? yp : (dy < 0 ? ym : 0)) +
+               (dz > 0 ? zp : (dz < 0 ? zm : 0));
+    }
+};
+
+// One thread advances the node pair (x, y, zp) / (x, y, zp+H), pair-node m.
+// Every access is one aligned vector of the two nodes, also for the x-shifted
+// neighbours of the odd step; crossing the periodic z seam swaps the two lanes.
+//
+// BLK (blocked pairs, NX % 32 == 0): a warp's 32 pairs are one block, whose Q
+// planes follow each other, so plane j of the thread's own pair is at a
+// compile-time offset (32 j) from one pointer, and a neighbour's is that plus
+// one of six axis offsets formed once per thread (BlkNbr).
+//
+// BULK: the warp's tile (m / 32) holds no boundary and no unused node, so the
+// boundary rules, the side store and the unused-node path are compiled out
+// (the bulk kernel then fits 64 registers: 4 resident blocks of 256 instead
+// of 3).  A BULK warp that finds such a node in its class bytes, loaded with
+// the populations, returns before it writes anything; k_step2 runs those
+// tiles from their list.
+template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK, bool BULK>
+__device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned seed, const unsigned m) {
     using PV = Pair<ST>;
     using V = typename PV::V;
-    const unsigned seed = step_seed(p, ODD);
-    const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned M = (unsigned)(p.N >> 1);
-    if (m >= M) return;
     const int H = p.pairH;
     const int x = (int)(m % (unsigned)p.nx);
     const unsigned t = m / (unsigned)p.nx;
@@ -955,16 +1004,32 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
     Nbr pn;                       // neighbour offsets in pair space
     pn.init(x, y, zp, p.nx, p.ny, H);
     const bool seam_lo = zp == 0, seam_hi = zp == H - 1;
-    const size_t Np = (size_t)p.N >> 1;   // pairs per plane
+    const unsigned n0 = (unsigned)(((size_t)zp * p.ny + y) * p.nx + x);
+    const unsigned n1 = (unsigned)(((size_t)(zp + H) * p.ny + y) * p.nx + x);
+    // the Power-Law state of both nodes, loaded with the populations
+    const float eta0 = (RHEO == VLBM_POWERLAW) ? p.omega[n0] : 0.f;
+    const float eta1 = (RHEO == VLBM_POWERLAW) ? p.omega[n1] : 0.f;
+    const size_t Np = (size_t)p.N >> 1;   // pairs per plane (plain pairs)
     V in[Q];
-    const V* plane = reinterpret_cast<const V*>(p.pop);
+    const V* __restrict__ P = reinterpret_cast<const V*>(p.pop);
+    const size_t own = BLK ? (size_t)(m >> 5) * (Q * 32) + (m & 31u) : 0;
+    const V* __restrict__ Pown = P + own;
+    BlkNbr bn;
+    if (BLK) bn.init<Q>(pn, m);
 #pragma unroll
-    for (int j = 0; j < Q; ++j, plane += Np) {
-        if (!ODD) {
-            in[j] = plane[m];
+    for (int j = 0; j < Q; ++j) {
+        if (BLK) {
+            if (!ODD) {
+                in[j] = Pown[32 * j];
+            } else {
+                const int i = lat_opp(j);
+                in[i] = Pown[(ptrdiff_t)bn.off(-lat_cx(i), -lat_cy(i), -lat_cz(i)) + 32 * j];
+            }
+        } else if (!ODD) {
+            in[j] = P[(size_t)j * Np + m];
         } else {
             const int i = lat_opp(j);
-            in[i] = plane[m + pn.off(-lat_cx(i), -lat_cy(i), -lat_cz(i))];
+            in[i] = P[(size_t)j * Np + (unsigned)((int)m + pn.off(-lat_cx(i), -lat_cy(i), -lat_cz(i)))];
         }
     }
     // Crossing the z seam exchanges the lanes.  Only the two seam planes of
@@ -977,15 +1042,21 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             if ((cz > 0 && seam_lo) || (cz < 0 && seam_hi)) in[i] = PV::swap(in[i]);
         }
     }
-    // both nodes as float2 deviations: lane 0 is (x, y, zp), lane 1 (x, y, zp + H)
+    // both nodes as float2: lane 0 is (x, y, zp), lane 1 (x, y, zp + H).  Half
+    // storage is read as stored (deviation * scale); the moment sums are
+    // scaled instead, and the boundary rules see scaled-back values.
+    constexpr bool SC = PV::kScaled;
     float2 g[Q];
 #pragma unroll
-    for (int i = 0; i < Q; ++i) g[i] = PV::get2(in[i], Lattice<Q>::w(i), p);
-    const unsigned n0 = (unsigned)(((size_t)zp * p.ny + y) * p.nx + x);
-    const unsigned n1 = (unsigned)(((size_t)(zp + H) * p.ny + y) * p.nx + x);
+    for (int i = 0; i < Q; ++i) g[i] = PV::raw2(in[i]);
     const uint8_t c0 = p.cls[n0], c1 = p.cls[n1];
+    if (BULK) {   // every lane of the tile that exists (m < M) votes; m % 32 is the lane
+        const unsigned valid = min(32u, (unsigned)(p.N >> 1) - (m & ~31u));
+        const unsigned tile = valid == 32u ? 0xffffffffu : ((1u << valid) - 1u);
+        if (__any_sync(tile, (c0 | c1) & (NODE_BC | NODE_UNUSED))) return;
+    }
     int slot0 = -1, slot1 = -1;
-    if ((c0 | c1) & NODE_BC) {   // boundary rules per lane, on scalars
+    if (!BULK && ((c0 | c1) & NODE_BC)) {   // boundary rules per lane, on scalars
 #pragma unroll
         for (int lane = 0; lane < 2; ++lane) {
             const uint8_t cl = lane ? c1 : c0;
@@ -997,12 +1068,12 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             if (p.apply_bc) {
                 float f[Q];
 #pragma unroll
-                for (int i = 0; i < Q; ++i) f[i] = lane_of(g[i], lane);
+                for (int i = 0; i < Q; ++i) f[i] = SC ? lane_of(g[i], lane) * p.inv_scale : lane_of(g[i], lane);
                 Nbr nb;
                 nb.init(x, y, zl, p.nx, p.ny, p.nz);
                 apply_bc<Q>(f, p, sl, x, y, zl, nb, nl);
 #pragma unroll
-                for (int i = 0; i < Q; ++i) set_lane(g[i], lane, f[i]);
+                for (int i = 0; i < Q; ++i) set_lane(g[i], lane, SC ? f[i] * p.scale : f[i]);
             }
         }
     }
@@ -1018,11 +1089,11 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             set_lane(fy2, lane, p.fy + p.fibm[N + nl]);
             set_lane(fz2, lane, p.fz + p.fibm[2 * N + nl]);
             p.fibm[nl] = 0.f; p.fibm[N + nl] = 0.f; p.fibm[2 * N + nl] = 0.f;
-            p.cls[nl] = cl & (uint8_t)~(NODE_IBM_FORCE | NODE_IBM_SET);
+            p.cls[nl] = cl & (uint8_t)~NODE_IBM_FORCE;
         }
     }
     constexpr bool NEED_PI = (OP == VLBM_OP_REGULARIZED) || (RHEO != VLBM_NEWTONIAN);
-    const Mom2 mm = moments2<Q, NEED_PI>(g, fx2, fy2, fz2, p.rho0);
+    const Mom2 mm = moments2<Q, NEED_PI, SC>(g, fx2, fy2, fz2, p.rho0, p.inv_scale);
     if ((!(mm.rho.x > 0.f && mm.rho.x < 1e30f) && !(c0 & NODE_UNUSED)) ||
         (!(mm.rho.y > 0.f && mm.rho.y < 1e30f) && !(c1 & NODE_UNUSED)))
         atomicOr(p.err, 1u);
@@ -1032,14 +1103,13 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
 #pragma unroll
         for (int lane = 0; lane < 2; ++lane) {
             const unsigned nl = lane ? n1 : n0;
-            const float old = (RHEO == VLBM_POWERLAW) ? p.omega[nl] : 0.f;
             float eta = 0.f;
-            set_lane(omega, lane, relax<RHEO>(p, old, lane_of(aux, lane), eta));
+            set_lane(omega, lane, relax<RHEO>(p, lane ? eta1 : eta0, lane_of(aux, lane), eta));
             if (RHEO == VLBM_POWERLAW) p.omega[nl] = eta;   // state update, lbm.cu:215-219
         }
     }
-    collide2<Q, OP>(g, mm, omega, fx2, fy2, fz2);
-    if ((c0 | c1) & NODE_UNUSED) {   // lbm.cu:23-24: not updated; rest equilibrium stays in the slots
+    collide2<Q, OP>(g, mm, omega, fx2, fy2, fz2, SC ? p.inv_scale : 1.f);
+    if (!BULK && ((c0 | c1) & NODE_UNUSED)) {   // lbm.cu:23-24: not updated; rest equilibrium stays in the slots
         const bool u0 = c0 & NODE_UNUSED, u1 = c1 & NODE_UNUSED;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -1047,7 +1117,7 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
             if (u1) g[i].y = 0.f;
         }
     }
-    if (slot0 >= 0 || slot1 >= 0) {   // post-collision values of boundary nodes (lbm.cu:463-470)
+    if (!BULK && (slot0 >= 0 || slot1 >= 0)) {   // post-collision values of boundary nodes (lbm.cu:463-470)
         const size_t nbc = (size_t)p.nbc;
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -1072,12 +1142,51 @@ __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
         }
     }
     pn.launder();
-    V* out = reinterpret_cast<V*>(p.pop);
+    if (BLK) bn.launder();
+    V* __restrict__ Po = reinterpret_cast<V*>(p.pop);
+    V* __restrict__ Powo = Po + own;
 #pragma unroll
-    for (int j = 0; j < Q; ++j, out += Np) {
-        if (!ODD) out[m] = in[lat_opp(j)];
-        else out[m + pn.off(lat_cx(j), lat_cy(j), lat_cz(j))] = in[j];
+    for (int j = 0; j < Q; ++j) {
+        if (BLK) {
+            if (!ODD) Powo[32 * j] = in[lat_opp(j)];
+            else Powo[(ptrdiff_t)bn.off(lat_cx(j), lat_cy(j), lat_cz(j)) + 32 * j] = in[j];
+        } else if (!ODD) {
+            Po[(size_t)j * Np + m] = in[lat_opp(j)];
+        } else {
+            Po[(size_t)j * Np + (unsigned)((int)m + pn.off(lat_cx(j), lat_cy(j), lat_cz(j)))] = in[j];
+        }
     }
+}
+
+// Resident 256-thread blocks per SM asked of the bulk pair kernel (-Xptxas -v):
+// regularized D3Q19 fits 64 registers for 4 blocks (0 bytes of spill in the
+// even step, 12-36 in the odd one); BGK keeps every population live across
+// the collision and spills 40-180 bytes there, so it takes 3; D3Q27 spills
+// 30-250 bytes at 80 registers (3 blocks) and takes 2.
+template <int Q, int OP> constexpr int step2_bulk_blocks() {
+    return Q == 19 ? (OP == VLBM_OP_REGULARIZED ? 4 : 3) : 2;
+}
+
+// The pair step over every tile; tiles with a boundary or unused node return
+// (step2_pair, BULK) and are advanced by k_step2.
+template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
+__global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP>()) k_step2_bulk(const StepParams p) {
+    const unsigned seed = step_seed(p, ODD);
+    const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= (unsigned)(p.N >> 1)) return;
+    step2_pair<Q, OP, RHEO, ST, ODD, BLK, true>(p, seed, m);
+}
+
+// The pair step over the tiles with a boundary or unused node, one warp per
+// tile of the list p.special_tiles.
+template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
+__global__ void __launch_bounds__(256) k_step2(const StepParams p) {
+    const unsigned seed = step_seed(p, ODD);
+    const unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= (unsigned)p.n_special) return;
+    const unsigned m = ((unsigned)p.special_tiles[w] << 5) | (threadIdx.x & 31u);
+    if (m >= (unsigned)(p.N >> 1)) return;
+    step2_pair<Q, OP, RHEO, ST, ODD, BLK, false>(p, seed, m);
 }
 
 }  // namespace vlbm
