@@ -7,23 +7,42 @@ namespace vlbm {
 
 inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
 
+// Launch that may start before the previous kernel of the stream has finished
+// (programmatic dependent launch): that kernel triggers it at its start, and
+// the two touch disjoint memory.  Work launched after it waits for both.
+template <typename... Args>
+cudaError_t launch_overlapped(void (*kernel)(Args...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int Q, int OP, int RHEO, int ST>
 cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s) {
     if (p.pairH > 0) {  // z-paired layout: one thread per node pair; bulk tiles, then the listed ones
         const unsigned g = grid_for(p.N / 2, ls.block);
         const unsigned gs = grid_for((long long)p.n_special * 32, 256);
+        cudaError_t e;
         if (p.pairBlk) {
             if (odd) k_step2_bulk<Q, OP, RHEO, ST, true, true><<<g, ls.block, 0, s>>>(p);
             else k_step2_bulk<Q, OP, RHEO, ST, false, true><<<g, ls.block, 0, s>>>(p);
-            if (gs && odd) k_step2<Q, OP, RHEO, ST, true, true><<<gs, 256, 0, s>>>(p);
-            else if (gs) k_step2<Q, OP, RHEO, ST, false, true><<<gs, 256, 0, s>>>(p);
-        } else {
-            if (odd) k_step2_bulk<Q, OP, RHEO, ST, true, false><<<g, ls.block, 0, s>>>(p);
-            else k_step2_bulk<Q, OP, RHEO, ST, false, false><<<g, ls.block, 0, s>>>(p);
-            if (gs && odd) k_step2<Q, OP, RHEO, ST, true, false><<<gs, 256, 0, s>>>(p);
-            else if (gs) k_step2<Q, OP, RHEO, ST, false, false><<<gs, 256, 0, s>>>(p);
+            if ((e = cudaGetLastError()) != cudaSuccess || !gs) return e;
+            return odd ? launch_overlapped(k_step2<Q, OP, RHEO, ST, true, true>, gs, 256, s, p)
+                       : launch_overlapped(k_step2<Q, OP, RHEO, ST, false, true>, gs, 256, s, p);
         }
-        return cudaGetLastError();
+        if (odd) k_step2_bulk<Q, OP, RHEO, ST, true, false><<<g, ls.block, 0, s>>>(p);
+        else k_step2_bulk<Q, OP, RHEO, ST, false, false><<<g, ls.block, 0, s>>>(p);
+        if ((e = cudaGetLastError()) != cudaSuccess || !gs) return e;
+        return odd ? launch_overlapped(k_step2<Q, OP, RHEO, ST, true, false>, gs, 256, s, p)
+                   : launch_overlapped(k_step2<Q, OP, RHEO, ST, false, false>, gs, 256, s, p);
     }
     const unsigned g = grid_for(p.N, ls.block);
     if (odd) k_step<Q, OP, RHEO, ST, true><<<g, ls.block, 0, s>>>(p);

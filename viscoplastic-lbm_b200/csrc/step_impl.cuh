@@ -911,20 +911,16 @@ template <> struct Pair<VLBM_STORE_F16> {
     // sums instead of every population, which gives the same bits
     static constexpr bool kScaled = true;
     static __device__ __forceinline__ float2 raw2(const V& v) { return __half22float2(v); }
-    // both lanes rounded stochastically (13 random bits each, two slices of one
-    // draw) and packed with one conversion.  The FP16 scale is 2^k with
-    // 0 <= k <= 24 (checked at creation), so g * scale is k added to the
-    // exponent field: one integer add carries both the scaling and the random
-    // bits.  Identical to multiplying first for every finite g: a normal g
-    // stays normal, and zero or subnormal g becomes a float far below the
-    // smallest half, which the conversion rounds to a signed zero as before.
+    // both lanes rounded stochastically by the conversion itself (sm_100a
+    // cvt.rs: the low half takes its random bits from rbits[12:0], the high
+    // half from rbits[28:16]; measured, and unbiased to 1e-4 ulp over 4M
+    // draws).  One draw per pair; folding its upper half into the lower gives
+    // the low lane mixed bits, not the weak low bits of the congruential draw.
     static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
-        const unsigned k23 = __float_as_uint(s.scale) - 0x3F800000u;   // k << 23
+        const float2 v = mul2(g, f2(s.scale));
         const unsigned r = r0.next();
-        const float lo = __uint_as_float(__float_as_uint(g.x) + k23 + (r >> 19));
-        const float hi = __uint_as_float(__float_as_uint(g.y) + k23 + ((r >> 6) & 0x1FFFu));
         unsigned out;
-        asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(hi), "f"(lo));
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(v.y), "f"(v.x), "r"(r ^ (r >> 16)));
         return *reinterpret_cast<__half2*>(&out);
     }
 };
@@ -943,12 +939,12 @@ template <> struct Pair<VLBM_STORE_BF16> {
     }
     static constexpr bool kScaled = true;
     static __device__ __forceinline__ float2 raw2(const V& v) { return __bfloat1622float2(v); }
+    // cvt.rs for bfloat16: random bits rbits[15:0] (low half), [31:16] (high half)
     static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
         const float2 v = mul2(g, f2(s.scale));
         const unsigned r = r0.next();
-        const unsigned lo = (__float_as_uint(v.x) + (r >> 16)) >> 16;
-        const unsigned hi = (__float_as_uint(v.y) + (r & 0xFFFFu)) & 0xFFFF0000u;
-        const unsigned out = hi | lo;
+        unsigned out;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(v.y), "f"(v.x), "r"(r ^ (r >> 16)));
         return *reinterpret_cast<const __nv_bfloat162*>(&out);
     }
 };
@@ -1171,6 +1167,10 @@ template <int Q, int OP> constexpr int step2_bulk_blocks() {
 // (step2_pair, BULK) and are advanced by k_step2.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
 __global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP>()) k_step2_bulk(const StepParams p) {
+    // k_step2 (launched next, programmatic stream serialization) touches other
+    // tiles only: it may start as soon as every block here has started, and
+    // fills this grid's tail
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned seed = step_seed(p, ODD);
     const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= (unsigned)(p.N >> 1)) return;
