@@ -101,12 +101,14 @@ __device__ __forceinline__ float2 stress_aux2(const Mom2& m, float2 fx, float2 f
 }
 
 // Collision in place on deviations, both lanes (the formulas of collide()).
-// The result is in deviation units; `gscale` is what the incoming g must be
-// multiplied by to be deviations (inv_scale for stored half values, 1
-// otherwise), a power of two that BGK folds into its (1 - omega) factor.
+// `gscale` is what the incoming g must be multiplied by to be deviations
+// (inv_scale for stored half values, 1 otherwise); the result is deviations
+// times `oscale` (the storage scale for half storage, 1 otherwise).  Both are
+// powers of two, folded into the weights and BGK's (1 - omega) factor, which
+// gives the same bits as scaling before and after.
 template <int Q, int OP>
 __device__ __forceinline__ void collide2(float2 (&g)[Q], const Mom2& m, float2 omega, float2 fx, float2 fy,
-                                         float2 fz, float gscale = 1.f) {
+                                         float2 fz, float gscale = 1.f, float oscale = 1.f) {
     const float2 B = fma2(omega, f2(-0.5f), f2(1.f));
     const float2 uu = fma2(m.ux, m.ux, fma2(m.uy, m.uy, mul2(m.uz, m.uz)));
     const float2 uF = fma2(m.ux, fx, fma2(m.uy, fy, mul2(m.uz, fz)));
@@ -120,7 +122,7 @@ __device__ __forceinline__ void collide2(float2 (&g)[Q], const Mom2& m, float2 o
         const float2 alpha = fma2(B, f2(3.f), mul2(A, f2(-1.f / 3.f)));
         const float2 r3 = mul2(m.rho, f2(3.f)), r45 = mul2(m.rho, f2(4.5f)), b9 = mul2(B, f2(9.f));
         const float2 pxy2 = add2(m.pxy, m.pxy), pxz2 = add2(m.pxz, m.pxz), pyz2 = add2(m.pyz, m.pyz);
-        g[0] = mul2(f2(Lattice<Q>::w(0)), K0);
+        g[0] = mul2(f2(Lattice<Q>::w(0) * oscale), K0);
 #pragma unroll
         for (int i = 1; i < Q; i += 2) {
             const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
@@ -143,17 +145,17 @@ __device__ __forceinline__ void collide2(float2 (&g)[Q], const Mom2& m, float2 o
             if (cy && cz) S = (cy * cz > 0) ? add2(S, pyz2) : sub2(S, pyz2);
             const float2 E = fma2(cu, fma2(r45, cu, mul2(b9, cF)), fma2(A, S, K0));
             const float2 O = fma2(alpha, cF, mul2(r3, cu));
-            const float2 w = f2(Lattice<Q>::w(i));
+            const float2 w = f2(Lattice<Q>::w(i) * oscale);
             g[i] = mul2(w, add2(E, O));
             g[i + 1] = mul2(w, sub2(E, O));
         }
     } else {
-        const float2 om1 = mul2(sub2(f2(1.f), omega), f2(gscale));
+        const float2 om1 = mul2(sub2(f2(1.f), omega), f2(gscale * oscale));
         const float2 base = fma2(omega, fma2(mul2(m.rho, uu), f2(-1.5f), m.drho), mul2(BuF, f2(-3.f)));
         const float2 orho = mul2(omega, m.rho);
         const float2 r45 = mul2(orho, f2(4.5f)), r3 = mul2(orho, f2(3.f)), b9 = mul2(B, f2(9.f)),
                      b3 = mul2(B, f2(3.f));
-        g[0] = fma2(om1, g[0], mul2(f2(Lattice<Q>::w(0)), base));
+        g[0] = fma2(om1, g[0], mul2(f2(Lattice<Q>::w(0) * oscale), base));
 #pragma unroll
         for (int i = 1; i < Q; i += 2) {
             const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
@@ -169,7 +171,7 @@ __device__ __forceinline__ void collide2(float2 (&g)[Q], const Mom2& m, float2 o
                 cu = first ? (cz > 0 ? m.uz : mul2(m.uz, f2(-1.f))) : (cz > 0 ? add2(cu, m.uz) : sub2(cu, m.uz));
                 cF = first ? (cz > 0 ? fz : mul2(fz, f2(-1.f))) : (cz > 0 ? add2(cF, fz) : sub2(cF, fz));
             }
-            const float2 w = f2(Lattice<Q>::w(i));
+            const float2 w = f2(Lattice<Q>::w(i) * oscale);
             const float2 E = mul2(w, fma2(cu, fma2(r45, cu, mul2(b9, cF)), base));
             const float2 O = mul2(w, fma2(r3, cu, mul2(b3, cF)));
             g[i] = fma2(om1, g[i], add2(E, O));

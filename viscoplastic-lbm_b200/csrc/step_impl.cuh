@@ -916,8 +916,8 @@ template <> struct Pair<VLBM_STORE_F16> {
     // half from rbits[28:16]; measured, and unbiased to 1e-4 ulp over 4M
     // draws).  One draw per pair; folding its upper half into the lower gives
     // the low lane mixed bits, not the weak low bits of the congruential draw.
-    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
-        const float2 v = mul2(g, f2(s.scale));
+    // v: deviations times the storage scale (collide2's output).
+    static __device__ __forceinline__ V pack2(float2 v, float, const StepParams&, Rng& r0, Rng&) {
         const unsigned r = r0.next();
         unsigned out;
         asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(v.y), "f"(v.x), "r"(r ^ (r >> 16)));
@@ -939,9 +939,9 @@ template <> struct Pair<VLBM_STORE_BF16> {
     }
     static constexpr bool kScaled = true;
     static __device__ __forceinline__ float2 raw2(const V& v) { return __bfloat1622float2(v); }
-    // cvt.rs for bfloat16: random bits rbits[15:0] (low half), [31:16] (high half)
-    static __device__ __forceinline__ V pack2(float2 g, float, const StepParams& s, Rng& r0, Rng&) {
-        const float2 v = mul2(g, f2(s.scale));
+    // cvt.rs for bfloat16: random bits rbits[15:0] (low half), [31:16] (high
+    // half); v: deviations times the storage scale
+    static __device__ __forceinline__ V pack2(float2 v, float, const StepParams&, Rng& r0, Rng&) {
         const unsigned r = r0.next();
         unsigned out;
         asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(v.y), "f"(v.x), "r"(r ^ (r >> 16)));
@@ -1000,8 +1000,9 @@ __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned s
     Nbr pn;                       // neighbour offsets in pair space
     pn.init(x, y, zp, p.nx, p.ny, H);
     const bool seam_lo = zp == 0, seam_hi = zp == H - 1;
-    const unsigned n0 = (unsigned)(((size_t)zp * p.ny + y) * p.nx + x);
-    const unsigned n1 = (unsigned)(((size_t)(zp + H) * p.ny + y) * p.nx + x);
+    // node indices: (x, y, zp) is m, (x, y, zp + H) is m + N/2 (the even bulk
+    // step needs neither x, y, zp nor the neighbour offsets)
+    const unsigned n0 = m, n1 = m + (unsigned)(p.N >> 1);
     // the Power-Law state of both nodes, loaded with the populations
     const float eta0 = (RHEO == VLBM_POWERLAW) ? p.omega[n0] : 0.f;
     const float eta1 = (RHEO == VLBM_POWERLAW) ? p.omega[n1] : 0.f;
@@ -1011,7 +1012,7 @@ __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned s
     const size_t own = BLK ? (size_t)(m >> 5) * (Q * 32) + (m & 31u) : 0;
     const V* __restrict__ Pown = P + own;
     BlkNbr bn;
-    if (BLK) bn.init<Q>(pn, m);
+    if (BLK && ODD) bn.init<Q>(pn, m);
 #pragma unroll
     for (int j = 0; j < Q; ++j) {
         if (BLK) {
@@ -1104,7 +1105,8 @@ __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned s
             if (RHEO == VLBM_POWERLAW) p.omega[nl] = eta;   // state update, lbm.cu:215-219
         }
     }
-    collide2<Q, OP>(g, mm, omega, fx2, fy2, fz2, SC ? p.inv_scale : 1.f);
+    // post-collision values as stored: deviations times the storage scale
+    collide2<Q, OP>(g, mm, omega, fx2, fy2, fz2, SC ? p.inv_scale : 1.f, SC ? p.scale : 1.f);
     if (!BULK && ((c0 | c1) & NODE_UNUSED)) {   // lbm.cu:23-24: not updated; rest equilibrium stays in the slots
         const bool u0 = c0 & NODE_UNUSED, u1 = c1 & NODE_UNUSED;
 #pragma unroll
@@ -1116,9 +1118,9 @@ __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned s
     if (!BULK && (slot0 >= 0 || slot1 >= 0)) {   // post-collision values of boundary nodes (lbm.cu:463-470)
         const size_t nbc = (size_t)p.nbc;
 #pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            if (slot0 >= 0) p.side_next[(size_t)i * nbc + slot0] = g[i].x;
-            if (slot1 >= 0) p.side_next[(size_t)i * nbc + slot1] = g[i].y;
+        for (int i = 0; i < Q; ++i) {   // the side store keeps deviations
+            if (slot0 >= 0) p.side_next[(size_t)i * nbc + slot0] = SC ? g[i].x * p.inv_scale : g[i].x;
+            if (slot1 >= 0) p.side_next[(size_t)i * nbc + slot1] = SC ? g[i].y * p.inv_scale : g[i].y;
         }
     }
     // one random stream per node pair, drawn in destination-plane order; each
@@ -1137,8 +1139,8 @@ __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned s
             if ((cz > 0 && seam_hi) || (cz < 0 && seam_lo)) in[j] = PV::swap(in[j]);
         }
     }
-    pn.launder();
-    if (BLK) bn.launder();
+    if (ODD) pn.launder();
+    if (ODD && BLK) bn.launder();
     V* __restrict__ Po = reinterpret_cast<V*>(p.pop);
     V* __restrict__ Powo = Po + own;
 #pragma unroll
