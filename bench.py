@@ -489,6 +489,7 @@ def main():
     ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 D3Q19/D3Q27 FP32/FP16 leg")
     ap.add_argument("--no-ibm", action="store_true", help="skip the 64-sphere IBM leg")
     ap.add_argument("--no-cavity", action="store_true", help="skip the 256^3 Power-Law lid-cavity leg")
+    ap.add_argument("--ibm-steps", type=int, default=50, help="timed steps of the 64-sphere IBM leg")
     ap.add_argument("--vel-set", type=int, default=19, choices=[19, 27])
     ap.add_argument("--size", type=int, nargs=3, default=[256, 128, 64], metavar=("NX", "NY", "NZ"))
     ap.add_argument("--e2e-steps", type=int, default=3000,
@@ -597,7 +598,7 @@ def main():
         cavity = cavity_leg(vlbm, torch, local)
     ibm_run = None
     if rank == 0 and world == 1 and not args.no_ibm:
-        ibm_run = ibm_leg(vlbm, torch, local)
+        ibm_run = ibm_leg(vlbm, torch, local, steps=args.ibm_steps)
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_leg(vlbm, args.serving_requests, args.serving_step_scale, args.serving_rate,
