@@ -213,7 +213,8 @@ def cube_leg(vlbm, torch, device, steps=200, warmup=10, n=256):
             mlups = nodes * steps / (ms / 1e3) / 1e6
             gbs = bpn * mlups * 1e6 / 1e9
             out[f"d3q{q}_{name}"] = {"mlups": mlups, "achieved_gbs": gbs, "frac": gbs / peak,
-                                     "bytes_per_node": bpn, "variant": sim.info().last_kernel_variant}
+                                     "bytes_per_node": bpn, "variant": sim.info().last_kernel_variant,
+                                     "layout": ("natural", "zpair", "zpair_blocked")[sim.info().layout]}
             sim.close()
         out[f"d3q{q}_f16_over_f32"] = out[f"d3q{q}_f16"]["mlups"] / out[f"d3q{q}_f32"]["mlups"]
     return out
@@ -375,9 +376,10 @@ def serving_leg(vlbm, n_req=512, step_scale=0.25, rate=20.0, budget_gb=64.0, max
     through the public API (create, node map, spheres, step, read ux,
     destroy), each in its own best layout (LAYOUT_AUTO: z-paired FP16 where NZ
     is even); it runs `plain_repeats` times and the fastest run is compared.
-    The batched arm submits each request to a vlbm_server when it arrives,
-    pumps it and fetches each result when it completes (the server keeps the
-    last 256 results).  The two arms round half-precision stores with
+    The batched arm submits each request to a vlbm_server when it arrives (the
+    server runs every lattice in the natural layout), pumps it and fetches each
+    result when it completes (the server keeps the last 256 results).  Where
+    the two arms' layouts differ they round half-precision stores with
     different random streams, so their ux fields are compared by relative L2.
     Latency = time the result is handed back - arrival time; solves/s =
     requests / (last completion - first arrival).
@@ -388,11 +390,6 @@ def serving_leg(vlbm, n_req=512, step_scale=0.25, rate=20.0, budget_gb=64.0, max
     arrivals -= arrivals[0]
     ibm = vlbm.IbmConfig.default(**SERVING_IBM)
     lu = float(sum(r["nodes"] * r["steps"] for r in reqs))
-
-    def natural(cfg):
-        c = vlbm.Config.from_buffer_copy(cfg)
-        c.layout = vlbm.LAYOUT_NATURAL   # the server's layout
-        return c
 
     def plain_run():
         t0 = time.perf_counter()
@@ -423,7 +420,7 @@ def serving_leg(vlbm, n_req=512, step_scale=0.25, rate=20.0, budget_gb=64.0, max
         now = time.perf_counter() - t0
         while nxt < n_req and arrivals[nxt] <= now:
             r = reqs[nxt]
-            srv.submit(natural(r["cfg"]), vlbm.BUILDER_DUCT_YZ, r["steps"], r["tag"], r["spheres"], ibm)
+            srv.submit(r["cfg"], vlbm.BUILDER_DUCT_YZ, r["steps"], r["tag"], r["spheres"], ibm)   # server: natural
             arrive_at[r["tag"]] = arrivals[nxt]
             nxt += 1
         st = srv.stats()
@@ -559,7 +556,11 @@ def main():
     bytes_per_node = info.bytes_per_node_step
     achieved_gbs = bytes_per_node * N / (ms / 1e3 / args.steps) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = committed_traffic(args.storage, args.layout)
+    # the layout the autotuner kept (one launch per step in the natural layout;
+    # the pair step adds the launch over the tiles that hold the channel's walls)
+    chosen_layout = ("natural", "zpair", "zpair")[info.layout]
+    launches_per_step = 1 if info.layout == 0 else 2
+    traffic = committed_traffic(args.storage, chosen_layout)
 
     # end to end through the public API with host buffers: upload the state from
     # pinned host memory, advance, read the macroscopics back
@@ -620,8 +621,9 @@ def main():
             "e2e": {"value": e2e_mlups, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "note": "vlbm_set_populations from pinned host + K steps + vlbm_get_macroscopics to host, "
                             "wall clock, bytes amortised over K steps"},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * launches_per_step,
             "kernel_variant": variant,
+            "layout": ("natural", "zpair", "zpair_blocked")[info.layout],
             "clocks": clk,
             "lattice_256": cube,
             "powerlaw_cavity_256": cavity,

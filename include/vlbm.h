@@ -241,7 +241,9 @@ typedef struct vlbm_info {
     double bytes_per_node_step;  /* algorithmic bytes: 2*Q*storage_bytes          */
     int32_t n_particles, n_lagrangian_nodes;
     int32_t last_kernel_variant; /* autotuned launch variant of the fused kernel  */
-    int32_t reserved[7];
+    int32_t layout;              /* population layout in use: 0 natural, 1 z-paired,
+                                    2 z-paired in blocks of 32 pair-nodes         */
+    int32_t reserved[6];
 } vlbm_info;
 vlbm_status vlbm_get_info(vlbm_sim* sim, vlbm_info* info);
 
@@ -485,8 +487,24 @@ vlbm_status vlbm_server_destroy(vlbm_server* srv);
 /* --------------------------------------------------------------- misc --- */
 const char* vlbm_last_error(void);     /* thread-local message of the last failure */
 int vlbm_abi_version(void);
-/* Autotuner: time the fused kernel variants for this simulation and keep the best. */
+/* Autotuner (no counterpart in the reference, whose launch shape is fixed at
+ * compile time, var.h:124): times the fused step on a copy of the state for
+ * each launch shape (64 / 128 / 256 threads per block: the variant returned)
+ * and, when the configuration leaves the layout to the library
+ * (VLBM_LAYOUT_AUTO) and NZ is even, for each tile a thread advances (one
+ * node in the natural layout, the node pair (z, z + NZ/2) in the z-paired one);
+ * the state is restored, in the fastest layout, and the fastest shape is
+ * kept.  vlbm_info.layout reports the layout in use; checkpoints record it, so
+ * an image saved before an autotune that changed the layout loads only into
+ * a simulation in the same layout. */
 vlbm_status vlbm_autotune(vlbm_sim* sim, int32_t* chosen_variant);
+/* Move the state into another population layout (VLBM_LAYOUT_NATURAL, or
+ * VLBM_LAYOUT_ZPAIR for an even NZ, in blocks of 32 pair-nodes where NX is a
+ * multiple of 32): the stored values are copied, so the state is unchanged,
+ * and the layout is kept by later autotuning.  No counterpart in the reference,
+ * which has one layout (idxPop, globalFunctions.h:111-147).  Allocates a
+ * temporary copy of the population array. */
+vlbm_status vlbm_set_layout(vlbm_sim* sim, int32_t layout);
 /* Force a kernel launch variant (0 = autotuned default). */
 vlbm_status vlbm_set_variant(vlbm_sim* sim, int32_t variant);
 

@@ -151,16 +151,79 @@ def test_divergence_is_reported_not_hidden(vlbm):
 
 
 def test_autotune_preserves_state(vlbm):
-    cfg = vlbm.Config.default(nx=32, ny=16, nz=8, fx=1e-4, tau=0.8)
+    """With the layout fixed, the autotuner changes only the launch shape, and
+    the launch shapes give the same bits."""
+    cfg = vlbm.Config.default(nx=32, ny=16, nz=8, fx=1e-4, tau=0.8, layout=vlbm.LAYOUT_NATURAL)
     a = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
     b = vlbm.Simulation(cfg, builder=vlbm.BUILDER_PLATES_Y)
     a.step(3)
     b.step(3)
     v = b.autotune()
     assert v in (1, 2, 3)
+    assert b.info().layout == 0
     a.step(10)
     b.step(10)
     np.testing.assert_array_equal(a.populations(), b.populations())
+
+
+LAYOUT_CASES = [(19, 0, 32), (19, 1, 32), (19, 2, 20), (27, 0, 32), (27, 1, 20)]
+
+
+@pytest.mark.parametrize("q,storage,nx", LAYOUT_CASES)
+def test_set_layout_moves_the_state_bit_for_bit(vlbm, oracle, q, storage, nx):
+    """vlbm_set_layout between the natural and the z-paired layout (blocked for
+    nx = 32, plain for nx = 20), at both AA parities: the populations read back
+    are unchanged bit for bit, and the run continues as the oracle's."""
+    ny, nz = 10, 6
+    cfg = vlbm.Config.default(nx=nx, ny=ny, nz=nz, vel_set=q, storage=storage, rheology=1, eta_p=0.1,
+                              yield_stress=2e-6, fx=2e-4)
+    m = vlbm.build_node_map(vlbm.BUILDER_PLATES_Y, nx, ny, nz)
+    sim = vlbm.Simulation(cfg, node_map=m)
+    first = sim.info().layout
+    steps = 0
+    for lay, k in ((vlbm.LAYOUT_NATURAL, 7), (vlbm.LAYOUT_ZPAIR, 6), (vlbm.LAYOUT_NATURAL, 5), (vlbm.LAYOUT_ZPAIR, 4)):
+        sim.step(k)
+        steps += k
+        before = sim.populations()
+        sim.set_layout(lay)
+        assert sim.info().layout == (0 if lay == vlbm.LAYOUT_NATURAL else (2 if nx % 32 == 0 else 1)), first
+        np.testing.assert_array_equal(sim.populations(), before)
+    sim.step(11)
+    steps += 11
+    sim.sync()
+    o = oracle.Oracle(cfg, m)
+    o.step(steps)
+    ug = sim.macroscopics()["ux"].astype(np.float64)
+    uo = o.macroscopics()["ux"]
+    tol = {0: 1e-4, 1: 5e-3, 2: 5e-2}[storage]
+    assert rel_l2(ug, uo) < tol, rel_l2(ug, uo)
+    if storage == 0:
+        assert np.max(np.abs(sim.populations().astype(np.float64) - o.populations())) <= POP_TOL
+
+
+@pytest.mark.parametrize("q,storage", [(19, 0), (19, 1), (27, 0)])
+def test_autotune_layout_choice_keeps_the_state(vlbm, oracle, q, storage):
+    """With LAYOUT_AUTO the autotuner also times the other layout; whichever it
+    keeps, the state it returns is the one it was given and the run goes on as
+    the oracle's."""
+    nx, ny, nz = 64, 12, 8
+    cfg = vlbm.Config.default(nx=nx, ny=ny, nz=nz, vel_set=q, storage=storage, rheology=1, eta_p=0.1,
+                              yield_stress=2e-6, fx=2e-4)
+    m = vlbm.build_node_map(vlbm.BUILDER_PLATES_Y, nx, ny, nz)
+    sim = vlbm.Simulation(cfg, node_map=m)
+    sim.step(9)
+    before = sim.populations()
+    assert sim.autotune() in (1, 2, 3)
+    assert sim.info().layout in (0, 2)
+    np.testing.assert_array_equal(sim.populations(), before)
+    assert sim.info().step == 9
+    sim.step(21)
+    sim.sync()
+    o = oracle.Oracle(cfg, m)
+    o.step(30)
+    ug = sim.macroscopics()["ux"].astype(np.float64)
+    tol = {0: 1e-4, 1: 5e-3}[storage]
+    assert rel_l2(ug, o.macroscopics()["ux"]) < tol
 
 
 @pytest.mark.parametrize("variant", [1, 2, 3])

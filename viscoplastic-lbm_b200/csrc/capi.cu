@@ -204,6 +204,12 @@ __global__ void k_tile_flags(const uint8_t* cls, long long M, uint8_t* flag, int
     if (sp) list[atomicAdd(count, 1)] = (int32_t)t;
 }
 
+// Z-paired pairs in blocks of 32: NX a multiple of 32 and the blocked
+// offsets within 32 bits.
+static int blocked_pairs_ok(const vlbm_sim* s) {
+    return (s->cfg.nx % 32 == 0 && (s->N / 2) * s->Q < (1ll << 31)) ? 1 : 0;
+}
+
 static vlbm_status build_pair_tiles(vlbm_sim* s) {
     if (s->pairH <= 0) return VLBM_OK;
     const long long M = s->N / 2, T = (M + 31) / 32;
@@ -399,7 +405,7 @@ vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator,
         // together) where NX is a multiple of 32 and the blocked offsets fit
         // 32 bits: the pair step then addresses every population from one
         // pointer (D3Q19 FP16 256^3: 57.6k against 53.3k MLUPS)
-        s->pairBlk = (s->pairH > 0 && cfg->nx % 32 == 0 && (s->N / 2) * s->Q < (1ll << 31)) ? 1 : 0;
+        s->pairBlk = s->pairH > 0 ? blocked_pairs_ok(s) : 0;
     }
     e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete s; return cuda_status(e, "cudaStreamCreate"); }
@@ -595,6 +601,7 @@ vlbm_status vlbm_get_info(vlbm_sim* s, vlbm_info* info) {
     info->device_bytes = (int64_t)s->device_bytes;
     info->bytes_per_node_step = 2.0 * s->Q * s->store_bytes;
     info->last_kernel_variant = s->variant;
+    info->layout = s->pairH == 0 ? 0 : (s->pairBlk ? 2 : 1);
     ibm_counts(s, &info->n_particles, &info->n_lagrangian_nodes);
     return VLBM_OK;
 }
@@ -608,8 +615,51 @@ vlbm_status vlbm_set_variant(vlbm_sim* s, int32_t variant) {
     return VLBM_OK;
 }
 
-// Project-written autotuner: times each launch variant over whole even/odd step
-// pairs on a copy of the state, then restores the state and keeps the fastest.
+// Switch the population layout of a simulation whose array already holds the
+// new layout's values: pairH / pairBlk and, for the pair step, its tile lists.
+static vlbm_status use_layout(vlbm_sim* s, int H, int blk) {
+    s->pairH = H;
+    s->pairBlk = H > 0 ? blk : 0;
+    return build_pair_tiles(s);
+}
+
+vlbm_status vlbm_set_layout(vlbm_sim* s, int32_t layout) {
+    CHECK_SIM(s);
+    if (layout != VLBM_LAYOUT_NATURAL && layout != VLBM_LAYOUT_ZPAIR) {
+        set_last_error("vlbm_set_layout takes VLBM_LAYOUT_NATURAL or VLBM_LAYOUT_ZPAIR");
+        return VLBM_ERR_INVALID;
+    }
+    if (layout == VLBM_LAYOUT_ZPAIR && s->cfg.nz % 2 != 0) {
+        set_last_error("the z-paired layout needs an even nz");
+        return VLBM_ERR_INVALID;
+    }
+    const int H = layout == VLBM_LAYOUT_ZPAIR ? s->cfg.nz / 2 : 0;
+    const int blk = H > 0 ? blocked_pairs_ok(s) : 0;
+    s->cfg.layout = layout;
+    if (H == s->pairH && blk == s->pairBlk) return VLBM_OK;
+    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    const size_t popb = (size_t)s->Q * s->N * s->store_bytes;
+    void* copy = nullptr;
+    VLBM_CUDA(cudaMalloc(&copy, popb));
+    cudaError_t e = cudaMemcpyAsync(copy, s->pop, popb, cudaMemcpyDeviceToDevice, s->stream);
+    if (e == cudaSuccess)
+        e = launch_relayout(s->Q, s->cfg.storage, copy, s->pop, s->cfg.nx, s->cfg.ny, s->N, s->pairH, s->pairBlk, H,
+                            blk, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(copy);
+    if (e != cudaSuccess) return cuda_status(e, "relayout");
+    return use_layout(s, H, blk);
+}
+
+// Project-written autotuner: per velocity set, storage and lattice size it
+// times the launch shape (64, 128 or 256 threads per block) and, when the
+// configuration leaves the layout to the library (VLBM_LAYOUT_AUTO, even NZ),
+// the tile a thread advances: one node (natural layout) or the node pair (z,
+// z + NZ/2) of the z-paired layout (in blocks of 32 pair-nodes where NX
+// allows).  Each candidate runs whole even/odd step pairs on a copy of the
+// state (moved into the candidate's layout by k_relayout, which copies the
+// stored values); the state is then restored in the fastest layout and the
+// fastest shape is kept.
 vlbm_status vlbm_autotune(vlbm_sim* s, int32_t* chosen) {
     CHECK_SIM(s);
     if (!s->geometry) { set_last_error("set the node map before autotuning"); return VLBM_ERR_STATE; }
@@ -626,30 +676,56 @@ vlbm_status vlbm_autotune(vlbm_sim* s, int32_t* chosen) {
     if (bo) VLBM_CUDA(cudaMemcpy(bo, s->omega, (size_t)s->N * sizeof(float), cudaMemcpyDeviceToDevice));
     const int parity = s->parity, side_cur = s->side_cur, apply = s->apply_bc;
     const long long step = s->step;
+    const int H0 = s->pairH, B0 = s->pairBlk;
+    struct Layout { int H, blk; };
+    std::vector<Layout> layouts{{H0, B0}};
+    if (s->cfg.layout == VLBM_LAYOUT_AUTO && s->cfg.nz % 2 == 0) {
+        if (H0 > 0) layouts.push_back({0, 0});
+        else layouts.push_back({s->cfg.nz / 2, blocked_pairs_ok(s)});
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     float best = 1e30f;
     int bestv = 3;
+    Layout bestl = layouts[0];
     const int reps = s->N > (1 << 22) ? 4 : 20;
-    for (int v = 1; v <= 3; ++v) {
-        vlbm_set_variant(s, v);
-        for (int w = 0; w < 2; ++w) fluid_step(s);
-        cudaEventRecord(e0, s->stream);
-        for (int r = 0; r < reps; ++r) fluid_step(s);
-        cudaEventRecord(e1, s->stream);
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) { best = ms; bestv = v; }
+    vlbm_status st = VLBM_OK;
+    for (const Layout& l : layouts) {
+        if (l.H != s->pairH || l.blk != s->pairBlk) {
+            cudaError_t e = launch_relayout(s->Q, s->cfg.storage, bp, s->pop, s->cfg.nx, s->cfg.ny, s->N, H0, B0, l.H,
+                                            l.blk, s->stream);
+            if (e != cudaSuccess) { st = cuda_status(e, "relayout"); break; }
+            if ((st = use_layout(s, l.H, l.blk)) != VLBM_OK) break;
+        }
+        for (int v = 1; v <= 3; ++v) {
+            vlbm_set_variant(s, v);
+            for (int w = 0; w < 2; ++w) fluid_step(s);
+            cudaEventRecord(e0, s->stream);
+            for (int r = 0; r < reps; ++r) fluid_step(s);
+            cudaEventRecord(e1, s->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; bestv = v; bestl = l; }
+        }
     }
     cudaEventDestroy(e0); cudaEventDestroy(e1);
-    VLBM_CUDA(cudaMemcpy(s->pop, bp, popb, cudaMemcpyDeviceToDevice));
+    if (st == VLBM_OK) {   // the saved state, in the fastest layout
+        cudaError_t e = (bestl.H == H0 && bestl.blk == B0)
+                            ? cudaMemcpy(s->pop, bp, popb, cudaMemcpyDeviceToDevice)
+                            : launch_relayout(s->Q, s->cfg.storage, bp, s->pop, s->cfg.nx, s->cfg.ny, s->N, H0, B0,
+                                              bestl.H, bestl.blk, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) st = cuda_status(e, "autotune restore");
+        else if (bestl.H != s->pairH || bestl.blk != s->pairBlk) st = use_layout(s, bestl.H, bestl.blk);
+    }
     if (sideb) { VLBM_CUDA(cudaMemcpy(s->side[0], bs0, sideb, cudaMemcpyDeviceToDevice));
                  VLBM_CUDA(cudaMemcpy(s->side[1], bs1, sideb, cudaMemcpyDeviceToDevice)); }
     if (bo) VLBM_CUDA(cudaMemcpy(s->omega, bo, (size_t)s->N * sizeof(float), cudaMemcpyDeviceToDevice));
     cudaFree(bp); cudaFree(bs0); cudaFree(bs1); cudaFree(bo);
     s->parity = parity; s->side_cur = side_cur; s->apply_bc = apply; s->step = step;
     sync_step_ctr(s, s->stream);
+    if (st != VLBM_OK) return st;
     vlbm_set_variant(s, bestv);
     if (chosen) *chosen = bestv;
     VLBM_CUDA(cudaGetLastError());

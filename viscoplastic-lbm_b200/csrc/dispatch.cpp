@@ -45,6 +45,13 @@ cudaError_t launch_batched(int Q, int st, const BatchLaunch* L, const BatchState
 #undef C_
 }
 
+cudaError_t launch_relayout(int Q, int st, const void* src, void* dst, int nx, int ny, long long N, int sH, int sB,
+                            int dH, int dB, cudaStream_t s) {
+#define C_(QQ, SS) launch_relayout_st<QQ, SS>(src, dst, nx, ny, N, sH, sB, dH, dB, s)
+    VLBM_SELECT(C_)
+#undef C_
+}
+
 #define VLBM_SELECT_INT(CALL)                                                      \
     if (Q == 19) {                                                                 \
         if (st == VLBM_STORE_F32) return CALL(19, VLBM_STORE_F32);                 \

@@ -28,6 +28,10 @@ template <int Q, int ST>
 cudaError_t launch_batched_st(const BatchLaunch* L, const BatchState* state, const BatchBlock* table, int ntiles,
                               int grid, bool odd, int op, int rheo, cudaStream_t s);
 
+template <int Q, int ST>
+cudaError_t launch_relayout_st(const void* src, void* dst, int nx, int ny, long long N, int sH, int sB, int dH,
+                               int dB, cudaStream_t s);
+
 // Run-time selection over (Q, storage).
 cudaError_t launch_step(int Q, int st, const StepParams& p, int op, int rheo, bool odd, LaunchShape ls,
                         cudaStream_t s);
@@ -40,6 +44,10 @@ cudaError_t launch_set_pops(int Q, int st, const StepParams& p, const float* in,
 // blocks of 256 threads.
 cudaError_t launch_batched(int Q, int st, const BatchLaunch* L, const BatchState* state, const BatchBlock* table,
                            int ntiles, int grid, bool odd, int op, int rheo, cudaStream_t s);
+// Copy a population array from layout (sH, sB) into layout (dH, dB) (pairH and
+// pairBlk of each; sH = 0 is the natural layout).
+cudaError_t launch_relayout(int Q, int st, const void* src, void* dst, int nx, int ny, long long N, int sH, int sB,
+                            int dH, int dB, cudaStream_t s);
 // Resident 256-thread blocks per SM of the batched kernel of a group.
 int batched_blocks_per_sm(int Q, int st, int op, int rheo);
 template <int Q, int ST>

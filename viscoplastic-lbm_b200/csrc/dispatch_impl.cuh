@@ -172,6 +172,13 @@ int batched_occupancy_st(int op, int rheo) {
     return occ_rh<Q, VLBM_OP_REGULARIZED, ST>(rheo);
 }
 
+template <int Q, int ST>
+cudaError_t launch_relayout_st(const void* src, void* dst, int nx, int ny, long long N, int sH, int sB, int dH,
+                               int dB, cudaStream_t s) {
+    k_relayout<Q, ST><<<grid_for(N, 256), 256, 0, s>>>(src, dst, nx, ny, N, sH, sB, dH, dB);
+    return cudaGetLastError();
+}
+
 #define VLBM_INSTANTIATE(QQ, SS)                                                                              \
     template cudaError_t launch_step_st<QQ, SS>(const StepParams&, int, int, bool, LaunchShape, cudaStream_t); \
     template cudaError_t launch_macro_st<QQ, SS>(const MacroParams&, int, bool, cudaStream_t);                 \
@@ -180,6 +187,8 @@ int batched_occupancy_st(int op, int rheo) {
                                                     cudaStream_t);                                              \
     template cudaError_t launch_batched_st<QQ, SS>(const BatchLaunch*, const BatchState*, const BatchBlock*, int,  \
                                                    int, bool, int, int, cudaStream_t);                          \
-    template int batched_occupancy_st<QQ, SS>(int, int);
+    template int batched_occupancy_st<QQ, SS>(int, int);                                                       \
+    template cudaError_t launch_relayout_st<QQ, SS>(const void*, void*, int, int, long long, int, int, int, int,  \
+                                                    cudaStream_t);
 
 }  // namespace vlbm

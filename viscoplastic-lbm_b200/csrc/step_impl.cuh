@@ -380,13 +380,38 @@ __device__ __forceinline__ void apply_bc(float (&f)[Q], const StepParams& p, int
 // (lane 0 / 1 of pair-node m).  Plain pairs: Q planes of N/2 pairs.  Blocked
 // pairs (NX % 32 == 0): blocks of 32 consecutive pair-nodes, each holding
 // all Q populations of its nodes, [m / 32][Q][32][2].
+// layout_elem: the same for any layout, H = 0 being the natural [Q][N] one.
+template <int Q>
+__device__ __forceinline__ size_t layout_elem(int i, int x, int y, int z, int nx, int ny, long long N, int H,
+                                              int blk) {
+    if (H == 0) return (size_t)i * (size_t)N + (((size_t)z * ny + y) * nx + x);
+    const int lane = z >= H ? 1 : 0;
+    const int zp = z - lane * H;
+    const size_t m = ((size_t)zp * ny + y) * nx + x;
+    if (blk) return (((((m >> 5) * Q + (size_t)i) << 5) | (m & 31u)) << 1) | (size_t)lane;
+    return (size_t)i * (size_t)N + ((m << 1) | (size_t)lane);
+}
 template <int Q>
 __device__ __forceinline__ size_t pair_elem(const StepParams& p, int i, int x, int y, int z) {
-    const int lane = z >= p.pairH ? 1 : 0;
-    const int zp = z - lane * p.pairH;
-    const size_t m = ((size_t)zp * p.ny + y) * p.nx + x;
-    if (p.pairBlk) return (((((m >> 5) * Q + (size_t)i) << 5) | (m & 31u)) << 1) | (size_t)lane;
-    return (size_t)i * (size_t)p.N + ((m << 1) | (size_t)lane);
+    return layout_elem<Q>(i, x, y, z, p.nx, p.ny, p.N, p.pairH, p.pairBlk);
+}
+
+// The population array moved from one layout (sH, sB) to another (dH, dB),
+// value for value: the stored bits are copied, so the state is unchanged.
+template <int Q, int ST>
+__global__ void __launch_bounds__(256) k_relayout(const void* src, void* dst, int nx, int ny, long long N, int sH,
+                                                  int sB, int dH, int dB) {
+    using T = typename Store<ST>::T;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int x = (int)(n % nx);
+    const long long t = n / nx;
+    const int y = (int)(t % ny), z = (int)(t / ny);
+    const T* S = static_cast<const T*>(src);
+    T* D = static_cast<T*>(dst);
+#pragma unroll
+    for (int i = 0; i < Q; ++i)
+        D[layout_elem<Q>(i, x, y, z, nx, ny, N, dH, dB)] = S[layout_elem<Q>(i, x, y, z, nx, ny, N, sH, sB)];
 }
 __device__ __forceinline__ int wrap1(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 

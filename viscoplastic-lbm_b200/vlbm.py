@@ -144,7 +144,7 @@ class Info(C.Structure):
         ("storage_bytes", C.c_int32), ("step", C.c_int64), ("n_bc_nodes", C.c_int64),
         ("device_bytes", C.c_int64), ("bytes_per_node_step", C.c_double),
         ("n_particles", C.c_int32), ("n_lagrangian_nodes", C.c_int32),
-        ("last_kernel_variant", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("last_kernel_variant", C.c_int32), ("layout", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -234,6 +234,7 @@ _SIGS = {
     "vlbm_server_destroy": [_P],
     "vlbm_autotune": [_P, C.POINTER(C.c_int32)],
     "vlbm_set_variant": [_P, C.c_int32],
+    "vlbm_set_layout": [_P, C.c_int32],
 }
 EXPORTED = sorted(list(_SIGS) + ["vlbm_last_error", "vlbm_abi_version"])
 
@@ -444,6 +445,9 @@ class Simulation:
 
     def set_variant(self, v):
         _check(_lib.vlbm_set_variant(self._h, v), "vlbm_set_variant")
+
+    def set_layout(self, layout):
+        _check(_lib.vlbm_set_layout(self._h, layout), "vlbm_set_layout")
 
 
 class Server:
