@@ -96,8 +96,7 @@ StepParams make_params(vlbm_sim* s) {
     p.nbc = s->nbc;
     p.pairH = s->pairH;
     p.pairBlk = s->pairBlk;
-    p.tile_special = s->tile_special;
-    p.special_tiles = s->special_tiles;
+    p.special_pairs = s->special_pairs;
     p.n_special = s->n_special;
     p.apply_bc = s->apply_bc;
     p.ctr = s->step_ctr;
@@ -187,21 +186,14 @@ static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
     return VLBM_OK;
 }
 
-// Pair-step tiles: 32 consecutive pair-nodes m (one warp; nodes m and m + M,
-// M = N/2).  A tile is special when one of its 64 nodes is a boundary or
-// unused node; the list of special tiles is filled in any order (every node
-// pair reads and writes only its own slots, so the order of the tiles does
-// not change the result).
-__global__ void k_tile_flags(const uint8_t* cls, long long M, uint8_t* flag, int32_t* list, int* count) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (M + 31) / 32) return;
-    bool sp = false;
-    for (int k = 0; k < 32 && !sp; ++k) {
-        const long long m = t * 32 + k;
-        if (m < M) sp = ((cls[m] | cls[m + M]) & (NODE_BC | NODE_UNUSED)) != 0;
-    }
-    flag[t] = sp ? 1 : 0;
-    if (sp) list[atomicAdd(count, 1)] = (int32_t)t;
+// Pair-nodes m (nodes m and m + M, M = N/2) with a boundary or unused node:
+// the pair step's bulk kernel leaves them to k_step2, which runs this list.
+// The list is filled in any order (every node pair reads and writes only its
+// own slots, so the order does not change the result).
+__global__ void k_special_pairs(const uint8_t* cls, long long M, int32_t* list, int* count) {
+    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    if ((cls[m] | cls[m + M]) & (NODE_BC | NODE_UNUSED)) list[atomicAdd(count, 1)] = (int32_t)m;
 }
 
 // Z-paired pairs in blocks of 32: NX a multiple of 32 and the blocked
@@ -212,19 +204,16 @@ static int blocked_pairs_ok(const vlbm_sim* s) {
 
 static vlbm_status build_pair_tiles(vlbm_sim* s) {
     if (s->pairH <= 0) return VLBM_OK;
-    const long long M = s->N / 2, T = (M + 31) / 32;
+    const long long M = s->N / 2;
     vlbm_status st;
     void* p;
-    if (!s->tile_special) {
-        if ((st = alloc_dev(s, &p, (size_t)T)) != VLBM_OK) return st;
-        s->tile_special = static_cast<uint8_t*>(p);
-        if ((st = alloc_dev(s, &p, (size_t)T * sizeof(int32_t) + sizeof(int32_t))) != VLBM_OK) return st;
-        s->special_tiles = static_cast<int32_t*>(p);
+    if (!s->special_pairs) {
+        if ((st = alloc_dev(s, &p, (size_t)M * sizeof(int32_t) + sizeof(int32_t))) != VLBM_OK) return st;
+        s->special_pairs = static_cast<int32_t*>(p);
     }
-    int* count = s->special_tiles + T;   // the counter sits behind the list
+    int* count = s->special_pairs + M;   // the counter sits behind the list
     VLBM_CUDA(cudaMemsetAsync(count, 0, sizeof(int), s->stream));
-    k_tile_flags<<<(unsigned)((T + 255) / 256), 256, 0, s->stream>>>(s->cls, M, s->tile_special, s->special_tiles,
-                                                                    count);
+    k_special_pairs<<<(unsigned)((M + 255) / 256), 256, 0, s->stream>>>(s->cls, M, s->special_pairs, count);
     VLBM_CUDA(cudaGetLastError());
     int n = 0;
     VLBM_CUDA(cudaMemcpyAsync(&n, count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
@@ -321,7 +310,7 @@ vlbm_sim::~vlbm_sim() {
     if (ibm) { ibm_destroy(ibm, allocator); ibm = nullptr; }
     for (void* p : {(void*)pop, (void*)cls, (void*)bc_slot, (void*)bc, (void*)bc_node, (void*)side[0], (void*)side[1],
                     (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch, (void*)bc_q,
-                    (void*)treat_prev, (void*)treat_red, (void*)tile_special, (void*)special_tiles})
+                    (void*)treat_prev, (void*)treat_red, (void*)special_pairs})
         free_with(allocator, p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }

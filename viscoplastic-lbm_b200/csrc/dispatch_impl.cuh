@@ -27,9 +27,9 @@ cudaError_t launch_overlapped(void (*kernel)(Args...), unsigned grid, unsigned b
 
 template <int Q, int OP, int RHEO, int ST>
 cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s) {
-    if (p.pairH > 0) {  // z-paired layout: one thread per node pair; bulk tiles, then the listed ones
+    if (p.pairH > 0) {  // z-paired layout: one thread per node pair; bulk pairs, then the listed ones
         const unsigned g = grid_for(p.N / 2, ls.block);
-        const unsigned gs = grid_for((long long)p.n_special * 32, 256);
+        const unsigned gs = grid_for(p.n_special, 256);
         cudaError_t e;
         if (p.pairBlk) {
             if (odd) k_step2_bulk<Q, OP, RHEO, ST, true, true><<<g, ls.block, 0, s>>>(p);

@@ -69,10 +69,9 @@ struct StepParams {
     int nbc;
     int pairH;                  // z-paired population layout: NZ/2, or 0 for the natural layout
     int pairBlk;                // z-paired layout stored in blocks of 32 pair-nodes (NX % 32 == 0)
-    // pair step tiles (32 consecutive pair-nodes, one warp): 1 where a tile holds
-    // a boundary or unused node, and the list of those tiles
-    const uint8_t* tile_special;
-    const int32_t* special_tiles;
+    // pair step: the pair-nodes that hold a boundary or unused node (run by
+    // k_step2; the bulk kernel leaves them)
+    const int32_t* special_pairs;
     int n_special;
     int apply_bc;               // 0 on the first step after (re)initialisation
     float omega_newt;           // 1/tau

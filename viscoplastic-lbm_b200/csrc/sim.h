@@ -48,8 +48,7 @@ struct vlbm_sim {
     int nbc = 0;
     int pairH = 0;                   // z-paired layout (NZ/2) or 0
     int pairBlk = 0;                 // z-paired pairs stored in blocks of 32 (pair_elem)
-    uint8_t* tile_special = nullptr; // [M/32] pair-step tiles with a boundary or unused node
-    int32_t* special_tiles = nullptr;  // indices of those tiles (n_special)
+    int32_t* special_pairs = nullptr; // pair-nodes with a boundary or unused node (n_special), then a counter
     int n_special = 0;
     float* omega = nullptr;          // [N] Power-Law state
     float* fibm = nullptr;           // [3][N] IBM force (allocated with spheres)

@@ -1007,12 +1007,12 @@ struct BlkNbr {
 // compile-time offset (32 j) from one pointer, and a neighbour's is that plus
 // one of six axis offsets formed once per thread (BlkNbr).
 //
-// BULK: the warp's tile (m / 32) holds no boundary and no unused node, so the
-// boundary rules, the side store and the unused-node path are compiled out
-// (the bulk kernel then fits 64 registers: 4 resident blocks of 256 instead
-// of 3).  A BULK warp that finds such a node in its class bytes, loaded with
-// the populations, returns before it writes anything; k_step2 runs those
-// tiles from their list.
+// BULK: the pair holds no boundary and no unused node, so the boundary
+// rules, the side store and the unused-node path are compiled out (the bulk
+// kernel then fits 64 registers for D3Q19: 4 resident blocks of 256 instead
+// of 3).  A BULK thread whose class bytes, loaded with the populations, show
+// such a node returns before it writes anything; k_step2 runs those pairs
+// from their list.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK, bool BULK>
 __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned seed, const unsigned m) {
     using PV = Pair<ST>;
@@ -1072,11 +1072,7 @@ __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned s
 #pragma unroll
     for (int i = 0; i < Q; ++i) g[i] = PV::raw2(in[i]);
     const uint8_t c0 = p.cls[n0], c1 = p.cls[n1];
-    if (BULK) {   // every lane of the tile that exists (m < M) votes; m % 32 is the lane
-        const unsigned valid = min(32u, (unsigned)(p.N >> 1) - (m & ~31u));
-        const unsigned tile = valid == 32u ? 0xffffffffu : ((1u << valid) - 1u);
-        if (__any_sync(tile, (c0 | c1) & (NODE_BC | NODE_UNUSED))) return;
-    }
+    if (BULK && ((c0 | c1) & (NODE_BC | NODE_UNUSED))) return;   // k_step2's pair
     int slot0 = -1, slot1 = -1;
     if (!BULK && ((c0 | c1) & NODE_BC)) {   // boundary rules per lane, on scalars
 #pragma unroll
@@ -1181,21 +1177,25 @@ __device__ __forceinline__ void step2_pair(const StepParams& p, const unsigned s
     }
 }
 
-// Resident 256-thread blocks per SM asked of the bulk pair kernel (-Xptxas -v):
-// regularized D3Q19 fits 64 registers for 4 blocks (0 bytes of spill in the
-// even step, 12-36 in the odd one); BGK keeps every population live across
-// the collision and spills 40-180 bytes there, so it takes 3; D3Q27 spills
-// 30-250 bytes at 80 registers (3 blocks) and takes 2.
-template <int Q, int OP> constexpr int step2_bulk_blocks() {
-    return Q == 19 ? (OP == VLBM_OP_REGULARIZED ? 4 : 3) : 2;
+// Resident 256-thread blocks per SM asked of the bulk pair kernel (-Xptxas -v
+// and timings at 256^3): regularized D3Q19 fits 64 registers for 4 blocks (0
+// bytes of spill in the even step, 12-36 in the odd one); BGK keeps every
+// population live across the collision and spills 40-180 bytes there, so it
+// takes 3.  D3Q27 at 80 registers (3 blocks) spills 30-56 bytes: worth it for
+// half storage, which is issue-bound (regularized FP16 46.5k against 42.1k
+// MLUPS at 2 blocks), not for FP32, which streams at the copy bandwidth
+// either way (30.0k against 30.5k), nor for BGK (64-250 bytes of spill).
+template <int Q, int OP, int ST> constexpr int step2_bulk_blocks() {
+    if (Q == 19) return OP == VLBM_OP_REGULARIZED ? 4 : 3;
+    return (OP == VLBM_OP_REGULARIZED && ST != VLBM_STORE_F32) ? 3 : 2;
 }
 
-// The pair step over every tile; tiles with a boundary or unused node return
+// The pair step over every pair; pairs with a boundary or unused node return
 // (step2_pair, BULK) and are advanced by k_step2.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
-__global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP>()) k_step2_bulk(const StepParams p) {
+__global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP, ST>()) k_step2_bulk(const StepParams p) {
     // k_step2 (launched next, programmatic stream serialization) touches other
-    // tiles only: it may start as soon as every block here has started, and
+    // pairs only: it may start as soon as every block here has started, and
     // fills this grid's tail
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned seed = step_seed(p, ODD);
@@ -1204,16 +1204,14 @@ __global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP>()) k_step2_bulk(
     step2_pair<Q, OP, RHEO, ST, ODD, BLK, true>(p, seed, m);
 }
 
-// The pair step over the tiles with a boundary or unused node, one warp per
-// tile of the list p.special_tiles.
+// The pair step over the pairs with a boundary or unused node, one thread per
+// entry of the list p.special_pairs.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
 __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
     const unsigned seed = step_seed(p, ODD);
-    const unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (w >= (unsigned)p.n_special) return;
-    const unsigned m = ((unsigned)p.special_tiles[w] << 5) | (threadIdx.x & 31u);
-    if (m >= (unsigned)(p.N >> 1)) return;
-    step2_pair<Q, OP, RHEO, ST, ODD, BLK, false>(p, seed, m);
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (unsigned)p.n_special) return;
+    step2_pair<Q, OP, RHEO, ST, ODD, BLK, false>(p, seed, (unsigned)p.special_pairs[k]);
 }
 
 }  // namespace vlbm
