@@ -455,6 +455,71 @@ def serving_leg(vlbm, n_req=512, step_scale=0.25, rate=20.0, budget_gb=64.0, max
             "sample": f"{n_req} requests of the Bingham-duct serving stream, step counts x{step_scale}"}
 
 
+def shard_leg(args, rank, world, local):
+    """The channel split into z-slabs, one per rank (zslab.ZSlab): NX x NY x
+    (NZ x world) nodes, NZ planes per GPU, halos traded over NCCL around every
+    odd step (a single rank trades with itself).  One JSON line, weak scaling."""
+    import torch
+    import vlbm
+    import zslab
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    storage = {"f32": vlbm.STORE_F32, "f16": vlbm.STORE_F16, "bf16": vlbm.STORE_BF16}[args.storage]
+    cfg = make_cfg(vlbm, storage)
+    cfg.nz = NZ * world
+    cfg.layout = {"auto": vlbm.LAYOUT_AUTO, "natural": vlbm.LAYOUT_NATURAL, "zpair": vlbm.LAYOUT_ZPAIR}[args.layout]
+    cfg.device = local
+    slab = zslab.ZSlab(cfg, vlbm.BUILDER_PLATES_Y, autotune=True)
+    stream = slab.stream
+    slab.sim.init_equilibrium(1.0, 0, 0, 0)
+    slab.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    slab.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    slab.sim.sync()
+    t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    n_own = NX * NY * slab.n
+    value = NX * NY * cfg.nz * args.steps / (ms_max / 1e3) / 1e6
+    info = slab.sim.info()
+    odd_steps = args.steps // 2
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+        "config": dict(config_dict(args.storage), workload="D3Q%d channel %dx%dx%d split into %d z-slabs of %d planes"
+                       % (Q, NX, NY, cfg.nz, world, slab.n), parallelism="z-slab x%d" % world),
+        "layout": ("natural", "zpair", "zpair_blocked")[info.layout],
+        "halo_bytes_per_message": slab.sim.halo_bytes(),
+        "halo_messages_per_odd_step": 4,
+        "own_nodes_per_gpu": n_own,
+        "gpu_launches": args.steps * (1 if info.layout == 0 else 2) + odd_steps * 4,
+        "clocks": clk,
+    }
+    slab.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_reference(args, rank, world):
     """The reference arm: the FP64 OpenMP oracle, the reference's step restated
     on the host cores (the reference itself has no CPU path), on the full
@@ -488,6 +553,8 @@ def main():
     ap.add_argument("--no-cavity", action="store_true", help="skip the 256^3 Power-Law lid-cavity leg")
     ap.add_argument("--ibm-steps", type=int, default=50, help="timed steps of the 64-sphere IBM leg")
     ap.add_argument("--vel-set", type=int, default=19, choices=[19, 27])
+    ap.add_argument("--shard", action="store_true",
+                    help="one lattice split into z-slabs over the ranks (NZ planes per GPU) instead of replicas")
     ap.add_argument("--size", type=int, nargs=3, default=[256, 128, 64], metavar=("NX", "NY", "NZ"))
     ap.add_argument("--e2e-steps", type=int, default=3000,
                     help="steps of the end-to-end leg (its host copies are amortised over them)")
@@ -514,6 +581,8 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    if args.shard:
+        return shard_leg(args, rank, world, local)
     import vlbm
 
     storage = {"f32": vlbm.STORE_F32, "f16": vlbm.STORE_F16, "bf16": vlbm.STORE_BF16}[args.storage]

@@ -126,7 +126,12 @@ typedef struct vlbm_config {
     double ux_bc[8], uy_bc[8], uz_bc[8], rho_bc[8]; /* var.h:114-117 UX_BC..RHO_BC */
     double storage_scale;        /* F16/BF16 deviation scale; 0 = library default (F16: a power of two 1..2^24) */
     int32_t layout;              /* VLBM_LAYOUT_*: population storage order          */
-    int32_t reserved[7];
+    /* z-slab of a larger lattice (one slab per GPU, lbm.cu:601-657 N_GPUS):
+     * slab_nz_total > 0 is the whole lattice's NZ and global plane
+     * slab_z_offset + z is this lattice's plane z (its first and last planes
+     * being the ghost planes, see vlbm_halo_pack).  0, 0 for a whole lattice. */
+    int32_t slab_z_offset, slab_nz_total;
+    int32_t reserved[5];
     /* Cylindrical ducts (var.h:142-162), axis along z through the lattice centre
      * (DUCT_CENTER_X/Y).  Radii <= 0 take the var.h values: outer NY/2 - 1.5,
      * inner outer/4.  Wall motion of the interpolated bounce-back
@@ -243,7 +248,9 @@ typedef struct vlbm_info {
     int32_t last_kernel_variant; /* autotuned launch variant of the fused kernel  */
     int32_t layout;              /* population layout in use: 0 natural, 1 z-paired,
                                     2 z-paired in blocks of 32 pair-nodes         */
-    int32_t reserved[6];
+    int32_t aa_parity;           /* 1: the next step is the in-place scheme's odd
+                                    (neighbour) step, the one that needs halos  */
+    int32_t reserved[5];
 } vlbm_info;
 vlbm_status vlbm_get_info(vlbm_sim* sim, vlbm_info* info);
 
@@ -507,6 +514,38 @@ vlbm_status vlbm_autotune(vlbm_sim* sim, int32_t* chosen_variant);
 vlbm_status vlbm_set_layout(vlbm_sim* sim, int32_t layout);
 /* Force a kernel launch variant (0 = autotuned default). */
 vlbm_status vlbm_set_variant(vlbm_sim* sim, int32_t variant);
+
+/* ------------------------------------------------------ z-slab halos --- */
+/* One lattice split along z over several GPUs, one slab (and one process) per
+ * GPU; replaces the N_GPUS slabs with a ghost plane and the per-step
+ * population transfer between neighbouring GPUs (gpuPopulationsTransfer,
+ * lbm.cu:601-657, called from main.cu:336-350).  A slab of n planes is a
+ * simulation of n + 2 planes whose planes 0 and n + 1 are ghost copies of the
+ * neighbouring slabs' edge planes, marked unused in the node map
+ * (vlbm_build_node_map_planes).  The in-place step touches other nodes only in
+ * its odd phase (vlbm_info.aa_parity == 1), so slabs exchange only around odd
+ * steps: before it, plane 1's c_z = +1 and plane n's c_z = -1 populations go
+ * to the neighbours' ghost planes n + 1 and 0; after it, the ghost planes'
+ * c_z = -1 and c_z = +1 populations go back to the neighbours' planes n and 1.
+ * A message is the stored values of the populations with c_z == dz (dz = +1 or
+ * -1) of one plane, [k][ny][nx] with k over those populations in lattice order
+ * (5 for D3Q19, 9 for D3Q27), in the storage type; the same bytes whatever
+ * the layout.  Pack and unpack are asynchronous on the simulation's stream;
+ * dst / src are device pointers of vlbm_halo_bytes bytes. */
+vlbm_status vlbm_halo_bytes(vlbm_sim* sim, size_t* bytes);
+vlbm_status vlbm_halo_pack(vlbm_sim* sim, int32_t z, int32_t dz, void* dst);
+vlbm_status vlbm_halo_unpack(vlbm_sim* sim, int32_t z, int32_t dz, const void* src);
+/* The same for a slab's two messages of one exchange in one launch. */
+vlbm_status vlbm_halo_pack2(vlbm_sim* sim, int32_t z0, int32_t dz0, void* dst0, int32_t z1, int32_t dz1,
+                            void* dst1);
+vlbm_status vlbm_halo_unpack2(vlbm_sim* sim, int32_t z0, int32_t dz0, const void* src0, int32_t z1, int32_t dz1,
+                              const void* src1);
+/* The builder's words for planes z_first .. z_first + n_planes - 1 of an
+ * nx x ny x nz lattice, taken modulo nz (so z_first = z0 - 1 and n_planes =
+ * n + 2 give a slab with its ghost planes); n must be nx*ny*n_planes.  The
+ * caller marks the ghost planes unused (word 0) before vlbm_set_node_map. */
+vlbm_status vlbm_build_node_map_planes(int builder, int nx, int ny, int nz, int z_first, int n_planes,
+                                       uint32_t* map_out, size_t n);
 
 #ifdef __cplusplus
 }

@@ -123,7 +123,8 @@ class Config(C.Structure):
         ("uz_bc", C.c_double * 8), ("rho_bc", C.c_double * 8),
         ("storage_scale", C.c_double),
         ("layout", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("slab_z_offset", C.c_int32), ("slab_nz_total", C.c_int32),
+        ("reserved", C.c_int32 * 5),
         ("duct_outer_radius", C.c_double), ("duct_inner_radius", C.c_double),
         ("duct_outer_velocity", C.c_double), ("duct_outer_rotation", C.c_double),
         ("duct_inner_velocity", C.c_double), ("duct_inner_rotation", C.c_double),

@@ -69,6 +69,12 @@ vlbm_status sim_validate_config(const vlbm_config& c, std::string& why) {
     if (c.rheology == VLBM_BINGHAM && !(c.eta_p > 0.0 && c.yield_stress >= 0.0)) { why = "Bingham needs eta_p > 0, yield_stress >= 0"; return VLBM_ERR_INVALID; }
     if (c.rheology == VLBM_POWERLAW && !(c.n_index > 0.0 && c.k_consistency > 0.0)) { why = "Power-Law needs n_index > 0, k_consistency > 0"; return VLBM_ERR_INVALID; }
     if (!(c.rho0 > 0.0)) { why = "rho0 must be > 0"; return VLBM_ERR_INVALID; }
+    if (c.slab_nz_total != 0 &&
+        !(c.nz >= 3 && c.nz <= c.slab_nz_total + 2 && c.slab_z_offset >= 0 && c.slab_z_offset < c.slab_nz_total)) {
+        why = "a z-slab needs 3 <= nz <= slab_nz_total + 2 (ghost planes included) and 0 <= slab_z_offset < "
+              "slab_nz_total";
+        return VLBM_ERR_INVALID;
+    }
     if (c.storage == VLBM_STORE_F16 && c.storage_scale > 0) {   // 2^k, 0 <= k <= 24
         int e = 0;
         const double m = std::frexp(c.storage_scale, &e);
@@ -591,8 +597,46 @@ vlbm_status vlbm_get_info(vlbm_sim* s, vlbm_info* info) {
     info->bytes_per_node_step = 2.0 * s->Q * s->store_bytes;
     info->last_kernel_variant = s->variant;
     info->layout = s->pairH == 0 ? 0 : (s->pairBlk ? 2 : 1);
+    info->aa_parity = s->parity;
     ibm_counts(s, &info->n_particles, &info->n_lagrangian_nodes);
     return VLBM_OK;
+}
+
+vlbm_status vlbm_halo_bytes(vlbm_sim* s, size_t* bytes) {
+    CHECK_SIM(s);
+    if (!bytes) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
+    *bytes = (size_t)(s->Q == 19 ? 5 : 9) * s->cfg.nx * s->cfg.ny * (size_t)s->store_bytes;
+    return VLBM_OK;
+}
+
+static vlbm_status halo_copy(vlbm_sim* s, const HaloSpec (&m)[2], bool unpack) {
+    CHECK_SIM(s);
+    if (!m[0].buf && !m[1].buf) { set_last_error("null halo message"); return VLBM_ERR_INVALID; }
+    for (const HaloSpec& h : m)
+        if (h.buf && (h.z < 0 || h.z >= s->cfg.nz || (h.dz != 1 && h.dz != -1))) {
+            set_last_error("halo plane out of range or dz not +1 / -1");
+            return VLBM_ERR_INVALID;
+        }
+    VLBM_CUDA(launch_halo(s->Q, s->cfg.storage, s->pop, m, s->cfg.nx, s->cfg.ny, s->N, s->pairH, s->pairBlk,
+                          unpack, s->stream));
+    return VLBM_OK;
+}
+vlbm_status vlbm_halo_pack(vlbm_sim* s, int32_t z, int32_t dz, void* dst) {
+    const HaloSpec m[2] = {{dst, z, dz}, {nullptr, 0, 1}};
+    return halo_copy(s, m, false);
+}
+vlbm_status vlbm_halo_unpack(vlbm_sim* s, int32_t z, int32_t dz, const void* src) {
+    const HaloSpec m[2] = {{const_cast<void*>(src), z, dz}, {nullptr, 0, 1}};
+    return halo_copy(s, m, true);
+}
+vlbm_status vlbm_halo_pack2(vlbm_sim* s, int32_t z0, int32_t dz0, void* dst0, int32_t z1, int32_t dz1, void* dst1) {
+    const HaloSpec m[2] = {{dst0, z0, dz0}, {dst1, z1, dz1}};
+    return halo_copy(s, m, false);
+}
+vlbm_status vlbm_halo_unpack2(vlbm_sim* s, int32_t z0, int32_t dz0, const void* src0, int32_t z1, int32_t dz1,
+                              const void* src1) {
+    const HaloSpec m[2] = {{const_cast<void*>(src0), z0, dz0}, {const_cast<void*>(src1), z1, dz1}};
+    return halo_copy(s, m, true);
 }
 
 vlbm_status vlbm_set_variant(vlbm_sim* s, int32_t variant) {

@@ -52,6 +52,13 @@ cudaError_t launch_relayout(int Q, int st, const void* src, void* dst, int nx, i
 #undef C_
 }
 
+cudaError_t launch_halo(int Q, int st, void* pop, const HaloSpec* msgs, int nx, int ny, long long N, int H,
+                        int blk, bool unpack, cudaStream_t s) {
+#define C_(QQ, SS) launch_halo_st<QQ, SS>(pop, msgs, nx, ny, N, H, blk, unpack, s)
+    VLBM_SELECT(C_)
+#undef C_
+}
+
 #define VLBM_SELECT_INT(CALL)                                                      \
     if (Q == 19) {                                                                 \
         if (st == VLBM_STORE_F32) return CALL(19, VLBM_STORE_F32);                 \

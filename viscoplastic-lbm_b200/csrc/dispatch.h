@@ -32,6 +32,15 @@ template <int Q, int ST>
 cudaError_t launch_relayout_st(const void* src, void* dst, int nx, int ny, long long N, int sH, int sB, int dH,
                                int dB, cudaStream_t s);
 
+// One z-slab halo message: buffer (nullptr = none), plane and c_z.
+struct HaloSpec {
+    void* buf;
+    int z, dz;
+};
+template <int Q, int ST>
+cudaError_t launch_halo_st(void* pop, const HaloSpec* msgs, int nx, int ny, long long N, int H, int blk,
+                           bool unpack, cudaStream_t s);
+
 // Run-time selection over (Q, storage).
 cudaError_t launch_step(int Q, int st, const StepParams& p, int op, int rheo, bool odd, LaunchShape ls,
                         cudaStream_t s);
@@ -48,6 +57,11 @@ cudaError_t launch_batched(int Q, int st, const BatchLaunch* L, const BatchState
 // pairBlk of each; sH = 0 is the natural layout).
 cudaError_t launch_relayout(int Q, int st, const void* src, void* dst, int nx, int ny, long long N, int sH, int sB,
                             int dH, int dB, cudaStream_t s);
+// Copy two halo messages (msgs[0], msgs[1]: the populations with c_z == dz of
+// plane z) between the population array (layout H, blk) and dense buffers in
+// one launch (unpack: buffers -> array).
+cudaError_t launch_halo(int Q, int st, void* pop, const HaloSpec* msgs, int nx, int ny, long long N, int H,
+                        int blk, bool unpack, cudaStream_t s);
 // Resident 256-thread blocks per SM of the batched kernel of a group.
 int batched_blocks_per_sm(int Q, int st, int op, int rheo);
 template <int Q, int ST>

@@ -179,6 +179,15 @@ cudaError_t launch_relayout_st(const void* src, void* dst, int nx, int ny, long 
     return cudaGetLastError();
 }
 
+template <int Q, int ST>
+cudaError_t launch_halo_st(void* pop, const HaloSpec* msgs, int nx, int ny, long long N, int H, int blk,
+                           bool unpack, cudaStream_t s) {
+    const HaloMsg m0{msgs[0].buf, msgs[0].z, msgs[0].dz}, m1{msgs[1].buf, msgs[1].z, msgs[1].dz};
+    k_halo<Q, ST><<<grid_for(2LL * halo_pops<Q>() * nx * ny, 256), 256, 0, s>>>(pop, m0, m1, nx, ny, N, H, blk,
+                                                                                unpack ? 1 : 0);
+    return cudaGetLastError();
+}
+
 #define VLBM_INSTANTIATE(QQ, SS)                                                                              \
     template cudaError_t launch_step_st<QQ, SS>(const StepParams&, int, int, bool, LaunchShape, cudaStream_t); \
     template cudaError_t launch_macro_st<QQ, SS>(const MacroParams&, int, bool, cudaStream_t);                 \
@@ -189,6 +198,8 @@ cudaError_t launch_relayout_st(const void* src, void* dst, int nx, int ny, long 
                                                    int, bool, int, int, cudaStream_t);                          \
     template int batched_occupancy_st<QQ, SS>(int, int);                                                       \
     template cudaError_t launch_relayout_st<QQ, SS>(const void*, void*, int, int, long long, int, int, int, int,  \
-                                                    cudaStream_t);
+                                                    cudaStream_t);                                              \
+    template cudaError_t launch_halo_st<QQ, SS>(void*, const HaloSpec*, int, int, long long, int, int, bool,      \
+                                                cudaStream_t);
 
 }  // namespace vlbm

@@ -288,7 +288,10 @@ void interp_record(const vlbm_config& cfg, int x, int y, int z, uint32_t m, BcRe
     }
     const double rr = std::sqrt(xn * xn + yn * yn);
     const double c = rr > 0 ? xn / rr : 0.0, s = rr > 0 ? yn / rr : 0.0;
-    const double w = inside ? cfg.duct_inner_rotation : cfg.duct_outer_rotation * ((double)z / (double)cfg.nz);
+    const bool slab = cfg.slab_nz_total != 0;   // z of the whole lattice for a z-slab
+    const double zg = slab ? (double)((cfg.slab_z_offset + z) % cfg.slab_nz_total) : (double)z;
+    const double w = inside ? cfg.duct_inner_rotation
+                            : cfg.duct_outer_rotation * (zg / (double)(slab ? cfg.slab_nz_total : cfg.nz));
     r.uw[0] = (float)(-w * rad * s);
     r.uw[1] = (float)(w * rad * c);
     r.uw[2] = (float)(inside ? cfg.duct_inner_velocity : cfg.duct_outer_velocity);
@@ -319,6 +322,7 @@ vlbm_status tables_from_candidates(const vlbm_config& cfg, std::vector<std::pair
             if (bb_role(dir, i) != 1) continue;
             int t[3] = {lat_cx(i), lat_cy(i), lat_cz(i)};
             for (int a = 0; a < 3; ++a) if (nrm[0][a] != 0) t[a] = 0;
+            if (cfg.slab_nz_total != 0 && t[2] != 0) return VLBM_ERR_UNSUPPORTED;   // neighbour in another slab
             const int xs = ((x - t[0]) % nx + nx) % nx, ys = ((y - t[1]) % ny + ny) % ny,
                       zs = ((z - t[2]) % nz + nz) % nz;
             const size_t kn = (size_t)nx * ((size_t)ny * zs + ys) + xs;
@@ -425,11 +429,19 @@ vlbm_status build_bc_tables(const vlbm_config& cfg, const uint32_t* map, size_t 
         }
         if (needs_slot(m)) cand.emplace_back(k, m);
     }
-    return tables_from_candidates(cfg, cand, [map](size_t k) { return map[k]; }, out);
+    const vlbm_status st = tables_from_candidates(cfg, cand, [map](size_t k) { return map[k]; }, out);
+    if (st == VLBM_ERR_UNSUPPORTED)
+        err = "free-slip walls normal to x or y read post-collision values of z neighbours, which a z-slab's "
+              "ghost planes do not hold";
+    return st;
 }
 
 vlbm_status build_bc_tables_builder(const vlbm_config& cfg, int builder, BcTables& out, std::string& err) {
     const int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
+    if (cfg.slab_nz_total != 0) {
+        err = "a z-slab takes its node map from vlbm_build_node_map_planes, not a builder id";
+        return VLBM_ERR_INVALID;
+    }
     uint32_t w;
     if (!builder_word(builder, 0, 0, 0, nx, ny, nz, w)) { err = "unknown builder id"; return VLBM_ERR_NOT_FOUND; }
     auto word_at = [&](size_t k) {
@@ -480,11 +492,15 @@ vlbm_status build_bc_tables_builder(const vlbm_config& cfg, int builder, BcTable
 
 using namespace vlbm;
 
-extern "C" vlbm_status vlbm_build_node_map(int builder, int nx, int ny, int nz, uint32_t* map_out,
-                                           size_t n) {
-    if (nx <= 0 || ny <= 0 || nz <= 0 || !map_out) { set_last_error("invalid builder arguments"); return VLBM_ERR_INVALID; }
-    if (n != (size_t)nx * ny * nz) { set_last_error("map size does not match nx*ny*nz"); return VLBM_ERR_INVALID; }
-    for (int z = 0; z < nz; ++z)
+extern "C" vlbm_status vlbm_build_node_map_planes(int builder, int nx, int ny, int nz, int z_first, int n_planes,
+                                                  uint32_t* map_out, size_t n) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || n_planes <= 0 || !map_out) {
+        set_last_error("invalid builder arguments");
+        return VLBM_ERR_INVALID;
+    }
+    if (n != (size_t)nx * ny * n_planes) { set_last_error("map size does not match nx*ny*n_planes"); return VLBM_ERR_INVALID; }
+    for (int k = 0; k < n_planes; ++k) {
+        const int z = (int)((((long long)z_first + k) % nz + nz) % nz);
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) {
                 uint32_t w;
@@ -492,7 +508,14 @@ extern "C" vlbm_status vlbm_build_node_map(int builder, int nx, int ny, int nz, 
                     set_last_error("unknown builder id");
                     return VLBM_ERR_NOT_FOUND;
                 }
-                map_out[(size_t)nx * ((size_t)ny * z + y) + x] = w;
+                map_out[(size_t)nx * ((size_t)ny * k + y) + x] = w;
             }
+    }
     return VLBM_OK;
+}
+
+extern "C" vlbm_status vlbm_build_node_map(int builder, int nx, int ny, int nz, uint32_t* map_out, size_t n) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !map_out) { set_last_error("invalid builder arguments"); return VLBM_ERR_INVALID; }
+    if (n != (size_t)nx * ny * nz) { set_last_error("map size does not match nx*ny*nz"); return VLBM_ERR_INVALID; }
+    return vlbm_build_node_map_planes(builder, nx, ny, nz, 0, nz, map_out, n);
 }

@@ -1050,6 +1050,10 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
     IBM_CUDA(cudaSetDevice(s->device));
     if (s->ibm) { set_last_error("spheres were already added to this simulation"); return VLBM_ERR_STATE; }
     if (n <= 0 || n > IBM_MAX_PARTICLES) { set_last_error("sphere count must be in 1..1024"); return VLBM_ERR_INVALID; }
+    if (s->cfg.slab_nz_total != 0) {
+        set_last_error("spheres are not supported on a z-slab (the IBM step runs on whole lattices)");
+        return VLBM_ERR_UNSUPPORTED;
+    }
     if (ib->stencil != 4) {
         set_last_error("only the Peskin 4-point stencil (STENCIL_4) is supported");
         return VLBM_ERR_UNSUPPORTED;

@@ -413,6 +413,46 @@ __global__ void __launch_bounds__(256) k_relayout(const void* src, void* dst, in
     for (int i = 0; i < Q; ++i)
         D[layout_elem<Q>(i, x, y, z, nx, ny, N, dH, dB)] = S[layout_elem<Q>(i, x, y, z, nx, ny, N, sH, sB)];
 }
+
+// z-slab halo message: the stored values of the populations with c_z == dz of
+// plane z, [k][y][x] with k counting those populations in lattice order,
+// copied out of (pack) or into (unpack) the population array of any layout.
+template <int Q>
+constexpr int halo_pops() { return Q == 19 ? 5 : 9; }
+struct HaloMsg {
+    void* buf;
+    int z, dz;
+};
+// Two messages per launch (a slab's two faces); message m covers threads
+// [m * M, (m + 1) * M), M = halo_pops * nx * ny.
+template <int Q, int ST>
+__global__ void __launch_bounds__(256) k_halo(void* pop, HaloMsg m0, HaloMsg m1, int nx, int ny, long long N,
+                                              int H, int blk, int unpack) {
+    using T = typename Store<ST>::T;
+    const long long plane = (long long)nx * ny;
+    const long long M = halo_pops<Q>() * plane;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * M) return;
+    const bool second = t >= M;
+    if (second) t -= M;
+    const HaloMsg& m = second ? m1 : m0;
+    if (!m.buf) return;
+    const int z = m.z, dz = m.dz;
+    const int k = (int)(t / plane);
+    const int r = (int)(t - (long long)k * plane);
+    int i = 0;
+#pragma unroll
+    for (int j = 1, c = 0; j < Q; ++j)
+        if (lat_cz(j) == dz) {
+            if (c == k) i = j;
+            ++c;
+        }
+    T* P = static_cast<T*>(pop);
+    T* B = static_cast<T*>(m.buf);
+    const size_t e = layout_elem<Q>(i, r % nx, r / nx, z, nx, ny, N, H, blk);
+    if (unpack) P[e] = B[t];
+    else B[t] = P[e];
+}
 __device__ __forceinline__ int wrap1(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 // Gather f_i(x, t) of node n (after boundary rules).  Returns the side-store

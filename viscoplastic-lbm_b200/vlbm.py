@@ -64,7 +64,8 @@ class Config(C.Structure):
         ("uz_bc", C.c_double * 8), ("rho_bc", C.c_double * 8),
         ("storage_scale", C.c_double),
         ("layout", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("slab_z_offset", C.c_int32), ("slab_nz_total", C.c_int32),
+        ("reserved", C.c_int32 * 5),
         ("duct_outer_radius", C.c_double), ("duct_inner_radius", C.c_double),
         ("duct_outer_velocity", C.c_double), ("duct_outer_rotation", C.c_double),
         ("duct_inner_velocity", C.c_double), ("duct_inner_rotation", C.c_double),
@@ -144,7 +145,8 @@ class Info(C.Structure):
         ("storage_bytes", C.c_int32), ("step", C.c_int64), ("n_bc_nodes", C.c_int64),
         ("device_bytes", C.c_int64), ("bytes_per_node_step", C.c_double),
         ("n_particles", C.c_int32), ("n_lagrangian_nodes", C.c_int32),
-        ("last_kernel_variant", C.c_int32), ("layout", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("last_kernel_variant", C.c_int32), ("layout", C.c_int32), ("aa_parity", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -235,6 +237,12 @@ _SIGS = {
     "vlbm_autotune": [_P, C.POINTER(C.c_int32)],
     "vlbm_set_variant": [_P, C.c_int32],
     "vlbm_set_layout": [_P, C.c_int32],
+    "vlbm_halo_bytes": [_P, C.POINTER(C.c_size_t)],
+    "vlbm_halo_pack": [_P, C.c_int32, C.c_int32, _P],
+    "vlbm_halo_unpack": [_P, C.c_int32, C.c_int32, _P],
+    "vlbm_halo_pack2": [_P, C.c_int32, C.c_int32, _P, C.c_int32, C.c_int32, _P],
+    "vlbm_halo_unpack2": [_P, C.c_int32, C.c_int32, _P, C.c_int32, C.c_int32, _P],
+    "vlbm_build_node_map_planes": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _U32P, C.c_size_t],
 }
 EXPORTED = sorted(list(_SIGS) + ["vlbm_last_error", "vlbm_abi_version"])
 
@@ -291,6 +299,15 @@ def build_node_map(builder, nx, ny, nz):
     out = np.zeros(nx * ny * nz, dtype=np.uint32)
     _check(_lib.vlbm_build_node_map(builder, nx, ny, nz, out.ctypes.data_as(_U32P), out.size),
            "vlbm_build_node_map")
+    return out
+
+
+def build_node_map_planes(builder, nx, ny, nz, z_first, n_planes):
+    """The builder's words of planes z_first .. z_first + n_planes - 1 (modulo nz)
+    of an nx x ny x nz lattice, [n_planes][ny][nx] uint32."""
+    out = np.zeros(nx * ny * n_planes, dtype=np.uint32)
+    _check(_lib.vlbm_build_node_map_planes(builder, nx, ny, nz, z_first, n_planes, out.ctypes.data_as(_U32P),
+                                           out.size), "vlbm_build_node_map_planes")
     return out
 
 
@@ -448,6 +465,31 @@ class Simulation:
 
     def set_layout(self, layout):
         _check(_lib.vlbm_set_layout(self._h, layout), "vlbm_set_layout")
+
+    def aa_parity(self):
+        """1 when the next step is the in-place scheme's odd (neighbour) step."""
+        return self.info().aa_parity
+
+    def halo_bytes(self):
+        n = C.c_size_t()
+        _check(_lib.vlbm_halo_bytes(self._h, C.byref(n)), "vlbm_halo_bytes")
+        return n.value
+
+    def halo_pack(self, z, dz, dst):
+        """Populations with c_z == dz of plane z into the device tensor dst (halo_bytes bytes)."""
+        _check(_lib.vlbm_halo_pack(self._h, z, dz, C.c_void_p(dst.data_ptr())), "vlbm_halo_pack")
+
+    def halo_unpack(self, z, dz, src):
+        _check(_lib.vlbm_halo_unpack(self._h, z, dz, C.c_void_p(src.data_ptr())), "vlbm_halo_unpack")
+
+    def halo_pack2(self, m0, m1):
+        """Two messages in one launch; each m is (z, dz, tensor)."""
+        _check(_lib.vlbm_halo_pack2(self._h, m0[0], m0[1], C.c_void_p(m0[2].data_ptr()),
+                                    m1[0], m1[1], C.c_void_p(m1[2].data_ptr())), "vlbm_halo_pack2")
+
+    def halo_unpack2(self, m0, m1):
+        _check(_lib.vlbm_halo_unpack2(self._h, m0[0], m0[1], C.c_void_p(m0[2].data_ptr()),
+                                      m1[0], m1[1], C.c_void_p(m1[2].data_ptr())), "vlbm_halo_unpack2")
 
 
 class Server:
