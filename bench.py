@@ -70,6 +70,7 @@ def measured_peak():
 TRAFFIC_PROFILES = {
     # (storage, resolved layout) -> ncu summary of that kernel on this workload
     ("f32", "natural"): "fused_step_d3q19_bingham_256x128x64.md",
+    ("f32", "zpair"): "fused_step2_d3q19_bingham_f32_256x128x64.md",
     ("f16", "zpair"): "fused_step2_d3q19_bingham_f16_256x128x64.md",
 }
 

@@ -1234,10 +1234,6 @@ template <int Q, int OP, int ST> constexpr int step2_bulk_blocks() {
 // (step2_pair, BULK) and are advanced by k_step2.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
 __global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP, ST>()) k_step2_bulk(const StepParams p) {
-    // k_step2 (launched next, programmatic stream serialization) touches other
-    // pairs only: it may start as soon as every block here has started, and
-    // fills this grid's tail
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned seed = step_seed(p, ODD);
     const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= (unsigned)(p.N >> 1)) return;
@@ -1248,6 +1244,11 @@ __global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP, ST>()) k_step2_b
 // entry of the list p.special_pairs.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
 __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
+    // The bulk grid, launched next with programmatic stream serialization,
+    // touches other pairs only (each pair owns the slots it reads and writes):
+    // it starts while these few long boundary threads are in flight instead
+    // of after them.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned seed = step_seed(p, ODD);
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= (unsigned)p.n_special) return;
