@@ -23,7 +23,7 @@
 //                    Peskin 4-point interpolation (warp reduction), direct
 //                    forcing, spreading with fixed-point atomics; per-CTA
 //                    force/torque partials
-//     k_ibm_update   partials added in a fixed order, particle velocity and
+//     k_ibm_update   one warp per sphere: partials added in a fixed order, particle velocity and
 //                    rotation update; in the last iteration also the particle
 //                    movement and the step clock
 //     k_ibm_euler    over the boxes, each node by its owner sphere's CTAs:
@@ -102,6 +102,24 @@ __device__ __forceinline__ void dcross(const double a[3], const double b[3], dou
     o[2] = a[0] * b[1] - a[1] * b[0];
 }
 __device__ __forceinline__ int wrapi(int v, int n) { v %= n; return v < 0 ? v + n : v; }
+// A box coordinate onto the lattice: box_lo is at least -1 - n (a node just
+// across a periodic face) and a box spans at most the lattice, so one
+// correction usually suffices; wrapi covers the rest.
+__device__ __forceinline__ int wrap_box(int v, int n) {
+    if (v < 0) v += n;
+    else if (v >= n) v -= n;
+    return ((unsigned)v < (unsigned)n) ? v : wrapi(v, n);
+}
+
+// The IBM launches of a step form one chain, each launched as a programmatic
+// dependent of the one before (launch_chained): a kernel waits for its
+// predecessor's completion before touching memory, then lets its own
+// dependent be scheduled, so at most two kernels overlap and only their launch
+// latency and ramp are hidden.
+__device__ __forceinline__ void chain_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // Peskin 4-point kernel (ibmGlobalFunctions.h:28-48, STENCIL_4)
 __device__ __forceinline__ float stencil4(float x) {
@@ -191,12 +209,18 @@ __device__ void ibm_box(const IbmParams& P, DPart* parts, int sphere, const doub
 }
 
 // -------------------------------------------------------------- gather --
-// Box node k (x fastest) of a sphere's box, wrapped onto the lattice.
-__device__ __forceinline__ unsigned box_node(const IbmParams& P, const DPart& p, long long k) {
-    const int bx = p.box_n[0], by = p.box_n[1];
-    const int ix = (int)(k % bx), iy = (int)((k / bx) % by), iz = (int)(k / ((long long)bx * by));
-    const int x = wrapi(p.box_lo[0] + ix, P.nx), y = wrapi(p.box_lo[1] + iy, P.ny), z = wrapi(p.box_lo[2] + iz, P.nz);
+// Box node k (x fastest) of a sphere's box, wrapped onto the lattice.  A box
+// holds at most the lattice's nodes (< 2^31), so its indices are 32-bit.
+__device__ __forceinline__ unsigned box_node(const IbmParams& P, const DPart& p, unsigned k) {
+    const unsigned bx = (unsigned)p.box_n[0], by = (unsigned)p.box_n[1];
+    const unsigned t = k / bx;
+    const int ix = (int)(k - t * bx), iy = (int)(t % by), iz = (int)(t / by);
+    const int x = wrap_box(p.box_lo[0] + ix, P.nx), y = wrap_box(p.box_lo[1] + iy, P.ny),
+              z = wrap_box(p.box_lo[2] + iz, P.nz);
     return (unsigned)(((size_t)z * P.ny + y) * P.nx + x);
+}
+__device__ __forceinline__ unsigned box_size(const DPart& p) {
+    return (unsigned)p.box_n[0] * (unsigned)p.box_n[1] * (unsigned)p.box_n[2];
 }
 
 // IBM macroscopics of every node of the spheres' boxes (gpuUpdateMacrIBM,
@@ -207,16 +231,19 @@ __device__ __forceinline__ unsigned box_node(const IbmParams& P, const DPart& p,
 template <int Q, int ST, bool ODD, bool PAIRED>
 __global__ void __launch_bounds__(IBM_THREADS) k_ibm_gather(StepParams sp, IbmParams P, const DPart* parts,
                                                              float* fields, unsigned* owner, int split) {
+    chain_enter();
     // `split` CTAs per sphere share its box
     const unsigned sphere = blockIdx.x / split;
     const DPart& p = parts[sphere];
     const int sub = blockIdx.x % split;
-    const int bx = p.box_n[0], by = p.box_n[1], bz = p.box_n[2];
-    const long long tot = (long long)bx * by * bz;
+    const unsigned bx = (unsigned)p.box_n[0], by = (unsigned)p.box_n[1];
+    const unsigned tot = box_size(p);
     const size_t N = (size_t)sp.N;
-    for (long long k = (long long)sub * blockDim.x + threadIdx.x; k < tot; k += (long long)split * blockDim.x) {
-        const int ix = (int)(k % bx), iy = (int)((k / bx) % by), iz = (int)(k / ((long long)bx * by));
-        const int x = wrapi(p.box_lo[0] + ix, P.nx), y = wrapi(p.box_lo[1] + iy, P.ny), z = wrapi(p.box_lo[2] + iz, P.nz);
+    for (unsigned k = sub * blockDim.x + threadIdx.x; k < tot; k += split * blockDim.x) {
+        const unsigned t = k / bx;
+        const int ix = (int)(k - t * bx), iy = (int)(t % by), iz = (int)(t / by);
+        const int x = wrap_box(p.box_lo[0] + ix, P.nx), y = wrap_box(p.box_lo[1] + iy, P.ny),
+                  z = wrap_box(p.box_lo[2] + iz, P.nz);
         const unsigned n = (unsigned)(((size_t)z * P.ny + y) * P.nx + x);
         Nbr nb;
         nb.init(x, y, z, sp.nx, sp.ny, sp.nz);
@@ -527,6 +554,7 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_begin(IbmParams P, DPart* p
                                                             const double* Z, double* fx, double* fy, double* fz,
                                                             double* dx, double* dy, double* dz, double* contrib,
                                                             const int* clock) {
+    chain_enter();
     if ((int)blockIdx.x < P.np) {
         ibm_box(P, parts, blockIdx.x, X, Y, Z, fx, fy, fz, dx, dy, dz);
         return;
@@ -620,6 +648,7 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_interp_spread(IbmParams P, 
                                                                     double* ndy, double* ndz, const float* fields,
                                                                     unsigned long long* faux, double* fpart,
                                                                     int split) {
+    chain_enter();
     __shared__ double red[32];
     const int sphere = blockIdx.x / split, sub = blockIdx.x % split;
     const DPart& p = parts[sphere];
@@ -722,16 +751,26 @@ __device__ void move_particle(const IbmParams& P, DPart& p) {
 // update; after the last forcing iteration also the particle movement
 // (gpuParticleMovement ibm.cu:899-993) and the step clock.
 __global__ void k_ibm_update(IbmParams P, DPart* parts, const double* fpart, int split, int last, int* clock) {
-    for (int i = threadIdx.x; i < P.np; i += blockDim.x) {
+    chain_enter();
+    // one warp per sphere: lane l adds partials l, l + 32, ..., then a fixed
+    // shuffle tree adds the lanes (the same order in every run)
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < P.np; i += gridDim.x * wpb) {
         DPart& p = parts[i];
         double t[6] = {0, 0, 0, 0, 0, 0};
-        for (int b = 0; b < split; ++b)
+        for (int b = lane; b < split; b += 32)
             for (int a = 0; a < 6; ++a) t[a] += fpart[((size_t)i * split + b) * 6 + a];
-        for (int a = 0; a < 3; ++a) { p.f[a] += t[a]; p.M[a] += t[3 + a]; }
-        update_center(P, p);
-        if (last) move_particle(P, p);
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t[a] += __shfl_down_sync(0xffffffffu, t[a], o);
+        if (lane == 0) {
+            for (int a = 0; a < 3; ++a) { p.f[a] += t[a]; p.M[a] += t[3 + a]; }
+            update_center(P, p);
+            if (last) move_particle(P, p);
+        }
     }
-    if (last && threadIdx.x == 0) *clock += 1;   // read by the next step's contacts
+    if (last && blockIdx.x == 0 && threadIdx.x == 0) *clock += 1;   // read by the next step's contacts
 }
 
 // gpuParticleNodeMovement ibm.cu:1044-1197
@@ -778,6 +817,7 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_euler(IbmParams P, float* f
                                                             float* fibm, uint8_t* cls, unsigned* owner,
                                                             const DPart* parts, const int* pid, double* X, double* Y,
                                                             double* Z, int split, int last) {
+    chain_enter();
     const size_t N = (size_t)P.nx * P.ny * P.nz;
     if (last)
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P.nnodes; k += gridDim.x * blockDim.x)
@@ -785,8 +825,8 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_euler(IbmParams P, float* f
     const unsigned sphere = blockIdx.x / split;
     const DPart& p = parts[sphere];
     const int sub = blockIdx.x % split;
-    const long long tot = (long long)p.box_n[0] * p.box_n[1] * p.box_n[2];
-    for (long long k = (long long)sub * blockDim.x + threadIdx.x; k < tot; k += (long long)split * blockDim.x) {
+    const unsigned tot = box_size(p);
+    for (unsigned k = sub * blockDim.x + threadIdx.x; k < tot; k += split * blockDim.x) {
         const unsigned n = box_node(P, p, k);
         if (owner[n] != sphere) continue;
         if (last) owner[n] = IBM_NO_OWNER;
@@ -811,8 +851,8 @@ __global__ void __launch_bounds__(IBM_THREADS) k_ibm_fixup(IbmParams P, const DP
     const size_t N = (size_t)P.nx * P.ny * P.nz;
     const DPart& p = parts[blockIdx.x / split];
     const int sub = blockIdx.x % split;
-    const long long tot = (long long)p.box_n[0] * p.box_n[1] * p.box_n[2];
-    for (long long k = (long long)sub * blockDim.x + threadIdx.x; k < tot; k += (long long)split * blockDim.x) {
+    const unsigned tot = box_size(p);
+    for (unsigned k = sub * blockDim.x + threadIdx.x; k < tot; k += split * blockDim.x) {
         const unsigned n = box_node(P, p, k);
         if (rho) rho[n] = fields[n];
         if (ux) ux[n] = fields[N + n];
@@ -866,16 +906,32 @@ static void host_mesh(double diameter, double mesh_scale, double breugem, std::v
         if (e_ != cudaSuccess) return cuda_status(e_, #call);   \
     } while (0)
 
+// A launch of the IBM chain (chain_enter): programmatic stream serialisation.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_chained(void (*kernel)(KArgs...), unsigned grid, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(IBM_THREADS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int Q, int ST>
 static cudaError_t launch_gather(vlbm_sim* s, IbmState* st) {
     const StepParams sp = make_params(s);
     const bool pr = sp.pairH > 0;
     if (s->parity == 1) {
-        if (pr) k_ibm_gather<Q, ST, true, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
-        else k_ibm_gather<Q, ST, true, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
+        if (pr) return launch_chained(k_ibm_gather<Q, ST, true, true>, st->np * st->gsplit, s->stream, sp, st->prm, (const DPart*)st->parts, st->fields, st->owner, st->gsplit);
+        else return launch_chained(k_ibm_gather<Q, ST, true, false>, st->np * st->gsplit, s->stream, sp, st->prm, (const DPart*)st->parts, st->fields, st->owner, st->gsplit);
     } else {
-        if (pr) k_ibm_gather<Q, ST, false, true><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
-        else k_ibm_gather<Q, ST, false, false><<<st->np * st->gsplit, IBM_THREADS, 0, s->stream>>>(sp, st->prm, st->parts, st->fields, st->owner, st->gsplit);
+        if (pr) return launch_chained(k_ibm_gather<Q, ST, false, true>, st->np * st->gsplit, s->stream, sp, st->prm, (const DPart*)st->parts, st->fields, st->owner, st->gsplit);
+        else return launch_chained(k_ibm_gather<Q, ST, false, false>, st->np * st->gsplit, s->stream, sp, st->prm, (const DPart*)st->parts, st->fields, st->owner, st->gsplit);
     }
     return cudaGetLastError();
 }
@@ -901,20 +957,19 @@ vlbm_status ibm_step(vlbm_sim* s) {
                                                      st->ndx, st->ndy, st->ndz, st->contrib, st->clock);
     IBM_CUDA(cudaGetLastError());
     IBM_CUDA(gather_dispatch(s, st));
+    // the rest of the chain: programmatic dependents (chain_enter)
     const int iters = std::max(1, st->cfg.max_iterations);
     for (int it = 0; it < iters; ++it) {
         const int last = it == iters - 1;
-        k_ibm_interp_spread<<<st->np * st->split, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nS,
-                                                                         st->nfx, st->nfy, st->nfz, st->ndx, st->ndy,
-                                                                         st->ndz, st->fields, st->faux, st->fpart,
-                                                                         st->split);
-        IBM_CUDA(cudaGetLastError());
-        k_ibm_update<<<1, IBM_THREADS, 0, cs>>>(P, st->parts, st->fpart, st->split, last, st->clock);
-        IBM_CUDA(cudaGetLastError());
-        k_ibm_euler<<<st->np * st->gsplit, IBM_THREADS, 0, cs>>>(P, st->fields, st->faux, s->fibm, s->cls, st->owner,
-                                                                 st->parts, st->npid, st->nx, st->ny, st->nz,
-                                                                 st->gsplit, last);
-        IBM_CUDA(cudaGetLastError());
+        IBM_CUDA(launch_chained(k_ibm_interp_spread, st->np * st->split, cs, P, (const DPart*)st->parts,
+                                (const double*)st->nx, (const double*)st->ny, (const double*)st->nz,
+                                (const double*)st->nS, st->nfx, st->nfy, st->nfz, st->ndx, st->ndy, st->ndz,
+                                (const float*)st->fields, st->faux, st->fpart, st->split));
+        IBM_CUDA(launch_chained(k_ibm_update, (st->np + IBM_THREADS / 32 - 1) / (IBM_THREADS / 32), cs, P, st->parts,
+                                (const double*)st->fpart, st->split, last, st->clock));
+        IBM_CUDA(launch_chained(k_ibm_euler, st->np * st->gsplit, cs, P, st->fields, st->faux, s->fibm, s->cls,
+                                st->owner, (const DPart*)st->parts, (const int*)st->npid, st->nx, st->ny, st->nz,
+                                st->gsplit, last));
     }
     return VLBM_OK;
 }
