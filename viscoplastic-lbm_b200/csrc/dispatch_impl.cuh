@@ -30,15 +30,14 @@ cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s
     if (p.pairH > 0) {  // z-paired layout: one thread per node pair; the listed pairs, then the bulk ones
         const unsigned g = grid_for(p.N / 2, ls.block);
         const unsigned gs = grid_for(p.n_special, 256);
-        if (gs) {   // a normal launch: it waits for the previous step
-            if (p.pairBlk) {
-                if (odd) k_step2<Q, OP, RHEO, ST, true, true><<<gs, 256, 0, s>>>(p);
-                else k_step2<Q, OP, RHEO, ST, false, true><<<gs, 256, 0, s>>>(p);
-            } else {
-                if (odd) k_step2<Q, OP, RHEO, ST, true, false><<<gs, 256, 0, s>>>(p);
-                else k_step2<Q, OP, RHEO, ST, false, false><<<gs, 256, 0, s>>>(p);
-            }
-            cudaError_t e = cudaGetLastError();
+        if (gs) {   // chained to the previous step (step_chain_enter)
+            cudaError_t e;
+            if (p.pairBlk)
+                e = odd ? launch_overlapped(k_step2<Q, OP, RHEO, ST, true, true>, gs, 256, s, p)
+                        : launch_overlapped(k_step2<Q, OP, RHEO, ST, false, true>, gs, 256, s, p);
+            else
+                e = odd ? launch_overlapped(k_step2<Q, OP, RHEO, ST, true, false>, gs, 256, s, p)
+                        : launch_overlapped(k_step2<Q, OP, RHEO, ST, false, false>, gs, 256, s, p);
             if (e != cudaSuccess) return e;
             if (p.pairBlk)
                 return odd ? launch_overlapped(k_step2_bulk<Q, OP, RHEO, ST, true, true>, g, ls.block, s, p)
@@ -46,6 +45,7 @@ cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s
             return odd ? launch_overlapped(k_step2_bulk<Q, OP, RHEO, ST, true, false>, g, ls.block, s, p)
                        : launch_overlapped(k_step2_bulk<Q, OP, RHEO, ST, false, false>, g, ls.block, s, p);
         }
+        // no boundary list: a normal launch (the bulk kernel reads before it waits)
         if (p.pairBlk) {
             if (odd) k_step2_bulk<Q, OP, RHEO, ST, true, true><<<g, ls.block, 0, s>>>(p);
             else k_step2_bulk<Q, OP, RHEO, ST, false, true><<<g, ls.block, 0, s>>>(p);
@@ -55,10 +55,9 @@ cudaError_t step_t(const StepParams& p, bool odd, LaunchShape ls, cudaStream_t s
         }
         return cudaGetLastError();
     }
-    const unsigned g = grid_for(p.N, ls.block);
-    if (odd) k_step<Q, OP, RHEO, ST, true><<<g, ls.block, 0, s>>>(p);
-    else k_step<Q, OP, RHEO, ST, false><<<g, ls.block, 0, s>>>(p);
-    return cudaGetLastError();
+    const unsigned g = grid_for(p.N, ls.block);   // chained to the previous step (step_chain_enter)
+    return odd ? launch_overlapped(k_step<Q, OP, RHEO, ST, true>, g, ls.block, s, p)
+               : launch_overlapped(k_step<Q, OP, RHEO, ST, false>, g, ls.block, s, p);
 }
 
 template <int Q, int OP, int ST>

@@ -760,8 +760,19 @@ __device__ __forceinline__ unsigned step_seed(const StepParams& p, bool odd) {
     return s;
 }
 
+// Consecutive steps form a chain of programmatic dependents: a step's first
+// kernel waits for the previous kernel in the stream to complete (and its
+// writes to be visible) before it reads anything, then lets its own dependent
+// be scheduled, so the next launch's latency and ramp overlap this grid's
+// tail.  After a kernel that does not trigger, the wait returns at once.
+__device__ __forceinline__ void step_chain_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <int Q, int OP, int RHEO, int ST, bool ODD>
 __global__ void __launch_bounds__(256) k_step(const StepParams p) {
+    step_chain_enter();
     const unsigned seed = step_seed(p, ODD);
     const unsigned n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= (unsigned)p.N) return;
@@ -1234,21 +1245,29 @@ template <int Q, int OP, int ST> constexpr int step2_bulk_blocks() {
 // (step2_pair, BULK) and are advanced by k_step2.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
 __global__ void __launch_bounds__(256, step2_bulk_blocks<Q, OP, ST>()) k_step2_bulk(const StepParams p) {
+    // Launched as the programmatic dependent of the step's boundary list
+    // (k_step2), whose pairs it does not touch: it reads without waiting.  It
+    // lets the next step's first kernel be scheduled.  One thread of the last
+    // block waits for the boundary list before it exits, so this grid cannot
+    // complete before the list and the next step's single wait covers both;
+    // the last block runs in the grid's last wave, when the list is long done,
+    // so no block holds its SM idle.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned seed = step_seed(p, ODD);
     const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= (unsigned)(p.N >> 1)) return;
-    step2_pair<Q, OP, RHEO, ST, ODD, BLK, true>(p, seed, m);
+    if (m < (unsigned)(p.N >> 1)) step2_pair<Q, OP, RHEO, ST, ODD, BLK, true>(p, seed, m);
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // The pair step over the pairs with a boundary or unused node, one thread per
 // entry of the list p.special_pairs.
 template <int Q, int OP, int RHEO, int ST, bool ODD, bool BLK>
 __global__ void __launch_bounds__(256) k_step2(const StepParams p) {
-    // The bulk grid, launched next with programmatic stream serialization,
-    // touches other pairs only (each pair owns the slots it reads and writes):
-    // it starts while these few long boundary threads are in flight instead
-    // of after them.
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    // The step's first kernel: it waits for the previous step, then lets the
+    // bulk grid start.  The bulk grid touches other pairs only (each pair owns
+    // the slots it reads and writes), so it runs while these few long
+    // boundary threads are in flight instead of after them.
+    step_chain_enter();
     const unsigned seed = step_seed(p, ODD);
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= (unsigned)p.n_special) return;
