@@ -481,7 +481,9 @@ vlbm_status vlbm_server_fetch(vlbm_server* srv, uint64_t tag, float* ux, size_t 
  * directly, [7] graph launches, [8] graph captures, [9] host seconds in graph
  * captures (part of [2]); then the device bytes of the server's memory cache,
  * [10] held by resident and retiring lattices and [11] cached for reuse (their
- * sum stays within the HBM budget).  Writes min(n, 12) values. */
+ * sum stays within the HBM budget); then the parts of [0]: [12] creating
+ * lattices, [13] their boundary tables, [14] their spheres, [15] handing
+ * them to the server stream.  Writes min(n, 16) values. */
 vlbm_status vlbm_server_profile(vlbm_server* srv, double* seconds, int32_t n);
 /* Tuning: sphere-free lattices with at least `nodes` nodes get their own
  * single-lattice launch each step instead of sharing the batched launch.

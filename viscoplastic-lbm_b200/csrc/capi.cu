@@ -188,7 +188,7 @@ static vlbm_status fill_side_equilibrium(vlbm_sim* s) {
     const long long tot = (long long)s->Q * s->nbc;
     k_fill_side<<<(unsigned)((tot + 255) / 256), 256, 0, s->stream>>>(s->side[0], s->side[1], s->nbc, s->Q);
     VLBM_CUDA(cudaGetLastError());
-    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    if (!s->async_setup) VLBM_CUDA(cudaStreamSynchronize(s->stream));
     return VLBM_OK;
 }
 
@@ -231,7 +231,10 @@ static vlbm_status build_pair_tiles(vlbm_sim* s) {
 // Install boundary tables: class bytes and slots (bulk everywhere, then the
 // boundary nodes scattered on the device), the records and the side store.
 static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
-    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    // the old tables are freed below: wait for work that may still read them
+    // (a simulation set up without host waits has none yet)
+    const bool wait = !s->async_setup;
+    if (wait || s->geometry) VLBM_CUDA(cudaStreamSynchronize(s->stream));
     sim_free(s, s->bc); sim_free(s, s->side[0]); sim_free(s, s->side[1]); sim_free(s, s->bc_node);
     sim_free(s, s->bc_q);
     s->bc = nullptr; s->side[0] = s->side[1] = nullptr; s->bc_node = nullptr; s->bc_q = nullptr;
@@ -243,15 +246,14 @@ static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
         const long long cnt = (long long)t.unused_nodes.size();
         void* d = nullptr;
         VLBM_CUDA(cudaMallocAsync(&d, (size_t)cnt * sizeof(int32_t), s->stream));
-        cudaError_t e = cudaMemcpyAsync(d, t.unused_nodes.data(), (size_t)cnt * sizeof(int32_t),
-                                        cudaMemcpyHostToDevice, s->stream);
+        cudaError_t e = sim_upload(s, d, t.unused_nodes.data(), (size_t)cnt * sizeof(int32_t));
         if (e == cudaSuccess) {
             k_mark_unused<<<(unsigned)((cnt + 255) / 256), 256, 0, s->stream>>>(static_cast<const int32_t*>(d), cnt,
                                                                                s->cls);
             e = cudaGetLastError();
         }
         cudaFreeAsync(d, s->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);   // before the host list goes away
+        if (e == cudaSuccess && wait) e = cudaStreamSynchronize(s->stream);   // before the host list goes away
         VLBM_CUDA(e);
     }
     if (s->nbc > 0) {
@@ -265,20 +267,17 @@ static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
             if ((st = alloc_dev(s, &p, (size_t)s->Q * s->nbc * sizeof(float))) != VLBM_OK) return st;
             s->side[b] = static_cast<float*>(p);
         }
-        VLBM_CUDA(cudaMemcpyAsync(s->bc, t.recs.data(), t.recs.size() * sizeof(BcRec), cudaMemcpyHostToDevice,
-                                  s->stream));
-        VLBM_CUDA(cudaMemcpyAsync(s->bc_node, t.bc_nodes.data(), t.bc_nodes.size() * sizeof(int32_t),
-                                  cudaMemcpyHostToDevice, s->stream));
+        VLBM_CUDA(sim_upload(s, s->bc, t.recs.data(), t.recs.size() * sizeof(BcRec)));
+        VLBM_CUDA(sim_upload(s, s->bc_node, t.bc_nodes.data(), t.bc_nodes.size() * sizeof(int32_t)));
         if (!t.q8.empty()) {
             if ((st = alloc_dev(s, &p, t.q8.size() * sizeof(float))) != VLBM_OK) return st;
             s->bc_q = static_cast<float*>(p);
-            VLBM_CUDA(cudaMemcpyAsync(s->bc_q, t.q8.data(), t.q8.size() * sizeof(float), cudaMemcpyHostToDevice,
-                                      s->stream));
+            VLBM_CUDA(sim_upload(s, s->bc_q, t.q8.data(), t.q8.size() * sizeof(float)));
         }
         k_scatter_bc<<<(s->nbc + 255) / 256, 256, 0, s->stream>>>(s->bc_node, s->nbc, s->cls, s->bc_slot);
         VLBM_CUDA(cudaGetLastError());
         if ((st = fill_side_equilibrium(s)) != VLBM_OK) return st;   // synchronises the stream
-    } else {
+    } else if (wait) {
         VLBM_CUDA(cudaStreamSynchronize(s->stream));
     }
     vlbm_status st = build_pair_tiles(s);
@@ -318,7 +317,22 @@ vlbm_sim::~vlbm_sim() {
                     (void*)omega, (void*)fibm, (void*)err, (void*)step_ctr, (void*)scratch, (void*)red_scratch, (void*)bc_q,
                     (void*)treat_prev, (void*)treat_red, (void*)special_pairs})
         free_with(allocator, p);
+    if (allocator)
+        for (void* h : staging) allocator->release_staging(h);
     if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+cudaError_t vlbm::sim_upload(vlbm_sim* s, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    if (s->async_setup && s->allocator) {
+        void* h = s->allocator->staging(bytes);
+        if (h) {   // pinned: the copy is queued and the host returns at once
+            std::memcpy(h, src, bytes);
+            s->staging.push_back(h);
+            return cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, s->stream);
+        }
+    }
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->stream);
 }
 
 #define CHECK_SIM(s)                                                        \
@@ -369,7 +383,8 @@ void vlbm::sim_release(vlbm_sim* s) {
     delete s;
 }
 
-vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator, vlbm_sim** out) {
+vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator, vlbm_sim** out,
+                             bool async_setup) {
     if (!cfg || !out) { set_last_error("null argument"); return VLBM_ERR_INVALID; }
     *out = nullptr;
     std::string why;
@@ -402,7 +417,16 @@ vlbm_status vlbm::sim_create(const vlbm_config* cfg, DeviceAllocator* allocator,
         // pointer (D3Q19 FP16 256^3: 57.6k against 53.3k MLUPS)
         s->pairBlk = s->pairH > 0 ? blocked_pairs_ok(s) : 0;
     }
-    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    s->async_setup = async_setup;
+    if (async_setup) {
+        // set-up kernels that run while a long queue of other work holds the
+        // SMs (a server admitting a lattice) are scheduled ahead of it
+        int least = 0, greatest = 0;
+        e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, greatest);
+    } else {
+        e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    }
     if (e != cudaSuccess) { delete s; return cuda_status(e, "cudaStreamCreate"); }
     s->own_stream = true;
     const size_t N = (size_t)s->N;
@@ -474,7 +498,7 @@ vlbm_status vlbm_init_equilibrium(vlbm_sim* s, double rho, double ux, double uy,
     if (s->fibm) VLBM_CUDA(cudaMemsetAsync(s->fibm, 0, (size_t)3 * s->N * sizeof(float), s->stream));
     if (s->nbc > 0) { vlbm_status st = fill_side_equilibrium(s); if (st != VLBM_OK) return st; }
     if (s->ibm) ibm_reset(s);
-    VLBM_CUDA(cudaStreamSynchronize(s->stream));
+    if (!s->async_setup) VLBM_CUDA(cudaStreamSynchronize(s->stream));
     return VLBM_OK;
 }
 

@@ -131,9 +131,9 @@ cudaError_t launch_set_pops_st(const StepParams& p, const float* in, float rho, 
 template <int Q, int OP, int RHEO, int ST>
 cudaError_t batched_t(const BatchLaunch* L, const BatchState* state, const BatchBlock* table, int ntiles, int grid,
                       bool odd, cudaStream_t s) {
-    if (odd) k_step_batched<Q, OP, RHEO, ST, true><<<grid, 256, 0, s>>>(L, state, table, ntiles);
-    else k_step_batched<Q, OP, RHEO, ST, false><<<grid, 256, 0, s>>>(L, state, table, ntiles);
-    return cudaGetLastError();
+    // chained to the previous launch of the stream (step_chain_enter)
+    return odd ? launch_overlapped(k_step_batched<Q, OP, RHEO, ST, true>, grid, 256, s, L, state, table, ntiles)
+               : launch_overlapped(k_step_batched<Q, OP, RHEO, ST, false>, grid, 256, s, L, state, table, ntiles);
 }
 
 template <int Q, int OP, int ST>

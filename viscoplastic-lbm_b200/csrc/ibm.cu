@@ -1213,20 +1213,23 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
         if (e == cudaSuccess) s->device_bytes += 3 * N * sizeof(float);
     }
     if (e != cudaSuccess) { ibm_destroy(st, s->allocator); return cuda_status(e, "IBM allocation"); }
-    e = cudaMemcpy(st->parts, parts.data(), parts.size() * sizeof(DPart), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(st->nx, X.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(st->ny, Y.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(st->nz, Z.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(st->nS, S.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(st->npid, pid.data(), nn * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(st->fields, 0, 4 * N * sizeof(float));
-    if (e == cudaSuccess) e = cudaMemset(st->faux, 0, 3 * N * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(st->owner, 0xFF, N * sizeof(unsigned));   // IBM_NO_OWNER
-    if (e == cudaSuccess) {   // the contact history clock starts at the lattice's step count
-        const int clock = (int)s->step;
-        e = cudaMemcpy(st->clock, &clock, sizeof(int), cudaMemcpyHostToDevice);
-    }
-    if (e == cudaSuccess) e = cudaMemset(s->fibm, 0, 3 * N * sizeof(float));
+    // uploads and clears on the simulation's stream; a simulation set up
+    // without host waits (a server admitting it while its batch work runs)
+    // uploads from pinned staging and leaves the work queued
+    const cudaStream_t ss = s->stream;
+    const int clock = (int)s->step;   // the contact history clock starts at the lattice's step count
+    e = sim_upload(s, st->parts, parts.data(), parts.size() * sizeof(DPart));
+    if (e == cudaSuccess) e = sim_upload(s, st->nx, X.data(), nn * sizeof(double));
+    if (e == cudaSuccess) e = sim_upload(s, st->ny, Y.data(), nn * sizeof(double));
+    if (e == cudaSuccess) e = sim_upload(s, st->nz, Z.data(), nn * sizeof(double));
+    if (e == cudaSuccess) e = sim_upload(s, st->nS, S.data(), nn * sizeof(double));
+    if (e == cudaSuccess) e = sim_upload(s, st->npid, pid.data(), nn * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->fields, 0, 4 * N * sizeof(float), ss);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->faux, 0, 3 * N * sizeof(unsigned long long), ss);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->owner, 0xFF, N * sizeof(unsigned), ss);   // IBM_NO_OWNER
+    if (e == cudaSuccess) e = sim_upload(s, st->clock, &clock, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->fibm, 0, 3 * N * sizeof(float), ss);
+    if (e == cudaSuccess && !s->async_setup) e = cudaStreamSynchronize(ss);   // the host vectors go out of scope
     if (e != cudaSuccess) { ibm_destroy(st, s->allocator); return cuda_status(e, "IBM setup"); }
     st->initial = parts;
     st->init_nodes.resize(3 * nn);

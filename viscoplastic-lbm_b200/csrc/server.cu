@@ -42,6 +42,9 @@ namespace vlbm {
 
 // After every lattice of the batch took its step.
 __global__ void k_batch_advance(BatchState* state, int nslots) {
+    // chained like the batched steps: wait for the step's last batched launch
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nslots) return;
     state[i].parity ^= 1;
@@ -52,8 +55,16 @@ __global__ void k_batch_advance(BatchState* state, int nslots) {
 
 cudaError_t launch_batch_advance(BatchState* state, int nslots, cudaStream_t s) {
     if (nslots <= 0) return cudaSuccess;
-    k_batch_advance<<<(nslots + 127) / 128, 128, 0, s>>>(state, nslots);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((nslots + 127) / 128);
+    cfg.blockDim = dim3(128);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_batch_advance, state, nslots);
 }
 
 }  // namespace vlbm
@@ -164,6 +175,28 @@ struct DevCache final : DeviceAllocator {
         free_bytes += it->second;
         live_bytes -= it->second;
     }
+    // pinned staging for the uploads of admitted lattices, reused best fit
+    std::multimap<size_t, void*> hfree_;
+    std::vector<void*> hall_;
+    std::unordered_map<void*, size_t> hsize_;
+    void* staging(size_t bytes) override {
+        const size_t need = (bytes + 4095) & ~(size_t)4095;
+        auto it = hfree_.lower_bound(need);
+        if (it != hfree_.end() && it->first <= 2 * need) {
+            void* h = it->second;
+            hfree_.erase(it);
+            return h;
+        }
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, need, cudaHostAllocDefault) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        hall_.push_back(h);
+        hsize_[h] = need;
+        return h;
+    }
+    void release_staging(void* h) override {
+        auto it = hsize_.find(h);
+        if (it != hsize_.end()) hfree_.insert({it->second, h});
+    }
     void trim(size_t keep) {
         while (free_bytes > keep && !free_.empty()) {
             auto it = std::prev(free_.end());
@@ -176,6 +209,7 @@ struct DevCache final : DeviceAllocator {
     ~DevCache() override {
         trim(0);
         for (auto& kv : size_of) cudaFree(kv.first);   // nothing should be live here
+        for (void* h : hall_) cudaFreeHost(h);
     }
 };
 
@@ -231,7 +265,7 @@ struct vlbm_server {
     double lattice_updates = 0.0;
     // admit, rebuild, enqueue (incl. graph captures), wait, read-out [s];
     // batch steps, direct kernel launches, graph launches, graph captures
-    double prof[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double prof[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // batch tables (rebuilt when the membership changes)
     bool dirty = true;
     BatchState* d_state = nullptr;
@@ -695,6 +729,23 @@ void fail_request(vlbm_server* sv, const Pending& p, vlbm_status st) {
     sv->done.push_back(c);
 }
 
+// Move a lattice built without host waits onto the server stream: the server
+// stream waits for its set-up (an event on the lattice's own stream, which is
+// released once that work completes); later calls wait as usual.
+vlbm_status hand_over(vlbm_server* sv, vlbm_sim* s) {
+    cudaEvent_t ready = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ready, s->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sv->stream, ready, 0);
+    if (ready) cudaEventDestroy(ready);
+    if (e != cudaSuccess) return cuda_status(e, "lattice hand-over");
+    if (s->own_stream) cudaStreamDestroy(s->stream);   // released when its work completes
+    s->stream = sv->stream;
+    s->own_stream = false;
+    s->async_setup = false;
+    return VLBM_OK;
+}
+
 // Admit queued requests in arrival order while the slot limit and the HBM
 // budget allow.  A new lattice is built on its own stream (its set-up copies
 // and kernels do not wait for the queued batch work) from the server's memory
@@ -710,11 +761,21 @@ vlbm_status server_admit(vlbm_server* sv) {
         cfg.device = sv->device;
         cfg.layout = VLBM_LAYOUT_NATURAL;   // the batched kernel streams one node per thread
         vlbm_sim* s = nullptr;
-        vlbm_status st = sim_create(&cfg, &sv->cache, &s);
+        const double a0 = now_s();
+        // built without host waits on a high-priority stream of its own; the
+        // server stream waits for the set-up through an event
+        vlbm_status st = sim_create(&cfg, &sv->cache, &s, true);
+        const double a1 = now_s();
         if (st == VLBM_OK) st = vlbm_set_builder(s, p.req.builder);
+        const double a2 = now_s();
         if (st == VLBM_OK && !p.spheres.empty())
             st = vlbm_add_spheres(s, &p.req.ibm, p.spheres.data(), (int32_t)p.spheres.size());
-        if (st == VLBM_OK) st = vlbm_set_stream(s, sv->stream);
+        const double a3 = now_s();
+        if (st == VLBM_OK) st = hand_over(sv, s);
+        sv->prof[12] += a1 - a0;
+        sv->prof[13] += a2 - a1;
+        sv->prof[14] += a3 - a2;
+        sv->prof[15] += now_s() - a3;
         if (st != VLBM_OK) {
             if (s) vlbm_destroy(s);
             fail_request(sv, p, st);
@@ -971,7 +1032,7 @@ vlbm_status vlbm_server_profile(vlbm_server* sv, double* seconds, int32_t n) {
     sv->prof[9] = sv->capture_s;
     sv->prof[10] = (double)sv->cache.live_bytes;
     sv->prof[11] = (double)sv->cache.free_bytes;
-    for (int32_t i = 0; i < n && i < 12; ++i) seconds[i] = sv->prof[i];
+    for (int32_t i = 0; i < n && i < 16; ++i) seconds[i] = sv->prof[i];
     return VLBM_OK;
 }
 

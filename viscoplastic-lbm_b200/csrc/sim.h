@@ -23,6 +23,11 @@ struct DeviceBuffer {
 struct DeviceAllocator {
     virtual cudaError_t allocate(void** p, size_t bytes) = 0;
     virtual void release(void* p) = 0;
+    // Pinned host memory for the uploads of a simulation built without host
+    // waits (async_setup): held by the simulation until it is destroyed, when
+    // its device work has completed.  nullptr: no staging, upload and wait.
+    virtual void* staging(size_t) { return nullptr; }
+    virtual void release_staging(void*) {}
     virtual ~DeviceAllocator() = default;
 };
 
@@ -72,6 +77,11 @@ struct vlbm_sim {
 
     vlbm::IbmState* ibm = nullptr;   // owned; released by ibm_destroy
     vlbm::DeviceAllocator* allocator = nullptr;   // not owned; nullptr: cudaMalloc/cudaFree
+    // Built without host waits: set-up work stays queued on `stream` and its
+    // uploads come from pinned staging buffers (allocator->staging), released
+    // with the simulation.
+    bool async_setup = false;
+    std::vector<void*> staging;
     ~vlbm_sim();
 };
 
@@ -86,7 +96,15 @@ void sim_free(vlbm_sim* s, void* p);
 cudaError_t alloc_with(DeviceAllocator* a, void** p, size_t bytes);
 void free_with(DeviceAllocator* a, void* p);
 // vlbm_create with a device-memory source (nullptr: cudaMalloc/cudaFree).
-vlbm_status sim_create(const vlbm_config* cfg, DeviceAllocator* allocator, vlbm_sim** out);
+// async_setup: the set-up runs on a high-priority stream of its own without
+// host waits (a server admitting a lattice while a long queue of other work
+// holds the SMs); the caller orders later work after it with an event.
+vlbm_status sim_create(const vlbm_config* cfg, DeviceAllocator* allocator, vlbm_sim** out,
+                       bool async_setup = false);
+// Upload `bytes` from host `src` to device `dst` on the simulation's stream:
+// through a pinned staging copy when the simulation is built without host
+// waits, else a plain copy after which the caller may wait.
+cudaError_t sim_upload(vlbm_sim* s, void* dst, const void* src, size_t bytes);
 // Free a simulation whose device work is known to be complete (no stream
 // synchronisation).
 void sim_release(vlbm_sim* s);

@@ -823,6 +823,7 @@ __global__ void __launch_bounds__(256, batch_min_blocks<Q>()) k_step_batched(con
                                                                             const BatchState* __restrict__ state,
                                                                             const BatchBlock* __restrict__ table,
                                                                             int ntiles) {
+    step_chain_enter();   // after the previous launch of the server stream
     __shared__ StepParams sp;
     __shared__ float* sides[2];
     __shared__ int use_bc;

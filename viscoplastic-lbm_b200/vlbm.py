@@ -531,11 +531,12 @@ class Server:
     def profile(self):
         """Host seconds per phase of the serving loop, launch counters and the
         device bytes of the memory cache (live, cached)."""
-        out = (C.c_double * 12)()
-        _check(_lib.vlbm_server_profile(self._h, out, 12), "vlbm_server_profile")
+        out = (C.c_double * 16)()
+        _check(_lib.vlbm_server_profile(self._h, out, 16), "vlbm_server_profile")
         return dict(zip(("admit_s", "rebuild_s", "enqueue_s", "wait_s", "readout_s", "batch_steps",
                          "direct_launches", "graph_launches", "graph_captures", "capture_s",
-                         "device_live_bytes", "device_cached_bytes"), list(out)))
+                         "device_live_bytes", "device_cached_bytes", "admit_create_s", "admit_tables_s",
+                         "admit_spheres_s", "admit_stream_s"), list(out)))
 
     def set_own_launch_min(self, nodes):
         """Lattices of at least `nodes` nodes get their own launch (-1: default rule)."""
