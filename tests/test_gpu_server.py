@@ -5,11 +5,13 @@ a lattice depends only on the lattice (its size and whether it has spheres),
 and the IBM step sums its spread forces in fixed point and its sphere forces in
 a fixed order, so a result does not depend on the other lattices.
 
-Server vs a plain vlbm_sim: lattices with their own launch (spheres, or large)
-run the same kernel and match bit for bit; small lattices run the batched
-kernel, which inlines the same per-node code but may contract a multiply-add
-differently (one FP32 rounding), so they must match to relative L2 1e-4 after
-the few hundred steps run here.
+Server vs a plain vlbm_sim: lattices with their own launches (spheres, or a
+full wave of the batched kernel) keep the library's layout (LAYOUT_AUTO) and
+run the same kernels, so they match a plain simulation in that layout bit for
+bit; small lattices run the batched kernel in the natural layout, which
+inlines the same per-node code but may contract a multiply-add differently
+(one FP32 rounding), so they must match a natural-layout simulation to
+relative L2 1e-4 after the few hundred steps run here.
 """
 import numpy as np
 import pytest
@@ -47,7 +49,10 @@ def cfg_of(vlbm, kw):
 
 
 def alone(vlbm, kw, builder, steps, spheres):
-    sim = vlbm.Simulation(cfg_of(vlbm, kw), builder=builder)
+    cfg = cfg_of(vlbm, kw)
+    if spheres:   # the server keeps the library's layout for lattices with spheres
+        cfg.layout = vlbm.LAYOUT_AUTO
+    sim = vlbm.Simulation(cfg, builder=builder)
     if spheres:
         sim.add_spheres(vlbm.IbmConfig.default(**IBM_KW), [vlbm.Sphere(**s) for s in spheres])
     sim.step(steps)
@@ -204,3 +209,18 @@ def test_device_footprint_stays_within_budget(vlbm):
     assert all(c.status == vlbm.OK for c in done)
     assert peak > 0
     srv.close()
+
+
+def test_large_lattice_keeps_the_library_layout(vlbm):
+    """A lattice that fills a wave of the batched kernel by itself steps with
+    launches of its own in the library's layout (z-paired for FP16): bit for
+    bit a plain simulation in LAYOUT_AUTO."""
+    kw = dict(nx=96, ny=48, nz=48, vel_set=19, rheology=1, eta_p=0.1, yield_stress=1e-5, fx=2e-5, storage=1)
+    got = alone_in_server(vlbm, kw, 5, 61, [])
+    sim = vlbm.Simulation(vlbm.Config.default(**kw), builder=5)
+    assert sim.info().layout != 0
+    sim.step(61)
+    sim.sync()
+    ref = sim.macroscopics()["ux"].ravel().copy()
+    sim.close()
+    np.testing.assert_array_equal(got, ref)

@@ -208,7 +208,9 @@ static int blocked_pairs_ok(const vlbm_sim* s) {
     return (s->cfg.nx % 32 == 0 && (s->N / 2) * s->Q < (1ll << 31)) ? 1 : 0;
 }
 
-static vlbm_status build_pair_tiles(vlbm_sim* s) {
+// host_count >= 0: the number of listed pairs, known on the host (a set-up
+// without host waits); else it is read back from the device.
+static vlbm_status build_pair_tiles(vlbm_sim* s, long long host_count = -1) {
     if (s->pairH <= 0) return VLBM_OK;
     const long long M = s->N / 2;
     vlbm_status st;
@@ -221,6 +223,10 @@ static vlbm_status build_pair_tiles(vlbm_sim* s) {
     VLBM_CUDA(cudaMemsetAsync(count, 0, sizeof(int), s->stream));
     k_special_pairs<<<(unsigned)((M + 255) / 256), 256, 0, s->stream>>>(s->cls, M, s->special_pairs, count);
     VLBM_CUDA(cudaGetLastError());
+    if (host_count >= 0) {
+        s->n_special = (int)host_count;
+        return VLBM_OK;
+    }
     int n = 0;
     VLBM_CUDA(cudaMemcpyAsync(&n, count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     VLBM_CUDA(cudaStreamSynchronize(s->stream));
@@ -280,7 +286,18 @@ static vlbm_status install_tables(vlbm_sim* s, const BcTables& t) {
     } else if (wait) {
         VLBM_CUDA(cudaStreamSynchronize(s->stream));
     }
-    vlbm_status st = build_pair_tiles(s);
+    long long listed = -1;
+    if (!wait && s->pairH > 0) {   // pairs holding a boundary or unused node, counted here
+        const long long M = s->N / 2;
+        std::vector<char> mark((size_t)M, 0);
+        listed = 0;
+        for (const std::vector<int32_t>* v : {&t.bc_nodes, &t.unused_nodes})
+            for (int32_t n : *v) {
+                const long long m = n < M ? n : n - M;
+                if (!mark[(size_t)m]) { mark[(size_t)m] = 1; ++listed; }
+            }
+    }
+    vlbm_status st = build_pair_tiles(s, listed);
     if (st != VLBM_OK) return st;
     s->geometry = true;
     return VLBM_OK;

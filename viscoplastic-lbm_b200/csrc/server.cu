@@ -385,12 +385,13 @@ vlbm_status server_rebuild(vlbm_server* sv) {
                                                                                       s->cfg.collision,
                                                                                       s->cfg.rheology)) *
                                              sv->sms * 256;
-            if (s->N >= wave) cand.emplace_back(s->N, (int)i);
+            if (s->N >= wave || s->pairH > 0) cand.emplace_back(s->N, (int)i);
             else host_us += 0.5;   // its share of the batched launches
         }
         std::sort(cand.begin(), cand.end(), std::greater<std::pair<long long, int>>());
         for (const auto& c : cand) {
-            if (sv->own_launch_min_nodes >= 0 || host_us + 4.0 <= 0.6 * gpu_us) {
+            // a z-paired lattice cannot join the natural-layout table
+            if (sv->res[c.second].sim->pairH > 0 || sv->own_launch_min_nodes >= 0 || host_us + 4.0 <= 0.6 * gpu_us) {
                 own[c.second] = 1;
                 host_us += 4.0;
             }
@@ -759,7 +760,18 @@ vlbm_status server_admit(vlbm_server* sv) {
         if (std::max(sv->bytes_in_use, sv->cache.live_bytes) + p.bytes > sv->budget) break;
         vlbm_config cfg = p.req.cfg;
         cfg.device = sv->device;
-        cfg.layout = VLBM_LAYOUT_NATURAL;   // the batched kernel streams one node per thread
+        {   // the batched kernel streams one node per thread (natural layout);
+            // lattices that always step with launches of their own (spheres, or
+            // a full wave of the batched kernel by themselves) take the
+            // library's layout, z-paired where that is faster
+            const long long n = (long long)cfg.nx * cfg.ny * cfg.nz;
+            const long long wave = sv->own_launch_min_nodes >= 0
+                                       ? sv->own_launch_min_nodes
+                                       : (long long)std::max(1, batched_blocks_per_sm(cfg.vel_set, cfg.storage,
+                                                                                      cfg.collision, cfg.rheology)) *
+                                             sv->sms * 256;
+            cfg.layout = (!p.spheres.empty() || n >= wave) ? VLBM_LAYOUT_AUTO : VLBM_LAYOUT_NATURAL;
+        }
         vlbm_sim* s = nullptr;
         const double a0 = now_s();
         // built without host waits on a high-priority stream of its own; the
