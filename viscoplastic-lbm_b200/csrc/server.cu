@@ -365,8 +365,9 @@ vlbm_status server_rebuild(vlbm_server* sv) {
     sv->own_res.clear();
     // Lattices with spheres step on their own side stream (fluid and IBM
     // launches).  A sphere-free lattice that fills a wave of the batched kernel
-    // by itself may get its own k_step launch (parameters in the constant bank,
-    // about 30 % faster per node than the batched kernel) on a side stream,
+    // by itself may get its own fused-step launches (parameters in the constant
+    // bank, about 30 % faster per node than the batched kernel; a z-paired
+    // lattice always does) on a side stream,
     // largest first, while the host time of all launches of a step stays below
     // about 60 % of the GPU time of the step; the rest share the batched
     // launches.  Estimates: 4 us of host time per launch, populations
