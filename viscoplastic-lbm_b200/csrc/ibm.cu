@@ -7,11 +7,11 @@
 // Eulerian nodes inside each sphere's stencil support are touched, in six
 // launches per step with one forcing iteration (three more per iteration):
 //
-//   k_ibm_begin      CTAs 0..np-1: unwrapped node extent -> Eulerian box of
-//                    each sphere, node forces reset (gpuResetNodesForces
-//                    ibm.cu:651-668); CTA np: old values, Hertz-Mindlin
-//                    contacts with deterministic slot updates and sums,
-//                    predictor
+//   k_ibm_begin      one CTA per sphere: unwrapped node extent -> Eulerian
+//                    box of each sphere, node forces reset (gpuResetNodesForces
+//                    ibm.cu:651-668); beside it and the gather, on a stream of
+//                    its own, one CTA: old values, Hertz-Mindlin contacts with
+//                    deterministic slot updates and sums, predictor
 //   k_ibm_gather     several CTAs per sphere: rho,u of the post-boundary
 //                    populations with the constant body force
 //                    (gpuUpdateMacrIBM ibm.cu:544-648) for the box nodes,
@@ -86,6 +86,8 @@ struct IbmState {
     double* contrib = nullptr;    // [np][np][6] pair force/torque on the row particle
     double* fpart = nullptr;      // [np][split][6] per-CTA force/torque partials
     int split = 1;                // CTAs per sphere in k_ibm_interp_spread
+    cudaStream_t cstream = nullptr;   // the contacts' launch, beside the boxes and the gather
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int gsplit = 1;               // CTAs per sphere in k_ibm_gather, k_ibm_euler and k_ibm_fixup
     std::vector<DPart> initial;   // for vlbm_init_equilibrium
     std::vector<double> init_nodes;
@@ -546,16 +548,19 @@ __device__ void ibm_contacts(const IbmParams& P, DPart* parts, double* contrib) 
     }
 }
 
-// One launch for the start of the IBM step: blocks 0..np-1 find the Eulerian
-// box of their sphere and reset its node forces (k_ibm_box part), block np
-// runs the old-value copy, the contacts and the predictor (they read
-// positions only, which the boxes do not change).
+// The start of the IBM step, two launches that run side by side: one CTA per
+// sphere finds the Eulerian box of its sphere and resets its node forces
+// (`contacts` 0, on the step's stream, followed by the gather); one CTA runs
+// the old-value copy, the contacts and the predictor (`contacts` 1, on the IBM
+// state's own stream, joined before the first interpolation).  They touch
+// different fields: the contacts read positions only, which the boxes and the
+// gather do not change.
 __global__ void __launch_bounds__(IBM_THREADS) k_ibm_begin(IbmParams P, DPart* parts, const double* X, const double* Y,
                                                             const double* Z, double* fx, double* fy, double* fz,
                                                             double* dx, double* dy, double* dz, double* contrib,
-                                                            const int* clock) {
+                                                            const int* clock, int contacts) {
     chain_enter();
-    if ((int)blockIdx.x < P.np) {
+    if (!contacts) {   // one CTA per sphere
         ibm_box(P, parts, blockIdx.x, X, Y, Z, fx, fy, fz, dx, dy, dz);
         return;
     }
@@ -953,10 +958,18 @@ vlbm_status ibm_step(vlbm_sim* s) {
     if (!st || st->np == 0) return VLBM_OK;
     const IbmParams& P = st->prm;
     cudaStream_t cs = s->stream;
-    k_ibm_begin<<<st->np + 1, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nfx, st->nfy, st->nfz,
-                                                     st->ndx, st->ndy, st->ndz, st->contrib, st->clock);
+    // contacts on the IBM state's stream, beside the boxes and the gather
+    IBM_CUDA(cudaEventRecord(st->ev_fork, cs));
+    IBM_CUDA(cudaStreamWaitEvent(st->cstream, st->ev_fork, 0));
+    k_ibm_begin<<<1, IBM_THREADS, 0, st->cstream>>>(P, st->parts, st->nx, st->ny, st->nz, st->nfx, st->nfy, st->nfz,
+                                                     st->ndx, st->ndy, st->ndz, st->contrib, st->clock, 1);
+    IBM_CUDA(cudaGetLastError());
+    IBM_CUDA(cudaEventRecord(st->ev_join, st->cstream));
+    k_ibm_begin<<<st->np, IBM_THREADS, 0, cs>>>(P, st->parts, st->nx, st->ny, st->nz, st->nfx, st->nfy, st->nfz,
+                                                 st->ndx, st->ndy, st->ndz, st->contrib, st->clock, 0);
     IBM_CUDA(cudaGetLastError());
     IBM_CUDA(gather_dispatch(s, st));
+    IBM_CUDA(cudaStreamWaitEvent(cs, st->ev_join, 0));   // the predictor before the first interpolation
     // the rest of the chain: programmatic dependents (chain_enter)
     const int iters = std::max(1, st->cfg.max_iterations);
     for (int it = 0; it < iters; ++it) {
@@ -1058,6 +1071,9 @@ void ibm_destroy(IbmState* st, DeviceAllocator* a) {
         free_with(a, p);
     free_with(a, st->npid); free_with(a, st->fields); free_with(a, st->faux); free_with(a, st->owner);
     free_with(a, st->clock);
+    if (st->ev_fork) cudaEventDestroy(st->ev_fork);
+    if (st->ev_join) cudaEventDestroy(st->ev_join);
+    if (st->cstream) cudaStreamDestroy(st->cstream);
     delete st;
 }
 
@@ -1199,6 +1215,9 @@ vlbm_status vlbm_add_spheres(vlbm_sim* s, const vlbm_ibm_config* ib, const vlbm_
         st->split = std::min(IBM_MAX_SPLIT, std::max(1, (most + IBM_NODES_PER_CTA - 1) / IBM_NODES_PER_CTA));
     }
     if (e == cudaSuccess) e = dalloc((void**)&st->fpart, (size_t)n * st->split * 6 * sizeof(double));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st->cstream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->ev_join, cudaEventDisableTiming);
     {   // CTAs per sphere of the box passes: about two box nodes per thread for the largest sphere
         long long maxbox = 1;
         for (int k = 0; k < n; ++k) {
