@@ -461,8 +461,11 @@ typedef struct vlbm_completion {
 
 /* A continuous-batching server on one GPU: requests are admitted by HBM budget,
  * stay resident, advance together in one batched launch per step, and retire at
- * their step count.  The reference has no counterpart (one compile-time
- * simulation per process). */
+ * their step count.  A lattice is built without host waits on a high-priority
+ * stream of its own (uploads from pinned staging); lattices with spheres or
+ * large enough to fill a wave of the batched kernel step with launches of
+ * their own in the library's layout.  The reference has no counterpart (one
+ * compile-time simulation per process). */
 vlbm_status vlbm_server_create(int device, size_t hbm_budget_bytes, int32_t max_resident,
                                vlbm_server** out);
 vlbm_status vlbm_server_submit(vlbm_server* srv, const vlbm_request* req);
