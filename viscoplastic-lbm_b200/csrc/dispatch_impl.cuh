@@ -8,8 +8,10 @@ namespace vlbm {
 inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
 
 // Launch that may start before the previous kernel of the stream has finished
-// (programmatic dependent launch): that kernel triggers it at its start, and
-// the two touch disjoint memory.  Work launched after it waits for both.
+// (programmatic dependent launch), once that kernel has triggered it.  Either
+// the two touch disjoint memory (the bulk grid after the step's boundary list)
+// or the launched kernel waits in-kernel (griddepcontrol.wait) for the
+// previous one's completion before it reads anything (the chained steps).
 template <typename... Args>
 cudaError_t launch_overlapped(void (*kernel)(Args...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
