@@ -150,3 +150,29 @@ def test_slab_refusals(vlbm):
     bad.slab_z_offset = 8
     with pytest.raises(vlbm.VlbmError):
         vlbm.Simulation(bad, builder=None)
+
+
+def test_single_rank_zslab_equals_the_whole_lattice(vlbm):
+    """ZSlab outside a process group: one rank whose slab is the whole lattice,
+    periodic onto itself through its own message buffers (what
+    `bench.py --shard` runs on one GPU); macroscopics after an even and after
+    an odd step and the FP64 sums equal the unsharded run's."""
+    kw = dict(eta_p=0.1, yield_stress=2e-6, fx=4e-5)
+    dims = (32, 12, 10)
+    cfg = make_cfg(vlbm, 19, "REG", "BINGHAM", dims, "NATURAL", kw)
+    whole = vlbm.Simulation(cfg, node_map=vlbm.build_node_map(vlbm.BUILDER_PLATES_Y, *dims))
+    slab = zslab.ZSlab(cfg, vlbm.BUILDER_PLATES_Y)
+    try:
+        assert (slab.z0, slab.n, slab.transport.world) == (0, dims[2], 1)
+        for steps in (7, 1):   # 7 and 8 steps taken: after an even and after an odd step
+            whole.step(steps)
+            slab.step(steps)
+            whole.sync()
+            torch.cuda.synchronize()
+            mw, ms = whole.macroscopics(), slab.macroscopics()
+            for k in ("rho", "ux", "uy", "uz"):
+                assert np.array_equal(ms[k], mw[k]), (steps, k)
+        assert np.allclose(slab.moments_sum(), whole.moments_sum(), rtol=1e-12, atol=1e-12)
+    finally:
+        slab.close()
+        whole.close()
